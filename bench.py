@@ -1,0 +1,426 @@
+#!/usr/bin/env python3
+"""Benchmark: elements ranked per second on one B200 (and weak-scaled over N).
+
+Workload (default): weighted list ranking of n = 2^28 elements, uint64
+indices, uint32 weights uniform in [0, 2^16), the list order a seeded random
+permutation; exact uint64 ranks.  Inputs are generated on the device by the
+library's seeded generators (no dataset exists for this path).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload list|list_local|forest_rrt|forest_cat]
+
+One JSON line on rank 0.  `value` is device-timed whole-job throughput with
+inputs resident in HBM; `e2e` is the same metric through the host-buffer API
+call (host->device copy of the inputs and device->host copy of root and rank
+inside the timed region).  Under torchrun every rank ranks its own instance
+(replicas, no data-path collective): scaling is weak.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "elements ranked/s"
+PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
+FALLBACK_HBM_GBS = 6650.0
+
+WORKLOADS = {
+    # name: (description, n, kind, layout/kind arg, weights)
+    "list": ("weighted list ranking, random permutation order, n=2^28, uint32 weights in [0,2^16)", 1 << 28,
+             "list", 0, True),
+    "list_local": ("weighted list ranking, runs of 64 consecutive indices in random run order, n=2^28, "
+                   "uint32 weights in [0,2^16)", 1 << 28, "list", 1, True),
+    "list20": ("list ranking, random permutation order, n=2^20, unit weights", 1 << 20, "list", 0, False),
+    "forest_rrt": ("tree rooting, 64 random recursive trees, n=2^26 vertices", 1 << 26, "forest", 0, False),
+    "forest_cat": ("tree rooting, 64 caterpillars (spine 2^19, uniform leaves), n=2^26 vertices", 1 << 26, "forest",
+                   1, False),
+}
+
+# Algorithmic bytes per unit (HBM roofline, integer work): stream-read succ
+# (8 B) + weights (4 B) + stream-write root and rank (16 B) + one random 32 B
+# sector for the dependent successor load.  Forest: 8 B parent + 16 B outputs
+# + 2 tour elements x (32 B random sector + 16 B streamed tour state).
+B_ALG = {"list": lambda w: 8 + (4 if w else 0) + 16 + 32, "forest": lambda w: 8 + 16 + 2 * (32 + 16)}
+# The chase kernel's own algorithmic bytes per element it visits: the
+# dependent 16 B record read lands in one random 32 B sector, and the 16 B
+# stamp it writes back.
+B_CHASE = 32 + 16
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def peaks():
+    if PEAKS_FILE.exists():
+        d = json.loads(PEAKS_FILE.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax = float(p[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device(f"cuda:{local}"))
+    else:
+        torch.cuda.set_device(0 if not torch.cuda.is_available() else local)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_reference_time(n_sample: int, wl: str, reps: int = 1) -> tuple[float, str, str]:
+    """The reference's own GatherChase (oracle/_ref, built from the reference
+    source) when present, else the oracle restatement; one host core."""
+    import numpy as np
+
+    import oracle
+
+    _, _, kind, arg, weighted = WORKLOADS[wl]
+    if kind == "list":
+        succ = oracle.gen_list(n_sample, 0xC1, arg)
+        rank = (oracle.gen_weights(n_sample, 0xC1 + 1, 16).astype(np.int64) if weighted
+                else np.ones(n_sample, np.int64))
+        rank[succ == np.arange(n_sample, dtype=np.uint64)] = 0
+    else:
+        succ = oracle.gen_forest(n_sample, 0xC2, arg, 64, n_sample // 128)
+        rank = np.where(succ == np.arange(n_sample, dtype=np.uint64), 0, 1).astype(np.int64)
+    use_ref = oracle.has_ref()
+    best = float("inf")
+    for _ in range(reps):
+        s, r = succ.copy(), rank.copy()
+        t0 = time.perf_counter()
+        if use_ref:
+            oracle.ref_local_pointer_chasing(s, r)
+        else:
+            oracle.local_pointer_chasing(s, r)
+        best = min(best, time.perf_counter() - t0)
+    return n_sample / best, ("reference" if use_ref else "port"), (
+        f"{n_sample}-element instance of the same generator, GatherChase "
+        f"(lib/kascade/local_pointer_chasing.cpp{' compiled from the reference source' if use_ref else ' restated'}),"
+        f" best of {reps}")
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    wl = args.workload
+    n_sample = args.cpu_sample
+    for _ in range(args.warmup):
+        cpu_reference_time(n_sample // 4, wl)
+    vals = []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        v, kind, sample = cpu_reference_time(n_sample, wl)
+        vals.append(v)
+    wall = time.perf_counter() - t0
+    v = statistics.median(vals)
+    out = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "elements/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * wall / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+        "config": {"workload": WORKLOADS[wl][0], "n": WORKLOADS[wl][1], "sample_n": n_sample,
+                   "parallelism": "one host core (GatherChase is sequential)"},
+        "cpu_baseline": {"value": v, "unit": "elements/s", "cores": 1, "kind": kind, "sample": sample},
+        "e2e": {"value": v, "unit": "elements/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference's MPI binary cannot be built here (no MPI, no network for its FetchContent "
+                "dependencies); its GatherChase source compiles standalone and is what runs",
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=list(WORKLOADS), default="list")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-sample", type=int, default=1 << 24)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true")
+    ap.add_argument("--spacing", type=int, default=0)
+    ap.add_argument("--chains", type=int, default=0)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+        return
+
+    import numpy as np
+    import torch
+
+    import kascade_b200 as kb
+
+    desc, n, kind, arg, weighted = WORKLOADS[args.workload]
+    dev = torch.device(f"cuda:{local}")
+    ctx = kb.Context(local)
+    stream = torch.cuda.current_stream(dev)
+    seed = 0xC1 + 1000 * rank
+    tuning = kb.GpuTuning(profile=True, ruler_spacing=args.spacing, chains_per_thread=args.chains)
+    if kind == "list":
+        inp = kb.gen_list(n, seed, arg, device=dev)
+        w = kb.gen_weights(n, seed + 1, 16, device=dev) if weighted else None
+        root = torch.empty(n, dtype=torch.int64, device=dev)
+        rk = torch.empty(n, dtype=torch.int64, device=dev)
+        ctx.reserve(kb.lib.kascade_scratch_bytes_rank_list(n))
+
+        def step():
+            kb.rank_list(inp, w, tuning=tuning, root_out=root, rank_out=rk, ctx=ctx)
+    else:
+        blocks = 64
+        spine = (n // blocks) // 2 if arg == 1 else 0
+        inp = kb.gen_forest(n, seed, arg, blocks, spine, device=dev)
+        w = None
+        root = torch.empty(n, dtype=torch.int64, device=dev)
+        rk = torch.empty(n, dtype=torch.int64, device=dev)
+        ctx.reserve(kb.lib.kascade_scratch_bytes_root_forest(n))
+
+        def step():
+            kb.root_forest(inp, tuning=tuning, root_out=root, depth_out=rk, ctx=ctx)
+
+    torch.cuda.synchronize()
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    ctx.reset_kernel_times()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    barrier(world)
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    t_ms = ev0.elapsed_time(ev1)
+    t_ms = max_over_ranks(t_ms, world)
+    ms_per_step = t_ms / args.steps
+    value = n * world / (ms_per_step / 1000.0)
+    ktimes = ctx.kernel_times()
+    launches = sum(c for (_, c) in ktimes.values())
+    step_kernel_ms = {k: v[0] / args.steps for k, v in ktimes.items()}
+    dominant = max(ktimes, key=lambda k: ktimes[k][0]) if ktimes else None
+    levels = ctx.levels()
+
+    hbm, hbm_src = peaks()
+    b_alg = B_ALG[kind](weighted)
+    pipe_gbs = n * b_alg / (ms_per_step / 1000.0) / 1e9
+    roofline = None
+    if dominant:
+        d_ms, d_cnt = ktimes[dominant]
+        per_launch_s = d_ms / d_cnt / 1000.0
+        if dominant == "chase":
+            # elements visited by the level-0 chase launch (every non-ruler
+            # element plus each ruler's own start record)
+            units = levels[0] if levels else n
+            per_launch_units = units * (1 if kind == "list" else 1)
+            launches_per_step = d_cnt / args.steps
+            # deeper-level chases are far smaller; attribute bytes of all
+            # levels, divided over the chase launches of one step
+            total_units = sum(levels[:-1]) if len(levels) > 1 else units
+            per_launch_bytes = B_CHASE * total_units / launches_per_step
+            bytes_note = (f"{B_CHASE} B per element visited (one random 32 B sector for the 16 B record + 16 B "
+                          f"stamp) x {total_units} elements over {launches_per_step:.0f} chase launches per step")
+        else:
+            per_launch_bytes = n * b_alg / (d_cnt / args.steps)
+            bytes_note = f"{b_alg} B/element x n per step, over this kernel's launches"
+        ach = per_launch_bytes / per_launch_s / 1e9
+        roofline = {"bound": "hbm", "kernel": dominant, "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
+                    "frac": round(ach / hbm, 4), "peak_source": f"{hbm_src} (MEASURED_PEAKS.json hbm_gbs)"
+                    if hbm_src == "measured" else "fallback 6.65 TB/s",
+                    "traffic": None, "algorithmic_bytes": bytes_note}
+    pipeline = {"b_alg_per_elem": b_alg, "achieved_gbs": round(pipe_gbs, 1), "frac": round(pipe_gbs / hbm, 4)}
+
+    # end-to-end through the host-buffer API (pinned host memory)
+    e2e = None
+    if args.e2e_steps > 0:
+        pin_in = torch.empty(n, dtype=torch.int64, pin_memory=True)
+        pin_in.copy_(inp.cpu())
+        pin_w = None
+        if w is not None:
+            pin_w = torch.empty(n, dtype=torch.int32, pin_memory=True)
+            pin_w.copy_(w.cpu())
+        pin_root = torch.empty(n, dtype=torch.int64, pin_memory=True)
+        pin_rank = torch.empty(n, dtype=torch.int64, pin_memory=True)
+        o = kb.GpuTuning(ruler_spacing=args.spacing, chains_per_thread=args.chains).to_opts()
+        import ctypes
+
+        def e2e_step():
+            if kind == "list":
+                st = kb.lib.kascade_rank_list_host(ctx.handle, pin_in.data_ptr(),
+                                                   pin_w.data_ptr() if pin_w is not None else None, n,
+                                                   pin_root.data_ptr(), pin_rank.data_ptr(), ctypes.byref(o),
+                                                   stream.cuda_stream)
+            else:
+                st = kb.lib.kascade_root_forest_host(ctx.handle, pin_in.data_ptr(), n, pin_root.data_ptr(),
+                                                     pin_rank.data_ptr(), ctypes.byref(o), stream.cuda_stream)
+            kb._lib.check(st, "host-buffer call", ctx.handle)
+
+        e2e_step()
+        barrier(world)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.e2e_steps):
+            e2e_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        te = max_over_ranks(e0.elapsed_time(e1), world) / args.e2e_steps
+        # correctness spot check of the host result against the device result
+        ok = bool(np.array_equal(pin_rank[:4096].numpy(), rk[:4096].cpu().numpy()))
+        h2d = n * 8 + (n * 4 if w is not None else 0)
+        e2e = {"value": n * world / (te / 1000.0), "unit": "elements/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": 16 * n, "ms_per_step": round(te, 3), "host_matches_device": ok}
+
+    secondary = {}
+    if not args.no_secondary and kind == "list" and args.workload == "list" and world == 1:
+        # the locality-biased layout of the same configuration
+        inp2 = kb.gen_list(n, seed, 1, device=dev)
+        tun2 = kb.GpuTuning(ruler_spacing=args.spacing, chains_per_thread=args.chains)
+        for _ in range(2):
+            kb.rank_list(inp2, w, tuning=tun2, root_out=root, rank_out=rk, ctx=ctx)
+        torch.cuda.synchronize()
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        for _ in range(3):
+            kb.rank_list(inp2, w, tuning=tun2, root_out=root, rank_out=rk, ctx=ctx)
+        a1.record(stream)
+        torch.cuda.synchronize()
+        tl = a0.elapsed_time(a1) / 3
+        secondary["list_local"] = {"workload": WORKLOADS["list_local"][0], "value": n / (tl / 1000.0),
+                                   "ms_per_step": round(tl, 3),
+                                   "pipeline_frac": round(n * b_alg / (tl / 1000.0) / 1e9 / hbm, 4)}
+        del inp2
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, kd, sample = cpu_reference_time(args.cpu_sample, args.workload)
+        cpu = {"value": v, "unit": "elements/s", "cores": 1, "kind": kd, "sample": sample}
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": "elements/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded device generator)",
+            "config": {"workload": desc, "n": n, "global_elements": n * world,
+                       "parallelism": f"replicas x{world} (independent instances, no collective)",
+                       "l2": "inputs larger than L2 (16 B records x n = %.1f GiB)" % (16 * n / 2**30),
+                       "ruler_spacing": args.spacing or "auto", "levels": levels},
+            "roofline": roofline, "pipeline_roofline": pipeline, "cpu_baseline": cpu, "e2e": e2e,
+            "clocks": clk, "gpu_launches": launches,
+            "kernels_ms_per_step": {k: round(v, 4) for k, v in sorted(step_kernel_ms.items())},
+            "secondary": secondary or None,
+        }
+        print(json.dumps(out), flush=True)
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

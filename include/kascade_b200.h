@@ -1,0 +1,233 @@
+/*
+ * kascade_b200 -- list ranking and tree rooting on one NVIDIA B200 (sm_100a).
+ *
+ * C ABI of libkascade_b200.so.  It replaces the free functions of the
+ * reference's lib/kascade (niklas-uhl/kascade) for one GPU: the MPI
+ * Distribution and Communicator arguments disappear, the arrays become
+ * device (or host) pointers plus a length, and errors become status codes.
+ *
+ * Conventions
+ *  - Indices are uint64_t (reference idx_t, lib/kascade/types.hpp:8); ranks
+ *    are int64_t in the reference-shaped calls (rank_t, types.hpp:9) and
+ *    uint64_t in the plain calls.  A root is an element that is its own
+ *    successor (lib/kascade/successor_utils.cpp:65-70).
+ *  - Element counts are limited to n <= 2^32 - 2 for lists and n <= 2^31 - 1
+ *    for forests (the library keeps 32-bit indices in HBM).
+ *  - Device-pointer calls are ordered on `stream` (a cudaStream_t, NULL =
+ *    legacy default stream).  They return once the result is complete and
+ *    its status known, unless kascade_opts.async is set, in which case they
+ *    return after enqueueing and kascade_ctx_sync() reports the status.
+ *  - One context per host thread; contexts own all scratch memory.
+ *  - No exceptions cross this boundary.
+ */
+#ifndef KASCADE_B200_H
+#define KASCADE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(_WIN32)
+#define KASCADE_API
+#else
+#define KASCADE_API __attribute__((visibility("default")))
+#endif
+
+typedef enum kascade_status {
+  KASCADE_OK = 0,
+  KASCADE_ERR_INVALID_ARG = 1,  /* bad pointer / size / option                    */
+  KASCADE_ERR_OUT_OF_RANGE = 2, /* a successor or parent index >= n               */
+  KASCADE_ERR_CYCLE = 3,        /* a cycle without a root (a bounded loop ran out) */
+  KASCADE_ERR_NOT_A_LIST = 4,   /* an element with two predecessors given to a
+                                   list ranker                                   */
+  KASCADE_ERR_TIMEOUT = 5,      /* a bounded device wait ran out                 */
+  KASCADE_ERR_OOM = 6,          /* device or pinned allocation failed            */
+  KASCADE_ERR_CUDA = 7,         /* a CUDA runtime call failed                    */
+  KASCADE_ERR_TOO_LARGE = 8,    /* n beyond the supported index range            */
+  KASCADE_ERR_UNSUPPORTED = 9   /* option not available in this build            */
+} kascade_status;
+
+/* Algorithms, mirroring kascade::Algorithm (lib/kascade/configuration.hpp:9-18).
+ * On one GPU the message layers of the variants disappear:
+ *  GATHER_CHASE, POINTER_DOUBLING, ASYNC_POINTER_DOUBLING and
+ *  RMA_POINTER_DOUBLING all run the double-buffered jump kernel (they accept
+ *  forests of trees as well as lists); SPARSE_RULING_SET runs the recursive
+ *  ruling-set ranker (lists only). */
+typedef enum kascade_algorithm {
+  KASCADE_ALGO_GATHER_CHASE = 0,
+  KASCADE_ALGO_POINTER_DOUBLING = 1,
+  KASCADE_ALGO_ASYNC_POINTER_DOUBLING = 2,
+  KASCADE_ALGO_RMA_POINTER_DOUBLING = 3,
+  KASCADE_ALGO_SPARSE_RULING_SET = 4,
+  KASCADE_ALGO_EULER_TOUR = 5
+} kascade_algorithm;
+
+/* Tunables.  Zero means "choose automatically" (the autotuned table).  The
+ * reference's ruler-selection strategies (ruler_selection.hpp:18-79) size the
+ * ruler set by the MPI rank count; on one GPU the mean ruler spacing is the
+ * tunable instead (sparse_ruling_set.cpp:120-136 picks; here a counter hash
+ * picks). */
+typedef struct kascade_opts {
+  uint32_t struct_size;       /* sizeof(kascade_opts)                               */
+  uint32_t algorithm;         /* kascade_algorithm for list ranking                 */
+  uint32_t ruler_spacing;     /* mean elements per ruler at level 0 (0 = auto)      */
+  uint32_t ruler_spacing_deep;/* the same for recursion levels >= 1 (0 = auto)      */
+  uint32_t max_levels;        /* ruling-set recursion depth before the base case
+                                 (sparse_ruling_set_rounds, configuration.hpp:70)  */
+  uint32_t base_case_size;    /* at most this many elements go to the one-CTA
+                                 base case (0 = auto)                              */
+  uint32_t chains_per_thread; /* independent chains in flight per thread (0=auto) */
+  uint32_t block_size;        /* threads per CTA of the chase kernel (0 = auto)     */
+  uint32_t validate;          /* 1: check is_list before a list-only algorithm      */
+  uint32_t async;             /* 1: return after enqueueing; see kascade_ctx_sync   */
+  uint32_t profile;           /* 1: time each kernel with CUDA events               */
+  uint32_t seed;              /* ruler-sampling seed                                */
+} kascade_opts;
+
+typedef struct kascade_ctx kascade_ctx;
+
+KASCADE_API const char* kascade_version(void);
+KASCADE_API const char* kascade_status_string(kascade_status s);
+KASCADE_API void kascade_opts_init(kascade_opts* opts);
+
+/* Context: device, scratch arena (grows on demand, reused across calls),
+ * status word and pinned read-back buffer. */
+KASCADE_API kascade_status kascade_ctx_create(int device, kascade_ctx** out);
+KASCADE_API kascade_status kascade_ctx_destroy(kascade_ctx* ctx);
+/* Pre-size the scratch arena to hold `bytes` (avoids growth inside a call). */
+KASCADE_API kascade_status kascade_ctx_reserve(kascade_ctx* ctx, uint64_t bytes);
+/* Scratch bytes a call of that size typically needs (the arena grows beyond
+ * this only for inputs made mostly of roots). */
+KASCADE_API uint64_t kascade_scratch_bytes_rank_list(uint64_t n);
+KASCADE_API uint64_t kascade_scratch_bytes_root_forest(uint64_t n);
+/* Wait for the context's last call on `stream` and return its status. */
+KASCADE_API kascade_status kascade_ctx_sync(kascade_ctx* ctx, void* stream);
+/* Detail of the last device-side error (e.g. the offending index). */
+KASCADE_API uint64_t kascade_ctx_error_info(kascade_ctx* ctx);
+/* Kernel timings of the last profiled call(s): fills up to `cap` entries of
+ * names/milliseconds/launch counts, returns the number of kernels. */
+KASCADE_API int kascade_ctx_kernel_times(kascade_ctx* ctx, const char** names, double* ms,
+                                         uint64_t* launches, int cap);
+KASCADE_API void kascade_ctx_reset_kernel_times(kascade_ctx* ctx);
+/* Per-call statistics of the last ranking (levels, rulers per level). */
+KASCADE_API int kascade_ctx_last_levels(kascade_ctx* ctx, uint64_t* sizes, int cap);
+
+/* ----------------------------------------------------------------------------
+ * List ranking, plain form (device pointers).
+ *   succ[i]   successor of i (succ[i] == i marks a root)
+ *   weights   distance from i to succ[i] (NULL = unit); ignored at roots
+ *   root_out  root of i;  rank_out: sum of weights from i to its root,
+ *             excluding the root (0 at roots)
+ * Replaces: set_initial_ranking_state + sparse_ruling_set / pointer_doubling
+ * (lib/kascade/list_ranking.hpp:83-86, sparse_ruling_set.hpp:13-18,
+ * pointer_doubling.hpp:18-23); outputs must not alias succ.
+ * ------------------------------------------------------------------------- */
+KASCADE_API kascade_status kascade_rank_list(kascade_ctx* ctx, const uint64_t* succ,
+                                             const uint32_t* weights, uint64_t n,
+                                             uint64_t* root_out, uint64_t* rank_out,
+                                             const kascade_opts* opts, void* stream);
+
+/* Host-pointer variant: copies in, ranks, copies out (pinned or pageable). */
+KASCADE_API kascade_status kascade_rank_list_host(kascade_ctx* ctx, const uint64_t* succ,
+                                                  const uint32_t* weights, uint64_t n,
+                                                  uint64_t* root_out, uint64_t* rank_out,
+                                                  const kascade_opts* opts, void* stream);
+
+/* ----------------------------------------------------------------------------
+ * Reference-shaped in-place calls (device pointers).  succ_array holds the
+ * successors on input and the roots on output; rank_array holds each
+ * element's distance to its successor on input (0 at roots) and its distance
+ * to the root on output.  Roots keep their input values, exactly as the
+ * reference's GatherChase leaves them (local_pointer_chasing.cpp:18-59).
+ * ------------------------------------------------------------------------- */
+/* kascade::sparse_ruling_set (sparse_ruling_set.hpp:13-18, .cpp:335-392) */
+KASCADE_API kascade_status kascade_sparse_ruling_set(kascade_ctx* ctx, const kascade_opts* opts,
+                                                     uint64_t* succ_array, int64_t* rank_array,
+                                                     uint64_t n, void* stream);
+/* kascade::pointer_doubling (pointer_doubling.hpp:18-23), also standing in for
+ * async_pointer_doubling and rma_pointer_doubling (:29-43) */
+KASCADE_API kascade_status kascade_pointer_doubling(kascade_ctx* ctx, const kascade_opts* opts,
+                                                    uint64_t* succ_array, int64_t* rank_array,
+                                                    uint64_t n, void* stream);
+/* kascade::rank_on_root / local_pointer_chasing (list_ranking.hpp:55-64):
+ * the GatherChase contract, forests of trees allowed */
+KASCADE_API kascade_status kascade_rank_on_root(kascade_ctx* ctx, uint64_t* succ_array,
+                                                int64_t* rank_array, uint64_t n, void* stream);
+/* kascade::set_initial_ranking_state (list_ranking.hpp:83-86, .cpp:148-168):
+ * root := succ, rank := 1 (0 at roots) */
+KASCADE_API kascade_status kascade_set_initial_ranking_state(kascade_ctx* ctx, const uint64_t* succ,
+                                                             uint64_t* root_array,
+                                                             int64_t* rank_array, uint64_t n,
+                                                             void* stream);
+/* kascade::is_list (successor_utils.hpp:19-24): 1 if no element has two
+ * predecessors */
+KASCADE_API kascade_status kascade_is_list(kascade_ctx* ctx, const uint64_t* succ, uint64_t n,
+                                           int* is_list_out, void* stream);
+
+/* ----------------------------------------------------------------------------
+ * Tree rooting (device pointers).
+ *   parent[v] (parent[v] == v marks a root) -> root_out[v], depth_out[v]
+ *   (edge count to the root; 0 at roots), via an Euler tour of the forest
+ *   ranked by the ruling-set ranker.
+ * Replaces: rank_via_euler_tour (eulertour.hpp:22-27, .cpp:372-412).
+ * ------------------------------------------------------------------------- */
+KASCADE_API kascade_status kascade_root_forest(kascade_ctx* ctx, const uint64_t* parent,
+                                               uint64_t n, uint64_t* root_out,
+                                               uint64_t* depth_out, const kascade_opts* opts,
+                                               void* stream);
+KASCADE_API kascade_status kascade_root_forest_host(kascade_ctx* ctx, const uint64_t* parent,
+                                                    uint64_t n, uint64_t* root_out,
+                                                    uint64_t* depth_out, const kascade_opts* opts,
+                                                    void* stream);
+/* In-place form of kascade::rank_via_euler_tour: succ_array holds parents on
+ * input and roots on output, rank_array receives depths; roots keep their
+ * input values (eulertour.cpp:270-313 writes non-roots only). */
+KASCADE_API kascade_status kascade_rank_via_euler_tour(kascade_ctx* ctx, const kascade_opts* opts,
+                                                       uint64_t* succ_array, int64_t* rank_array,
+                                                       uint64_t n, void* stream);
+/* kascade::compute_euler_tour (eulertour.hpp:32-34, .cpp:414-427) on one rank:
+ * the tour's successor array in the reference's element numbering, m =
+ * 2 (n - #roots) + #roots elements.  tour_succ must hold 2n entries; *m_out
+ * receives m.  (The high-degree proxy variant is not provided.) */
+KASCADE_API kascade_status kascade_compute_euler_tour(kascade_ctx* ctx, const uint64_t* parent,
+                                                      uint64_t n, uint64_t* tour_succ,
+                                                      uint64_t* m_out, void* stream);
+
+/* ----------------------------------------------------------------------------
+ * Pack / unpack of an active sub-list (lib/kascade/pack.hpp:23-177).
+ * active[] lists k element indices in increasing order; every active
+ * element's successor must be active.  pack writes the sub-list in the dense
+ * index space 0..k-1; unpack writes a ranked sub-list back, translating its
+ * successors (roots) to original indices.
+ * ------------------------------------------------------------------------- */
+KASCADE_API kascade_status kascade_pack(kascade_ctx* ctx, const uint64_t* succ,
+                                        const int64_t* rank, uint64_t n, const uint64_t* active,
+                                        uint64_t k, uint64_t* succ_packed, int64_t* rank_packed,
+                                        void* stream);
+KASCADE_API kascade_status kascade_unpack(kascade_ctx* ctx, const uint64_t* succ_packed,
+                                          const int64_t* rank_packed, const uint64_t* active,
+                                          uint64_t k, uint64_t* succ, int64_t* rank, uint64_t n,
+                                          void* stream);
+
+/* ----------------------------------------------------------------------------
+ * Seeded synthetic inputs (device pointers), the benchmark generators.
+ *   layout: 0 random permutation order, 1 runs of 64 consecutive indices in
+ *   random run order, 2 identity order.  kind: 0 random recursive trees in
+ *   `blocks` trees, 1 caterpillars (`blocks` of them, spine length `spine`).
+ * ------------------------------------------------------------------------- */
+KASCADE_API kascade_status kascade_gen_list(uint64_t n, uint64_t seed, uint32_t layout,
+                                            uint64_t* succ, void* stream);
+KASCADE_API kascade_status kascade_gen_weights(uint64_t n, uint64_t seed, uint32_t wbits,
+                                               uint32_t* weights, void* stream);
+KASCADE_API kascade_status kascade_gen_forest(uint64_t n, uint64_t seed, uint32_t kind,
+                                              uint64_t blocks, uint64_t spine, uint64_t* parent,
+                                              void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KASCADE_B200_H */

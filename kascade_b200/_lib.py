@@ -1,0 +1,155 @@
+"""ctypes binding of libkascade_b200.so (the C ABI in include/kascade_b200.h).
+
+The shared library is built in-tree (``python -m kascade_b200.build`` or
+``__graft_entry__.build()``).  There is no fallback: if the library is absent
+or fails to load, importing this module raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = Path(os.environ.get("KASCADE_B200_LIB", _PKG / "libkascade_b200.so"))
+
+if not LIB_PATH.exists():
+    raise ImportError(
+        f"kascade_b200: native library {LIB_PATH} is missing; build it with "
+        "`python -m kascade_b200.build` (nvcc for sm_100a is required)"
+    )
+
+lib = ctypes.CDLL(str(LIB_PATH))
+
+c_void_p = ctypes.c_void_p
+c_u64 = ctypes.c_uint64
+c_u32 = ctypes.c_uint32
+c_int = ctypes.c_int
+P = ctypes.POINTER
+
+
+class Opts(ctypes.Structure):
+    """Mirror of ``kascade_opts``."""
+
+    _fields_ = [
+        ("struct_size", c_u32),
+        ("algorithm", c_u32),
+        ("ruler_spacing", c_u32),
+        ("ruler_spacing_deep", c_u32),
+        ("max_levels", c_u32),
+        ("base_case_size", c_u32),
+        ("chains_per_thread", c_u32),
+        ("block_size", c_u32),
+        ("validate", c_u32),
+        ("async_", c_u32),
+        ("profile", c_u32),
+        ("seed", c_u32),
+    ]
+
+
+_ctx_p = c_void_p
+_status = c_int
+
+_SIGS = {
+    "kascade_version": (ctypes.c_char_p, []),
+    "kascade_status_string": (ctypes.c_char_p, [c_int]),
+    "kascade_opts_init": (None, [P(Opts)]),
+    "kascade_ctx_create": (_status, [c_int, P(c_void_p)]),
+    "kascade_ctx_destroy": (_status, [_ctx_p]),
+    "kascade_ctx_reserve": (_status, [_ctx_p, c_u64]),
+    "kascade_scratch_bytes_rank_list": (c_u64, [c_u64]),
+    "kascade_scratch_bytes_root_forest": (c_u64, [c_u64]),
+    "kascade_ctx_sync": (_status, [_ctx_p, c_void_p]),
+    "kascade_ctx_error_info": (c_u64, [_ctx_p]),
+    "kascade_ctx_kernel_times": (
+        c_int,
+        [_ctx_p, P(ctypes.c_char_p), P(ctypes.c_double), P(c_u64), c_int],
+    ),
+    "kascade_ctx_reset_kernel_times": (None, [_ctx_p]),
+    "kascade_ctx_last_levels": (c_int, [_ctx_p, P(c_u64), c_int]),
+    "kascade_rank_list": (
+        _status,
+        [_ctx_p, c_void_p, c_void_p, c_u64, c_void_p, c_void_p, P(Opts), c_void_p],
+    ),
+    "kascade_rank_list_host": (
+        _status,
+        [_ctx_p, c_void_p, c_void_p, c_u64, c_void_p, c_void_p, P(Opts), c_void_p],
+    ),
+    "kascade_sparse_ruling_set": (_status, [_ctx_p, P(Opts), c_void_p, c_void_p, c_u64, c_void_p]),
+    "kascade_pointer_doubling": (_status, [_ctx_p, P(Opts), c_void_p, c_void_p, c_u64, c_void_p]),
+    "kascade_rank_on_root": (_status, [_ctx_p, c_void_p, c_void_p, c_u64, c_void_p]),
+    "kascade_set_initial_ranking_state": (
+        _status,
+        [_ctx_p, c_void_p, c_void_p, c_void_p, c_u64, c_void_p],
+    ),
+    "kascade_is_list": (_status, [_ctx_p, c_void_p, c_u64, P(c_int), c_void_p]),
+    "kascade_root_forest": (
+        _status,
+        [_ctx_p, c_void_p, c_u64, c_void_p, c_void_p, P(Opts), c_void_p],
+    ),
+    "kascade_root_forest_host": (
+        _status,
+        [_ctx_p, c_void_p, c_u64, c_void_p, c_void_p, P(Opts), c_void_p],
+    ),
+    "kascade_rank_via_euler_tour": (_status, [_ctx_p, P(Opts), c_void_p, c_void_p, c_u64, c_void_p]),
+    "kascade_compute_euler_tour": (_status, [_ctx_p, c_void_p, c_u64, c_void_p, P(c_u64), c_void_p]),
+    "kascade_pack": (
+        _status,
+        [_ctx_p, c_void_p, c_void_p, c_u64, c_void_p, c_u64, c_void_p, c_void_p, c_void_p],
+    ),
+    "kascade_unpack": (
+        _status,
+        [_ctx_p, c_void_p, c_void_p, c_void_p, c_u64, c_void_p, c_void_p, c_u64, c_void_p],
+    ),
+    "kascade_gen_list": (_status, [c_u64, c_u64, c_u32, c_void_p, c_void_p]),
+    "kascade_gen_weights": (_status, [c_u64, c_u64, c_u32, c_void_p, c_void_p]),
+    "kascade_gen_forest": (_status, [c_u64, c_u64, c_u32, c_u64, c_u64, c_void_p, c_void_p]),
+}
+
+for _name, (_res, _args) in _SIGS.items():
+    _fn = getattr(lib, _name)
+    _fn.restype = _res
+    _fn.argtypes = _args
+
+
+STATUS_NAMES = {
+    0: "OK",
+    1: "INVALID_ARG",
+    2: "OUT_OF_RANGE",
+    3: "CYCLE",
+    4: "NOT_A_LIST",
+    5: "TIMEOUT",
+    6: "OOM",
+    7: "CUDA",
+    8: "TOO_LARGE",
+    9: "UNSUPPORTED",
+}
+
+
+class KascadeError(RuntimeError):
+    """A non-OK ``kascade_status``; ``.status`` holds the code."""
+
+    def __init__(self, status: int, where: str, info: int | None = None):
+        self.status = status
+        self.name = STATUS_NAMES.get(status, str(status))
+        msg = lib.kascade_status_string(status).decode()
+        detail = f" (info {info})" if info else ""
+        super().__init__(f"{where}: KASCADE_ERR_{self.name}: {msg}{detail}")
+
+
+def check(status: int, where: str, ctx=None) -> None:
+    if status != 0:
+        info = lib.kascade_ctx_error_info(ctx) if ctx else None
+        raise KascadeError(status, where, info)
+
+
+def declared_symbols(header: Path | None = None) -> list[str]:
+    """Function names declared with KASCADE_API in the public C headers."""
+    import re
+
+    inc = _PKG.parent / "include"
+    names: list[str] = []
+    for h in [header] if header else sorted(inc.glob("*.h")):
+        text = Path(h).read_text()
+        names += re.findall(r"KASCADE_API[^;{(]*?\b(kascade_\w+)\s*\(", text, flags=re.S)
+    return names

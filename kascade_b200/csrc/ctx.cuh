@@ -1,0 +1,107 @@
+// Library context: device properties, a growable scratch arena, the device
+// status word, a pinned read-back buffer and optional per-kernel timing.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+struct kascade_ctx {
+  int device = 0;
+  int sm_count = 148;
+  size_t l2_bytes = 0;
+  size_t smem_optin = 0;
+  ks::DevStatus* d_status = nullptr;
+  unsigned long long* h_pinned = nullptr;  // KS_PINNED_WORDS words
+  // scratch arena: blocks are never freed inside a call, so pointers handed
+  // out by alloc() stay valid until the next begin_call()
+  struct Block {
+    char* ptr;
+    size_t cap;
+    size_t used;
+  };
+  std::vector<Block> blocks;
+  size_t reserve_bytes = 0;
+  // profiling
+  bool profile = false;
+  struct Pending {
+    const char* name;
+    cudaEvent_t a, b;
+  };
+  std::vector<Pending> pending;
+  std::vector<cudaEvent_t> event_pool;
+  std::map<std::string, std::pair<double, unsigned long long>> times;
+  std::vector<std::string> time_names;  // stable storage for returned names
+  std::vector<unsigned long long> last_levels;
+  unsigned long long error_info = 0;
+  kascade_status last_status = KASCADE_OK;
+  // ordering between calls issued on different streams: the next call's
+  // stream waits for the previous call's completion event before it reuses
+  // the arena
+  cudaEvent_t done_event = nullptr;
+  cudaStream_t last_stream = nullptr;
+  bool async_pending = false;
+};
+
+namespace ks {
+
+constexpr int KS_PINNED_WORDS = 64;
+
+// Arena -------------------------------------------------------------------
+kascade_status arena_begin_call(kascade_ctx& ctx, cudaStream_t s);
+void* arena_alloc(kascade_ctx& ctx, size_t bytes);  // nullptr on OOM
+template <class T>
+T* alloc(kascade_ctx& ctx, size_t count) {
+  return reinterpret_cast<T*>(arena_alloc(ctx, count * sizeof(T) + 16));
+}
+
+// Status --------------------------------------------------------------------
+kascade_status cuda_status(cudaError_t e);
+// Clear the device status word (stream-ordered).
+kascade_status status_reset(kascade_ctx& ctx, cudaStream_t s);
+// Synchronise `s`, read the device status word, collect kernel timings.
+kascade_status status_finish(kascade_ctx& ctx, cudaStream_t s);
+// Read one device word into the pinned buffer and wait for it.
+kascade_status read_u32(kascade_ctx& ctx, const uint32_t* dptr, uint32_t* out, cudaStream_t s);
+
+// Profiling ----------------------------------------------------------------
+struct ProfScope {
+  kascade_ctx& ctx;
+  cudaStream_t s;
+  const char* name;
+  cudaEvent_t b = nullptr;
+  ProfScope(kascade_ctx& c, const char* nm, cudaStream_t st);
+  ~ProfScope();
+};
+
+inline unsigned grid_for(const kascade_ctx& ctx, uint64_t work, unsigned block, unsigned per_sm_cap) {
+  uint64_t g = (work + block - 1) / block;
+  uint64_t cap = (uint64_t)ctx.sm_count * per_sm_cap;
+  if (g > cap) g = cap;
+  if (g == 0) g = 1;
+  return (unsigned)g;
+}
+
+}  // namespace ks
+
+#define KS_CHECK_LAUNCH()                                   \
+  do {                                                      \
+    cudaError_t _e = cudaGetLastError();                    \
+    if (_e != cudaSuccess) return ks::cuda_status(_e);      \
+  } while (0)
+
+#define KS_TRY(expr)                                        \
+  do {                                                      \
+    kascade_status _s = (expr);                             \
+    if (_s != KASCADE_OK) return _s;                        \
+  } while (0)
+
+#define KS_CUDA(expr)                                       \
+  do {                                                      \
+    cudaError_t _e = (expr);                                \
+    if (_e != cudaSuccess) return ks::cuda_status(_e);      \
+  } while (0)

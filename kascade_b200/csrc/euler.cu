@@ -1,0 +1,271 @@
+// Tree rooting via an Euler tour of the forest.
+//
+// Reference: rank_via_euler_tour / compute_euler_tour_impl / map_euler_tour_back
+// (lib/kascade/eulertour.cpp:68-162, 230-313, 372-427) with the forest built
+// by reverse_rooted_tree + make_graph (lib/kascade/successor_utils.cpp:236-300).
+//
+// Layout used for ranking (m = 2n elements):
+//   slot v        (v < n)  : the up edge v -> parent(v); for a root r it is
+//                            the tour's terminal element (weight 0, the
+//                            reference's dummy root element)
+//   slot n + q    (q < n)  : the down edge parent -> child of the q-th entry
+//                            of the children array sorted by parent; a root's
+//                            own entry (key = value = r) is an unused self loop
+// so that the depth of v is the rank of slot v and the final map-back is a
+// coalesced pass over slots 0..n-1.  Rotation at a vertex: parent first, then
+// children in increasing id; the tour of a tree starts at the down edge to
+// the root's first child and ends in the root's terminal slot.
+#include "ranker.cuh"
+#include "sort.cuh"
+
+namespace ks {
+
+namespace {
+
+constexpr int TB_ITEMS = 4;
+
+inline int bits_for(uint64_t n) {
+  int b = 1;
+  while (b < 63 && (1ull << b) < n) b++;
+  return b;
+}
+
+// seg[v] = [start, end) of v's entries in the sorted children array
+__global__ void __launch_bounds__(256) k_seg_bounds(const uint32_t* __restrict__ keys, uint32_t n,
+                                                    uint2* __restrict__ seg) {
+  for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t k = keys[q];
+    if (q == 0 || keys[q - 1] != k) seg[k].x = (uint32_t)q;
+    if (q + 1 == n || keys[q + 1] != k) seg[k].y = (uint32_t)(q + 1);
+  }
+}
+
+// Writes both tour records of every sorted entry q, samples rulers among the
+// written slots and numbers them (one atomic per tile, as in prepare).
+__global__ void __launch_bounds__(256) k_tour_build(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
+                                                    uint32_t n, const uint2* __restrict__ seg, Rec* __restrict__ rec,
+                                                    uint32_t* __restrict__ ruler_elem, uint32_t* __restrict__ counter,
+                                                    uint32_t salt, uint32_t thresh, DevStatus* st) {
+  __shared__ uint32_t sm[33];
+  __shared__ uint32_t sbase;
+  const uint64_t tile_sz = (uint64_t)blockDim.x * TB_ITEMS;
+  for (uint64_t tile = (uint64_t)blockIdx.x * tile_sz; tile < n; tile += (uint64_t)gridDim.x * tile_sz) {
+    Rec ru[TB_ITEMS], rd[TB_ITEMS];
+    uint32_t su[TB_ITEMS], sd[TB_ITEMS];
+    uint32_t rl = 0, cnt = 0;
+#pragma unroll
+    for (int i = 0; i < TB_ITEMS; ++i) {
+      const uint64_t q = tile + (uint64_t)i * blockDim.x + threadIdx.x;
+      su[i] = sd[i] = 0;
+      if (q >= n) continue;
+      const uint32_t p = keys[q], c = vals[q];
+      const uint32_t slot_down = n + (uint32_t)q;
+      if (p == c) {
+        // root r = p: terminal slot r and the unused down slot, both self loops
+        ru[i].a = 0;
+        ru[i].b = p;
+        su[i] = p;
+        rd[i].a = 0;
+        rd[i].b = slot_down;
+        sd[i] = slot_down;
+        rl |= 3u << (2 * i);
+        cnt += 2;
+      } else {
+        // up edge c -> p: continue with p's next child, else leave p
+        uint64_t q1 = q + 1;
+        if (q1 < n && keys[q1] == p && vals[q1] == p) q1++;
+        const uint32_t succ_up = (q1 < n && keys[q1] == p) ? n + (uint32_t)q1 : p;
+        ru[i].a = 1ull;
+        ru[i].b = succ_up;
+        su[i] = c;
+        // down edge p -> c: descend to c's first child, else come back up
+        const uint2 sg = seg[c];
+        rd[i].a = ~0ull;  // -1
+        rd[i].b = (sg.x < sg.y) ? n + sg.x : c;
+        sd[i] = slot_down;
+        if (sampled(c, salt, thresh)) {
+          rl |= 1u << (2 * i);
+          cnt++;
+        }
+        if (sampled(slot_down, salt, thresh)) {
+          rl |= 2u << (2 * i);
+          cnt++;
+        }
+      }
+    }
+    uint32_t total;
+    uint32_t pre = block_exclusive_scan(cnt, sm, &total);
+    if (threadIdx.x == 0) {
+      uint32_t b = total ? atomicAdd(counter, total) : 0u;
+      if ((uint64_t)b + total > MAX_RULERS) set_error(st, KASCADE_ERR_TOO_LARGE, b);
+      sbase = b;
+    }
+    __syncthreads();
+    uint32_t id = sbase + pre;
+#pragma unroll
+    for (int i = 0; i < TB_ITEMS; ++i) {
+      const uint64_t q = tile + (uint64_t)i * blockDim.x + threadIdx.x;
+      if (q >= n) continue;
+      ru[i].c = TAG_UNREACHED;
+      rd[i].c = TAG_UNREACHED;
+      if ((rl >> (2 * i)) & 1u) {
+        if (id < MAX_RULERS) {
+          ru[i].c = TAG_RULER | id;
+          ruler_elem[id] = su[i];
+        }
+        id++;
+      }
+      if ((rl >> (2 * i)) & 2u) {
+        if (id < MAX_RULERS) {
+          rd[i].c = TAG_RULER | id;
+          ruler_elem[id] = sd[i];
+        }
+        id++;
+      }
+      rec[su[i]] = ru[i];
+      rec[sd[i]] = rd[i];
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// compute_euler_tour in the reference's numbering (one rank).
+// ---------------------------------------------------------------------------
+// deg[v] = #children + (v not a root); droot[v] = 1 for roots with deg > 0
+__global__ void __launch_bounds__(256) k_ref_degrees(const uint64_t* __restrict__ parent, uint32_t n,
+                                                     const uint2* __restrict__ seg, uint32_t* __restrict__ deg,
+                                                     uint32_t* __restrict__ droot) {
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x) {
+    const bool root = parent[v] == v;
+    const uint2 sg = seg[v];
+    const uint32_t children = (sg.y - sg.x) - (root ? 1u : 0u);
+    const uint32_t d = children + (root ? 0u : 1u);
+    deg[v] = d;
+    droot[v] = (root && d > 0) ? 1u : 0u;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_iota64(uint64_t* __restrict__ out, uint64_t m) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = i;
+}
+
+// Per sorted child entry (p, c): the element (c, p) and the element (p, c).
+// A vertex v's neighbours in the reference CSR are ordered by decreasing key,
+// with key(child) = child id and key(parent) = v (successor_utils.cpp:281-293
+// appends (i, parent) then (parent, i) for i ascending; make_graph fills each
+// segment from its end).
+__global__ void __launch_bounds__(256) k_ref_tour(const uint64_t* __restrict__ parent, const uint32_t* __restrict__ keys,
+                                                  const uint32_t* __restrict__ vals, uint32_t n,
+                                                  const uint2* __restrict__ seg, const uint32_t* __restrict__ deg,
+                                                  const uint32_t* __restrict__ xadj, const uint32_t* __restrict__ didx,
+                                                  uint32_t num_edges, uint64_t* __restrict__ tour) {
+  for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t p = keys[q], c = vals[q];
+    if (p == c) continue;
+    const bool proot = parent[p] == p;
+    const uint2 sp = seg[p], sc = seg[c];
+    const uint32_t cc_p = (sp.y - sp.x) - (proot ? 1u : 0u);
+    // index of c among p's children in increasing id order
+    uint32_t j = (uint32_t)q - sp.x;
+    if (proot && p < c) j -= 1;  // p's own entry sits before c
+    const uint32_t pos_c_in_p = (cc_p - 1 - j) + ((!proot && p > c) ? 1u : 0u);
+    // number of c's children with id > c (c is not a root: no own entry)
+    uint32_t lo = sc.x, hi = sc.y;
+    while (lo < hi) {
+      uint32_t mid = (lo + hi) >> 1;
+      if (vals[mid] <= c)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    const uint32_t pos_p_in_c = sc.y - lo;
+    const uint32_t dp = deg[p], dc = deg[c];
+    const uint32_t id_up = xadj[c] + pos_p_in_c;
+    const uint32_t id_down = xadj[p] + pos_c_in_p;
+    // succ of (c, p): (p, nbr_p[(pos_c_in_p + 1) mod deg p]), or p's dummy
+    uint32_t k = (pos_c_in_p + 1) % dp;
+    tour[id_up] = (proot && k == 0) ? (uint64_t)num_edges + didx[p] : (uint64_t)xadj[p] + k;
+    // succ of (p, c): (c, nbr_c[(pos_p_in_c + 1) mod deg c])
+    k = (pos_p_in_c + 1) % dc;
+    tour[id_down] = (uint64_t)xadj[c] + k;
+  }
+}
+
+kascade_status sort_children(kascade_ctx& ctx, const uint64_t* parent, uint32_t n, uint32_t** keys, uint32_t** vals,
+                             uint2** seg, cudaStream_t s) {
+  SortSource src;
+  src.parent = parent;
+  KS_TRY(radix_sort_pairs(ctx, src, n, bits_for(n), keys, vals, s));
+  *seg = alloc<uint2>(ctx, n);
+  if (!*seg) return KASCADE_ERR_OOM;
+  KS_CUDA(cudaMemsetAsync(*seg, 0, sizeof(uint2) * (size_t)n, s));
+  ProfScope ps(ctx, "seg_bounds", s);
+  k_seg_bounds<<<grid_for(ctx, n, 256, 8), 256, 0, s>>>(*keys, n, *seg);
+  KS_CHECK_LAUNCH();
+  return KASCADE_OK;
+}
+
+}  // namespace
+
+kascade_status root_forest_impl(kascade_ctx& ctx, const uint64_t* parent, uint32_t n, uint64_t* root_out,
+                                uint64_t* depth_out, int keep_roots, const Params& p, cudaStream_t s) {
+  if (n == 0) return KASCADE_OK;
+  uint32_t *keys, *vals;
+  uint2* seg;
+  KS_TRY(sort_children(ctx, parent, n, &keys, &vals, &seg, s));
+  const uint32_t m = 2 * n;
+  Rec* rec = alloc<Rec>(ctx, m);
+  uint32_t* ruler_elem = alloc<uint32_t>(ctx, m);
+  uint32_t* ctr = alloc<uint32_t>(ctx, 1);
+  if (!rec || !ruler_elem || !ctr) return KASCADE_ERR_OOM;
+  KS_CUDA(cudaMemsetAsync(ctr, 0, sizeof(uint32_t), s));
+  {
+    ProfScope ps(ctx, "tour_build", s);
+    const unsigned grid = grid_for(ctx, ((uint64_t)n + 256 * TB_ITEMS - 1) / (256 * TB_ITEMS) * 256, 256, 8);
+    k_tour_build<<<grid, 256, 0, s>>>(keys, vals, n, seg, rec, ruler_elem, ctr, mix32(p.seed ^ 0x70757254u),
+                                      (uint32_t)(4294967296.0 / (double)(p.spacing0 < 2 ? 2 : p.spacing0)),
+                                      ctx.d_status);
+    KS_CHECK_LAUNCH();
+  }
+  uint32_t r = 0;
+  KS_TRY(read_u32(ctx, ctr, &r, s));
+  SinkTour sink{root_out, depth_out, n, keep_roots};
+  return rank_records(ctx, rec, m, r, ruler_elem, sink, p, s);
+}
+
+kascade_status compute_euler_tour_impl(kascade_ctx& ctx, const uint64_t* parent, uint32_t n, uint64_t* tour,
+                                       uint64_t* m_out, cudaStream_t s) {
+  *m_out = 0;
+  if (n == 0) return KASCADE_OK;
+  uint32_t *keys, *vals;
+  uint2* seg;
+  KS_TRY(sort_children(ctx, parent, n, &keys, &vals, &seg, s));
+  uint32_t* deg = alloc<uint32_t>(ctx, n);
+  uint32_t* droot = alloc<uint32_t>(ctx, n);
+  uint32_t* xadj = alloc<uint32_t>(ctx, n);
+  uint32_t* tot = alloc<uint32_t>(ctx, 2);
+  if (!deg || !droot || !xadj || !tot) return KASCADE_ERR_OOM;
+  const unsigned grid = grid_for(ctx, n, 256, 8);
+  k_ref_degrees<<<grid, 256, 0, s>>>(parent, n, seg, deg, droot);
+  KS_CHECK_LAUNCH();
+  KS_TRY(exclusive_scan_u32(ctx, deg, xadj, n, tot, s));
+  KS_TRY(exclusive_scan_u32(ctx, droot, droot, n, tot + 1, s));
+  uint32_t num_edges = 0;
+  KS_TRY(read_u32(ctx, tot, &num_edges, s));
+  // m = num_edges + #roots; #roots = n - num_edges / 2
+  const uint64_t roots = (uint64_t)n - num_edges / 2;
+  const uint64_t m = (uint64_t)num_edges + roots;
+  k_iota64<<<grid_for(ctx, m, 256, 8), 256, 0, s>>>(tour, m);
+  KS_CHECK_LAUNCH();
+  {
+    ProfScope ps(ctx, "ref_tour", s);
+    k_ref_tour<<<grid, 256, 0, s>>>(parent, keys, vals, n, seg, deg, xadj, droot, num_edges, tour);
+    KS_CHECK_LAUNCH();
+  }
+  *m_out = m;
+  return KASCADE_OK;
+}
+
+}  // namespace ks

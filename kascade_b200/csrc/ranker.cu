@@ -1,0 +1,720 @@
+// Ruling-set list ranker and pointer doubling for one B200.
+//
+// Reference counterparts (niklas-uhl/kascade):
+//   ruler sampling      lib/kascade/sparse_ruling_set_detail/ruler_selection.hpp:18-115,
+//                       sparse_ruling_set.cpp:106-136 (shuffled candidates) -> here a
+//                       counter hash of the index, plus every root
+//   ruler chasing       sparse_ruling_set.cpp:147-273 (init / work_on_item) and
+//                       ruler_chasing_engine.hpp:57-101 (sync rounds) -> one
+//                       persistent kernel, every hop a dependent 16 B load
+//   unreached fix-up    post_invert.hpp:195-264 -> elements ahead of their list's
+//                       first ruler walk forward during propagation
+//   pack / recursion    pack.hpp:23-79, sparse_ruling_set.cpp:291-310, 376-392
+//                       -> the chase writes the ruler sub-list directly in
+//                       dense ruler-id space
+//   propagation (pull)  ruler_propagation.hpp:148-256 -> one coalesced pass
+//   pointer doubling    pointer_doubling_generic.hpp:43-60, 171-212, 418-438,
+//                       609-700 -> double-buffered jump kernel
+#include <cstdio>
+
+#include "ranker.cuh"
+
+namespace ks {
+
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int PREP_ITEMS = 8;
+constexpr int PROP_ITEMS = 4;
+constexpr int BASE_THREADS = 1024;
+constexpr int BASE_PER_THREAD = 8;  // base_max <= BASE_THREADS * BASE_PER_THREAD
+
+struct WUnit {
+  __device__ __forceinline__ uint64_t operator()(uint64_t) const { return 1ull; }
+};
+struct WU32 {
+  const uint32_t* p;
+  __device__ __forceinline__ uint64_t operator()(uint64_t x) const { return (uint64_t)__ldcs(p + x); }
+};
+struct WI64 {
+  const int64_t* p;
+  __device__ __forceinline__ uint64_t operator()(uint64_t x) const {
+    return (uint64_t)__ldcs(reinterpret_cast<const long long*>(p) + x);
+  }
+};
+
+inline uint32_t thresh_for(uint32_t spacing) {
+  if (spacing <= 1) return 0xFFFFFFFFu;
+  double t = 4294967296.0 / (double)spacing;
+  return t >= 4294967295.0 ? 0xFFFFFFFFu : (uint32_t)t;
+}
+inline uint32_t salt_for(uint32_t seed, int level) { return mix32(seed + 0x9E3779B9u * (uint32_t)(level + 1)); }
+
+// ---------------------------------------------------------------------------
+// prepare: build records, sample rulers (every root is a ruler), number them.
+// One atomicAdd per 2048-element tile hands out dense ruler ids.
+// ---------------------------------------------------------------------------
+template <class W>
+__global__ void __launch_bounds__(256) k_prepare_arrays(const uint64_t* __restrict__ succ, W w, uint32_t n,
+                                                        Rec* __restrict__ rec, uint32_t* __restrict__ ruler_elem,
+                                                        uint32_t* __restrict__ counter, uint32_t salt,
+                                                        uint32_t thresh, DevStatus* st) {
+  __shared__ uint32_t sm[33];
+  __shared__ uint32_t sbase;
+  const uint64_t tile_sz = (uint64_t)blockDim.x * PREP_ITEMS;
+  for (uint64_t tile = (uint64_t)blockIdx.x * tile_sz; tile < n; tile += (uint64_t)gridDim.x * tile_sz) {
+    uint32_t sv[PREP_ITEMS];
+    uint64_t wv[PREP_ITEMS];
+    uint32_t rl = 0, cnt = 0;
+#pragma unroll
+    for (int i = 0; i < PREP_ITEMS; ++i) {
+      uint64_t x = tile + (uint64_t)i * blockDim.x + threadIdx.x;
+      sv[i] = 0;
+      wv[i] = 0;
+      if (x < n) {
+        unsigned long long s = __ldcs(reinterpret_cast<const unsigned long long*>(succ) + x);
+        if (s >= n) {
+          set_error(st, KASCADE_ERR_OUT_OF_RANGE, x);
+          s = x;
+        }
+        sv[i] = (uint32_t)s;
+        wv[i] = w(x);
+        if (s == x || sampled((uint32_t)x, salt, thresh)) {
+          rl |= 1u << i;
+          cnt++;
+        }
+      }
+    }
+    uint32_t total;
+    uint32_t pre = block_exclusive_scan(cnt, sm, &total);
+    if (threadIdx.x == 0) {
+      uint32_t b = total ? atomicAdd(counter, total) : 0u;
+      if ((uint64_t)b + total > MAX_RULERS) set_error(st, KASCADE_ERR_TOO_LARGE, b);
+      sbase = b;
+    }
+    __syncthreads();
+    uint32_t id = sbase + pre;
+#pragma unroll
+    for (int i = 0; i < PREP_ITEMS; ++i) {
+      uint64_t x = tile + (uint64_t)i * blockDim.x + threadIdx.x;
+      if (x < n) {
+        Rec r;
+        r.a = wv[i];
+        r.b = sv[i];
+        r.c = TAG_UNREACHED;
+        if (rl & (1u << i)) {
+          if (id < MAX_RULERS) {
+            r.c = TAG_RULER | id;
+            ruler_elem[id] = (uint32_t)x;
+          }
+          id++;
+        }
+        rec[x] = r;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Deeper levels: the chase of the level above wrote the records (tag
+// unreached); sample rulers in place and record each ruler's level-0 index.
+__global__ void __launch_bounds__(256) k_prepare_level(Rec* __restrict__ rec, uint32_t n,
+                                                       const uint32_t* __restrict__ elem0,
+                                                       uint32_t* __restrict__ ruler_elem,
+                                                       uint32_t* __restrict__ elem0_next,
+                                                       uint32_t* __restrict__ counter, uint32_t salt,
+                                                       uint32_t thresh, DevStatus* st) {
+  __shared__ uint32_t sm[33];
+  __shared__ uint32_t sbase;
+  const uint64_t tile_sz = (uint64_t)blockDim.x * PREP_ITEMS;
+  for (uint64_t tile = (uint64_t)blockIdx.x * tile_sz; tile < n; tile += (uint64_t)gridDim.x * tile_sz) {
+    Rec rv[PREP_ITEMS];
+    uint32_t rl = 0, cnt = 0;
+#pragma unroll
+    for (int i = 0; i < PREP_ITEMS; ++i) {
+      uint64_t x = tile + (uint64_t)i * blockDim.x + threadIdx.x;
+      if (x < n) {
+        rv[i] = rec[x];
+        if (rv[i].b == (uint32_t)x || sampled((uint32_t)x, salt, thresh)) {
+          rl |= 1u << i;
+          cnt++;
+        }
+      }
+    }
+    uint32_t total;
+    uint32_t pre = block_exclusive_scan(cnt, sm, &total);
+    if (threadIdx.x == 0) sbase = total ? atomicAdd(counter, total) : 0u;
+    __syncthreads();
+    uint32_t id = sbase + pre;
+#pragma unroll
+    for (int i = 0; i < PREP_ITEMS; ++i) {
+      uint64_t x = tile + (uint64_t)i * blockDim.x + threadIdx.x;
+      if (x < n) {
+        Rec r = rv[i];
+        r.c = TAG_UNREACHED;
+        if (rl & (1u << i)) {
+          r.c = TAG_RULER | id;
+          ruler_elem[id] = (uint32_t)x;
+          elem0_next[id] = elem0 ? elem0[x] : (uint32_t)x;
+          id++;
+        }
+        rec[x] = r;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// chase: persistent, C chains in flight per thread, rulers handed out to each
+// warp in batches of 32*C from one global counter.  A hop reads the 16 B
+// record of the next element; an unreached element is stamped with
+// (distance from ruler, ruler id) in the same record.  A chain ends at the
+// next ruler (or root) and writes its ruler's sub-list record:
+// (weight = distance to that ruler, successor = that ruler's id).
+// ---------------------------------------------------------------------------
+template <int C>
+__global__ void __launch_bounds__(256) k_chase(Rec* __restrict__ rec, uint32_t n,
+                                               const uint32_t* __restrict__ ruler_elem, uint32_t r,
+                                               Rec* __restrict__ rec_next, uint32_t* __restrict__ work,
+                                               DevStatus* st) {
+  constexpr uint32_t BATCH = 32u * C;
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t lt = lanemask_lt();
+  uint32_t cid[C], cx[C], hops[C];
+  uint64_t acc[C];
+  uint32_t act = 0;
+  uint32_t q_base = 0, q_left = 0;  // warp-uniform local batch of ruler ids
+  bool drained = false;             // warp-uniform
+#pragma unroll
+  for (int c = 0; c < C; ++c) {
+    cid[c] = cx[c] = hops[c] = 0;
+    acc[c] = 0;
+  }
+  while (true) {
+    if (!drained) {
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        bool need = !(act & (1u << c));
+        uint32_t m = __ballot_sync(FULL, need);
+        while (m != 0u && !drained) {
+          if (q_left == 0u) {
+            uint32_t b = 0;
+            if (lane == 0) b = atomicAdd(work, BATCH);
+            b = __shfl_sync(FULL, b, 0);
+            if (b >= r) {
+              drained = true;
+              break;
+            }
+            q_base = b;
+            q_left = min(BATCH, r - b);
+          }
+          const uint32_t take = min((uint32_t)__popc(m), q_left);
+          const uint32_t my_rank = __popc(m & lt);
+          const bool mine = need && my_rank < take;
+          if (mine) {
+            const uint32_t id = q_base + my_rank;
+            const uint32_t x0 = __ldg(ruler_elem + id);
+            const Rec r0 = ld_rec_cg(rec + x0);
+            if (r0.b == x0) {
+              Rec o;
+              o.a = 0;
+              o.b = id;
+              o.c = TAG_UNREACHED;
+              st_rec_cg(rec_next + id, o);
+            } else {
+              cid[c] = id;
+              cx[c] = r0.b;
+              acc[c] = r0.a;
+              hops[c] = 0;
+              act |= 1u << c;
+            }
+          }
+          const uint32_t served = __ballot_sync(FULL, mine);
+          m &= ~served;
+          need = need && !mine;
+          q_base += take;
+          q_left -= take;
+        }
+      }
+    }
+    if (!__any_sync(FULL, act != 0u)) {
+      if (drained) break;
+      continue;
+    }
+    Rec rr[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c)
+      if (act & (1u << c)) rr[c] = ld_rec_cg(rec + cx[c]);
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      if (!(act & (1u << c))) continue;
+      const uint32_t tg = rr[c].c;
+      if (tag_unreached(tg)) {
+        Rec wv;
+        wv.a = acc[c];
+        wv.b = rr[c].b;
+        wv.c = cid[c];
+        st_rec_cg(rec + cx[c], wv);
+        acc[c] += rr[c].a;
+        cx[c] = rr[c].b;
+        if (++hops[c] > n) {
+          set_error(st, KASCADE_ERR_CYCLE, cid[c]);
+          act &= ~(1u << c);
+        }
+      } else if (tag_ruler(tg)) {
+        Rec o;
+        o.a = acc[c];
+        o.b = tag_id(tg);
+        o.c = TAG_UNREACHED;
+        st_rec_cg(rec_next + cid[c], o);
+        act &= ~(1u << c);
+      } else {
+        // already stamped by another chase: two predecessors
+        set_error(st, KASCADE_ERR_NOT_A_LIST, cx[c]);
+        act &= ~(1u << c);
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// propagate: rank(x) = rank(ruler) - distance(ruler, x); elements no chase
+// reached (ahead of their list's first ruler) walk forward to the first
+// stamped element and add the weights they pass.
+// ---------------------------------------------------------------------------
+template <class Sink>
+__global__ void __launch_bounds__(256) k_propagate(const Rec* __restrict__ rec, uint32_t n_out, uint32_t n_all,
+                                                   const Out* __restrict__ out_next, Sink sink, DevStatus* st) {
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x * PROP_ITEMS + threadIdx.x; base < n_out;
+       base += (uint64_t)stride * PROP_ITEMS) {
+    Rec rv[PROP_ITEMS];
+#pragma unroll
+    for (int i = 0; i < PROP_ITEMS; ++i) {
+      uint64_t x = base + (uint64_t)i * blockDim.x;
+      if (x < n_out) rv[i] = ld_rec_cs(rec + x);
+    }
+#pragma unroll
+    for (int i = 0; i < PROP_ITEMS; ++i) {
+      uint64_t x = base + (uint64_t)i * blockDim.x;
+      if (x >= n_out) continue;
+      Rec r = rv[i];
+      bool is_root = false;
+      uint64_t acc = 0;
+      if (tag_unreached(r.c)) {
+        // Brent's cycle detection keeps an invalid (rootless, ruler-free)
+        // cycle to O(cycle length) steps instead of n per element.
+        uint32_t hops = 0, lam = 0, power = 1, mark = (uint32_t)x;
+        bool cyc = false;
+        while (tag_unreached(r.c)) {
+          acc += r.a;
+          const uint32_t y = r.b;
+          if (y == mark || ++hops > n_all) {
+            cyc = true;
+            break;
+          }
+          if (++lam == power) {
+            mark = y;
+            power <<= 1;
+            lam = 0;
+          }
+          r = ld_rec_cg(rec + y);
+        }
+        if (cyc) {
+          set_error(st, KASCADE_ERR_CYCLE, x);
+          continue;
+        }
+      } else if (tag_ruler(r.c)) {
+        is_root = (r.b == (uint32_t)x);
+      }
+      uint64_t rank;
+      uint32_t root;
+      if (tag_ruler(r.c)) {
+        Out o = ld_out(out_next + tag_id(r.c));
+        rank = o.rank + acc;
+        root = o.root;
+      } else {
+        Out o = ld_out(out_next + r.c);
+        rank = o.rank - r.a + acc;
+        root = o.root;
+      }
+      sink.put((uint32_t)x, rank, root, is_root);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// base case: one CTA, Wyllie pointer jumping in shared memory.
+// ---------------------------------------------------------------------------
+template <class Sink>
+__global__ void __launch_bounds__(BASE_THREADS) k_base(const Rec* __restrict__ rec, uint32_t n,
+                                                       const uint32_t* __restrict__ elem0, Sink sink,
+                                                       DevStatus* st) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  uint64_t* rk = reinterpret_cast<uint64_t*>(smem);
+  uint32_t* sc = reinterpret_cast<uint32_t*>(smem + 8ull * n);
+  uint8_t* isroot = smem + 12ull * n;
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+    Rec r = rec[i];
+    bool root = (r.b == i);
+    sc[i] = r.b;
+    rk[i] = root ? 0ull : r.a;
+    isroot[i] = root ? 1 : 0;
+  }
+  __syncthreads();
+  int round = 0;
+  while (true) {
+    uint32_t ns[BASE_PER_THREAD];
+    uint64_t nr[BASE_PER_THREAD];
+    int changed = 0;
+#pragma unroll
+    for (int j = 0; j < BASE_PER_THREAD; ++j) {
+      uint32_t i = threadIdx.x + j * blockDim.x;
+      if (i < n) {
+        uint32_t s = sc[i];
+        if (!isroot[s]) {
+          ns[j] = sc[s];
+          nr[j] = rk[i] + rk[s];
+          changed = 1;
+        } else {
+          ns[j] = s;
+          nr[j] = rk[i];
+        }
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < BASE_PER_THREAD; ++j) {
+      uint32_t i = threadIdx.x + j * blockDim.x;
+      if (i < n) {
+        sc[i] = ns[j];
+        rk[i] = nr[j];
+      }
+    }
+    if (!__syncthreads_or(changed)) break;
+    if (++round > 40) {
+      if (threadIdx.x == 0) set_error(st, KASCADE_ERR_CYCLE, 0);
+      break;
+    }
+  }
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+    uint32_t rt = sc[i];
+    if (elem0) rt = elem0[rt];
+    sink.put(i, rk[i], rt, isroot[i] != 0);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// pointer doubling: double-buffered jump rounds over 16 B records.
+// done bit 0: successor is a root; bit 1: the element is a root.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_pd_init(const Rec* __restrict__ rec, uint32_t n, PdRec* __restrict__ a) {
+  for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; x < n; x += (uint64_t)gridDim.x * blockDim.x) {
+    Rec r = rec[x];
+    bool root = (r.b == (uint32_t)x);
+    PdRec p;
+    p.rank = root ? 0ull : r.a;
+    p.succ = r.b;
+    p.done = root ? 3u : 0u;
+    a[x] = p;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_pd_round(const PdRec* __restrict__ a, PdRec* __restrict__ b, uint32_t n,
+                                                  uint32_t* __restrict__ active) {
+  uint32_t cnt = 0;
+  for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; x < n; x += (uint64_t)gridDim.x * blockDim.x) {
+    PdRec e = a[x];
+    if (!(e.done & 1u)) {
+      PdRec t = a[e.succ];
+      e.rank += t.rank;
+      e.succ = t.succ;
+      e.done = t.done & 1u;
+      cnt += (e.done & 1u) ? 0u : 1u;
+    }
+    b[x] = e;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(FULL, cnt, o);
+  if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(active, cnt);
+}
+
+template <class Sink>
+__global__ void __launch_bounds__(256) k_pd_final(const PdRec* __restrict__ a, uint32_t n,
+                                                  const uint32_t* __restrict__ elem0, Sink sink) {
+  for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; x < n; x += (uint64_t)gridDim.x * blockDim.x) {
+    PdRec e = a[x];
+    uint32_t rt = e.succ;
+    if (elem0) rt = elem0[rt];
+    sink.put((uint32_t)x, e.rank, rt, (e.done & 2u) != 0u);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// is_list: count predecessors.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_count_preds(const uint64_t* __restrict__ succ, uint64_t n,
+                                                     uint32_t* __restrict__ cnt, uint32_t* __restrict__ bad) {
+  for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; x < n; x += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t s = succ[x];
+    if (s >= n) {
+      atomicOr(bad, 2u);
+      continue;
+    }
+    if (s == x) continue;
+    if (atomicAdd(cnt + s, 1u) >= 1u) atomicOr(bad, 1u);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host-side launch helpers
+// ---------------------------------------------------------------------------
+template <class K>
+int occupancy(K kernel, int block, size_t smem) {
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, block, smem) != cudaSuccess) {
+    cudaGetLastError();
+    nb = 1;
+  }
+  return nb < 1 ? 1 : nb;
+}
+
+template <int C>
+kascade_status launch_chase_c(kascade_ctx& ctx, Rec* rec, uint32_t n, const uint32_t* ruler_elem, uint32_t r,
+                              Rec* rec_next, uint32_t* work, cudaStream_t s) {
+  static int occ = -1;
+  if (occ < 0) occ = occupancy(k_chase<C>, 256, 0);
+  unsigned grid = (unsigned)(ctx.sm_count * occ);
+  uint64_t need = ((uint64_t)r + 32ull * C - 1) / (32ull * C);  // warps worth of work
+  uint64_t need_blocks = (need + 7) / 8;
+  if (need_blocks < grid) grid = (unsigned)(need_blocks ? need_blocks : 1);
+  ProfScope ps(ctx, "chase", s);
+  k_chase<C><<<grid, 256, 0, s>>>(rec, n, ruler_elem, r, rec_next, work, ctx.d_status);
+  KS_CHECK_LAUNCH();
+  return KASCADE_OK;
+}
+
+kascade_status launch_chase(kascade_ctx& ctx, Rec* rec, uint32_t n, const uint32_t* ruler_elem, uint32_t r,
+                            Rec* rec_next, const Params& p, cudaStream_t s) {
+  uint32_t* work = alloc<uint32_t>(ctx, 1);
+  if (!work) return KASCADE_ERR_OOM;
+  KS_CUDA(cudaMemsetAsync(work, 0, sizeof(uint32_t), s));
+  switch (p.chains) {
+    case 1:
+      return launch_chase_c<1>(ctx, rec, n, ruler_elem, r, rec_next, work, s);
+    case 4:
+      return launch_chase_c<4>(ctx, rec, n, ruler_elem, r, rec_next, work, s);
+    default:
+      return launch_chase_c<2>(ctx, rec, n, ruler_elem, r, rec_next, work, s);
+  }
+}
+
+template <class Sink>
+kascade_status launch_propagate(kascade_ctx& ctx, const Rec* rec, uint32_t n_out, uint32_t n_all, const Out* out_next,
+                                const Sink& sink, cudaStream_t s) {
+  unsigned grid = grid_for(ctx, ((uint64_t)n_out + PROP_ITEMS - 1) / PROP_ITEMS, 256, 8);
+  ProfScope ps(ctx, "propagate", s);
+  k_propagate<Sink><<<grid, 256, 0, s>>>(rec, n_out, n_all, out_next, sink, ctx.d_status);
+  KS_CHECK_LAUNCH();
+  return KASCADE_OK;
+}
+
+template <class Sink>
+kascade_status launch_base(kascade_ctx& ctx, const Rec* rec, uint32_t n, const uint32_t* elem0, const Sink& sink,
+                           cudaStream_t s) {
+  if (n == 0) return KASCADE_OK;
+  size_t smem = 13ull * n + 16;
+  static bool configured = false;
+  if (!configured) {
+    KS_CUDA(cudaFuncSetAttribute(k_base<Sink>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(13 * BASE_THREADS * BASE_PER_THREAD + 16)));
+    configured = true;
+  }
+  ProfScope ps(ctx, "base_case", s);
+  k_base<Sink><<<1, BASE_THREADS, smem, s>>>(rec, n, elem0, sink, ctx.d_status);
+  KS_CHECK_LAUNCH();
+  return KASCADE_OK;
+}
+
+kascade_status rank_deep(kascade_ctx& ctx, Rec* rec, uint32_t n, const uint32_t* elem0, const SinkOut& sink,
+                         int level, const Params& p, cudaStream_t s);
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Public (library-internal) entry points
+// ---------------------------------------------------------------------------
+Params make_params(const kascade_ctx& ctx, const kascade_opts* o, uint64_t n) {
+  (void)ctx;
+  Params p;
+  // Spacing trades chase critical path (~ spacing * ln(n/spacing) hops)
+  // against ruler-table size; these defaults are the tuned values for
+  // random lists on B200 (see the autotune table in the batch path).
+  if (n <= (1u << 16)) p.spacing0 = 16;
+  else if (n <= (1u << 22)) p.spacing0 = 32;
+  else p.spacing0 = 48;
+  if (o) {
+    if (o->ruler_spacing) p.spacing0 = o->ruler_spacing;
+    if (o->ruler_spacing_deep) p.spacing_deep = o->ruler_spacing_deep;
+    if (o->max_levels) p.max_levels = o->max_levels;
+    if (o->base_case_size) p.base_max = o->base_case_size;
+    if (o->chains_per_thread) p.chains = o->chains_per_thread;
+    if (o->block_size) p.block = o->block_size;
+    if (o->seed) p.seed = o->seed;
+    p.algorithm = o->algorithm;
+  }
+  if (p.base_max > (uint32_t)(BASE_THREADS * BASE_PER_THREAD)) p.base_max = BASE_THREADS * BASE_PER_THREAD;
+  if (p.spacing0 < 2) p.spacing0 = 2;
+  if (p.spacing_deep < 2) p.spacing_deep = 2;
+  return p;
+}
+
+kascade_status prepare_arrays(kascade_ctx& ctx, const uint64_t* succ, WKind wk, const void* w, uint32_t n, Rec* rec,
+                              uint32_t* ruler_elem, uint32_t* r_out, const Params& p, cudaStream_t s) {
+  uint32_t* ctr = alloc<uint32_t>(ctx, 1);
+  if (!ctr) return KASCADE_ERR_OOM;
+  KS_CUDA(cudaMemsetAsync(ctr, 0, sizeof(uint32_t), s));
+  unsigned grid = grid_for(ctx, ((uint64_t)n + 256 * PREP_ITEMS - 1) / (256 * PREP_ITEMS) * 256, 256, 8);
+  uint32_t salt = salt_for(p.seed, 0), th = thresh_for(p.spacing0);
+  {
+    ProfScope ps(ctx, "prepare", s);
+    switch (wk) {
+      case WKind::Unit:
+        k_prepare_arrays<WUnit><<<grid, 256, 0, s>>>(succ, WUnit{}, n, rec, ruler_elem, ctr, salt, th, ctx.d_status);
+        break;
+      case WKind::U32:
+        k_prepare_arrays<WU32><<<grid, 256, 0, s>>>(succ, WU32{(const uint32_t*)w}, n, rec, ruler_elem, ctr, salt, th,
+                                                    ctx.d_status);
+        break;
+      case WKind::I64:
+        k_prepare_arrays<WI64><<<grid, 256, 0, s>>>(succ, WI64{(const int64_t*)w}, n, rec, ruler_elem, ctr, salt, th,
+                                                    ctx.d_status);
+        break;
+    }
+    KS_CHECK_LAUNCH();
+  }
+  return read_u32(ctx, ctr, r_out, s);
+}
+
+template <class Sink>
+kascade_status pointer_double_records(kascade_ctx& ctx, const Rec* rec, uint32_t n, const uint32_t* elem0,
+                                      const Sink& sink, cudaStream_t s) {
+  if (n == 0) return KASCADE_OK;
+  PdRec* a = alloc<PdRec>(ctx, n);
+  PdRec* b = alloc<PdRec>(ctx, n);
+  uint32_t* active = alloc<uint32_t>(ctx, 1);
+  if (!a || !b || !active) return KASCADE_ERR_OOM;
+  unsigned grid = grid_for(ctx, n, 256, 8);
+  {
+    ProfScope ps(ctx, "pd_init", s);
+    k_pd_init<<<grid, 256, 0, s>>>(rec, n, a);
+    KS_CHECK_LAUNCH();
+  }
+  int rounds = 0;
+  while (true) {
+    KS_CUDA(cudaMemsetAsync(active, 0, sizeof(uint32_t), s));
+    {
+      ProfScope ps(ctx, "pd_round", s);
+      k_pd_round<<<grid, 256, 0, s>>>(a, b, n, active);
+      KS_CHECK_LAUNCH();
+    }
+    PdRec* t = a;
+    a = b;
+    b = t;
+    uint32_t left = 0;
+    KS_TRY(read_u32(ctx, active, &left, s));
+    if (left == 0) break;
+    if (++rounds > 64) {
+      ctx.error_info = left;
+      return KASCADE_ERR_CYCLE;
+    }
+  }
+  {
+    ProfScope ps(ctx, "pd_final", s);
+    k_pd_final<Sink><<<grid, 256, 0, s>>>(a, n, elem0, sink);
+    KS_CHECK_LAUNCH();
+  }
+  return KASCADE_OK;
+}
+
+namespace {
+
+kascade_status rank_deep(kascade_ctx& ctx, Rec* rec, uint32_t n, const uint32_t* elem0, const SinkOut& sink,
+                         int level, const Params& p, cudaStream_t s) {
+  ctx.last_levels.push_back(n);
+  if (n <= p.base_max) return launch_base(ctx, rec, n, elem0, sink, s);
+  uint32_t* ruler_elem = alloc<uint32_t>(ctx, n);
+  uint32_t* elem0_next = alloc<uint32_t>(ctx, n);
+  uint32_t* ctr = alloc<uint32_t>(ctx, 1);
+  if (!ruler_elem || !elem0_next || !ctr) return KASCADE_ERR_OOM;
+  KS_CUDA(cudaMemsetAsync(ctr, 0, sizeof(uint32_t), s));
+  unsigned grid = grid_for(ctx, ((uint64_t)n + 256 * PREP_ITEMS - 1) / (256 * PREP_ITEMS) * 256, 256, 8);
+  {
+    ProfScope ps(ctx, "prepare_level", s);
+    k_prepare_level<<<grid, 256, 0, s>>>(rec, n, elem0, ruler_elem, elem0_next, ctr, salt_for(p.seed, level),
+                                         thresh_for(p.spacing_deep), ctx.d_status);
+    KS_CHECK_LAUNCH();
+  }
+  uint32_t r = 0;
+  KS_TRY(read_u32(ctx, ctr, &r, s));
+  if ((uint32_t)level >= p.max_levels || (uint64_t)r * 10 > (uint64_t)n * 7)
+    return pointer_double_records(ctx, rec, n, elem0, sink, s);
+  Rec* rec_next = alloc<Rec>(ctx, r);
+  Out* out_next = alloc<Out>(ctx, r);
+  if (!rec_next || !out_next) return KASCADE_ERR_OOM;
+  KS_TRY(launch_chase(ctx, rec, n, ruler_elem, r, rec_next, p, s));
+  KS_TRY(rank_deep(ctx, rec_next, r, elem0_next, SinkOut{out_next}, level + 1, p, s));
+  return launch_propagate(ctx, rec, n, n, out_next, sink, s);
+}
+
+}  // namespace
+
+template <class Sink>
+kascade_status rank_records(kascade_ctx& ctx, Rec* rec, uint32_t n, uint32_t r0, uint32_t* ruler_elem0,
+                            const Sink& sink, const Params& p, cudaStream_t s) {
+  ctx.last_levels.clear();
+  ctx.last_levels.push_back(n);
+  if (n == 0) return KASCADE_OK;
+  if (n <= p.base_max) return launch_base(ctx, rec, n, nullptr, sink, s);
+  if (p.algorithm != KASCADE_ALGO_SPARSE_RULING_SET || p.max_levels == 0 || (uint64_t)r0 * 10 > (uint64_t)n * 7)
+    return pointer_double_records(ctx, rec, n, nullptr, sink, s);
+  Rec* rec1 = alloc<Rec>(ctx, r0);
+  Out* out1 = alloc<Out>(ctx, r0);
+  if (!rec1 || !out1) return KASCADE_ERR_OOM;
+  KS_TRY(launch_chase(ctx, rec, n, ruler_elem0, r0, rec1, p, s));
+  // level-1 elements are level-0 rulers: their level-0 index is ruler_elem0
+  KS_TRY(rank_deep(ctx, rec1, r0, ruler_elem0, SinkOut{out1}, 1, p, s));
+  return launch_propagate(ctx, rec, sink.limit(n), n, out1, sink, s);
+}
+
+kascade_status check_is_list(kascade_ctx& ctx, const uint64_t* succ, uint64_t n, int* ok, cudaStream_t s) {
+  uint32_t* cnt = alloc<uint32_t>(ctx, n);
+  uint32_t* bad = alloc<uint32_t>(ctx, 1);
+  if (!cnt || !bad) return KASCADE_ERR_OOM;
+  KS_CUDA(cudaMemsetAsync(cnt, 0, n * sizeof(uint32_t), s));
+  KS_CUDA(cudaMemsetAsync(bad, 0, sizeof(uint32_t), s));
+  unsigned grid = grid_for(ctx, n, 256, 8);
+  {
+    ProfScope ps(ctx, "is_list", s);
+    k_count_preds<<<grid, 256, 0, s>>>(succ, n, cnt, bad);
+    KS_CHECK_LAUNCH();
+  }
+  uint32_t b = 0;
+  KS_TRY(read_u32(ctx, bad, &b, s));
+  if (b & 2u) return KASCADE_ERR_OUT_OF_RANGE;
+  *ok = (b & 1u) ? 0 : 1;
+  return KASCADE_OK;
+}
+
+// explicit instantiations for the level-0 sinks
+template kascade_status rank_records<SinkPlain>(kascade_ctx&, Rec*, uint32_t, uint32_t, uint32_t*, const SinkPlain&,
+                                                const Params&, cudaStream_t);
+template kascade_status rank_records<SinkTour>(kascade_ctx&, Rec*, uint32_t, uint32_t, uint32_t*, const SinkTour&,
+                                               const Params&, cudaStream_t);
+template kascade_status pointer_double_records<SinkPlain>(kascade_ctx&, const Rec*, uint32_t, const uint32_t*,
+                                                          const SinkPlain&, cudaStream_t);
+template kascade_status pointer_double_records<SinkTour>(kascade_ctx&, const Rec*, uint32_t, const uint32_t*,
+                                                         const SinkTour&, cudaStream_t);
+
+}  // namespace ks

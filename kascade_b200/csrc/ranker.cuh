@@ -1,0 +1,117 @@
+// Internal interface of the ruling-set list ranker.
+//
+// Pipeline for a list of n elements held as 16 B records (Rec):
+//   prepare   : counter-hash ruler sampling + ruler ids       (level 0 from the
+//               caller's arrays, deeper levels in place)
+//   chase     : every ruler walks its successors until the next ruler,
+//               stamping (ruler id, distance) into each record it passes and
+//               writing the ruler's sub-list record for the next level
+//   recurse   : the sub-list of rulers is ranked the same way, down to a
+//               one-CTA shared-memory base case (or pointer doubling when a
+//               level does not shrink)
+//   propagate : one coalesced pass: rank = rank(ruler) - distance, root =
+//               root(ruler); elements ahead of their list's first ruler walk
+//               forward to the first stamped element
+#pragma once
+
+#include "common.cuh"
+#include "ctx.cuh"
+
+namespace ks {
+
+struct Params {
+  uint32_t spacing0 = 48;      // mean elements per ruler, level 0
+  uint32_t spacing_deep = 24;  // mean elements per ruler, deeper levels
+  uint32_t max_levels = 6;
+  uint32_t base_max = 8192;    // one-CTA base case bound
+  uint32_t chains = 2;         // chains in flight per thread (1, 2 or 4)
+  uint32_t block = 256;
+  uint32_t seed = 0x6b617363u;
+  uint32_t algorithm = KASCADE_ALGO_SPARSE_RULING_SET;
+};
+
+Params make_params(const kascade_ctx& ctx, const kascade_opts* opts, uint64_t n);
+
+// Where results of level 0 go ------------------------------------------------
+// A sink receives, for element x, its rank, its root (level-0 index) and
+// whether x itself is a root.
+
+// Plain arrays. keep_roots: leave root entries untouched (the reference's
+// in-place contract); otherwise roots get (x, 0).
+struct SinkPlain {
+  uint64_t* root;
+  uint64_t* rank;
+  int keep_roots;
+  // elements [0, limit(n)) produce output
+  uint32_t limit(uint32_t n) const { return n; }
+  __device__ __forceinline__ void put(uint32_t x, uint64_t rk, uint32_t rt, bool is_root) const {
+    if (is_root) {
+      if (!keep_roots) {
+        __stcs(root + x, (unsigned long long)x);
+        __stcs(rank + x, 0ull);
+      }
+      return;
+    }
+    __stcs(root + x, (unsigned long long)rt);
+    __stcs(rank + x, (unsigned long long)rk);
+  }
+};
+
+// Euler tour: elements 0..nv-1 are the vertices' up edges (roots: the tour's
+// terminal element), so only those produce output.
+struct SinkTour {
+  uint64_t* root;
+  uint64_t* depth;
+  uint32_t nv;
+  int keep_roots;
+  uint32_t limit(uint32_t n) const { return n < nv ? n : nv; }
+  __device__ __forceinline__ void put(uint32_t x, uint64_t rk, uint32_t rt, bool is_root) const {
+    if (x >= nv) return;
+    if (is_root) {
+      if (!keep_roots) {
+        __stcs(root + x, (unsigned long long)x);
+        __stcs(depth + x, 0ull);
+      }
+      return;
+    }
+    __stcs(root + x, (unsigned long long)rt);
+    __stcs(depth + x, (unsigned long long)rk);
+  }
+};
+
+// Deeper levels write Out records.
+struct SinkOut {
+  Out* out;
+  uint32_t limit(uint32_t n) const { return n; }
+  __device__ __forceinline__ void put(uint32_t x, uint64_t rk, uint32_t rt, bool is_root) const {
+    st_out(out + x, is_root ? 0ull : rk, rt);
+  }
+};
+
+// Weight readers for building level-0 records.
+enum class WKind { Unit, U32, I64 };
+
+// Build level-0 records from (succ, weights), sample rulers and number them.
+// ruler_elem must hold n entries; *r_out receives the ruler count.
+kascade_status prepare_arrays(kascade_ctx& ctx, const uint64_t* succ, WKind wk, const void* w,
+                              uint32_t n, Rec* rec, uint32_t* ruler_elem, uint32_t* r_out,
+                              const Params& p, cudaStream_t s);
+
+// Rank level-0 records that carry ruler tags (r0 rulers, listed in
+// ruler_elem0) and deliver the results to the sink.
+template <class Sink>
+kascade_status rank_records(kascade_ctx& ctx, Rec* rec, uint32_t n, uint32_t r0,
+                            uint32_t* ruler_elem0, const Sink& sink, const Params& p,
+                            cudaStream_t s);
+
+// Pointer doubling on level-0 records (tags ignored).
+template <class Sink>
+kascade_status pointer_double_records(kascade_ctx& ctx, const Rec* rec, uint32_t n,
+                                      const uint32_t* elem0, const Sink& sink,
+                                      cudaStream_t s);
+
+// Validation: *ok = 1 if no element has two predecessors.
+kascade_status check_is_list(kascade_ctx& ctx, const uint64_t* succ, uint64_t n, int* ok,
+                             cudaStream_t s);
+
+}  // namespace ks

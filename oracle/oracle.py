@@ -1,0 +1,170 @@
+"""ctypes wrappers around the oracle shared libraries (test infrastructure)."""
+from __future__ import annotations
+
+import ctypes
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_SO = HERE / "_build" / "libkascade_oracle.so"
+REF_SO = HERE / "_ref" / "libkascade_ref.so"
+
+__all__ = [
+    "build", "has_ref", "rank_list", "root_forest", "local_pointer_chasing", "pointer_doubling",
+    "euler_tour", "rank_via_euler_tour", "is_list", "pack", "unpack", "gen_list", "gen_weights",
+    "gen_forest", "ref_gather_rank", "ref_local_pointer_chasing",
+]
+
+
+def build() -> None:
+    """Build the oracle (and oracle/_ref when the reference tree is present)."""
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True, capture_output=True)
+
+
+_lib = None
+_ref = None
+
+
+def _o():
+    global _lib
+    if _lib is None:
+        if not ORACLE_SO.exists():
+            build()
+        _lib = ctypes.CDLL(str(ORACLE_SO))
+    return _lib
+
+
+def has_ref() -> bool:
+    return REF_SO.exists()
+
+
+def _r():
+    global _ref
+    if _ref is None:
+        if not REF_SO.exists():
+            raise FileNotFoundError(f"{REF_SO} not built (reference source tree absent)")
+        _ref = ctypes.CDLL(str(REF_SO))
+    return _ref
+
+
+def _p(a: np.ndarray | None):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+U64 = ctypes.c_uint64
+U32 = ctypes.c_uint32
+
+
+def rank_list(succ: np.ndarray, weights: np.ndarray | None = None):
+    succ = np.ascontiguousarray(succ, np.uint64)
+    w = None if weights is None else np.ascontiguousarray(weights, np.uint32)
+    root = np.empty_like(succ)
+    rank = np.empty(succ.size, np.uint64)
+    rc = _o().oracle_rank_list(_p(succ), _p(w), U64(succ.size), _p(root), _p(rank))
+    if rc != 0:
+        raise ValueError("oracle: cycle without a root")
+    return root, rank
+
+
+def root_forest(parent: np.ndarray):
+    parent = np.ascontiguousarray(parent, np.uint64)
+    root = np.empty_like(parent)
+    depth = np.empty(parent.size, np.uint64)
+    rc = _o().oracle_root_forest(_p(parent), U64(parent.size), _p(root), _p(depth))
+    if rc != 0:
+        raise ValueError("oracle: cycle without a root")
+    return root, depth
+
+
+def local_pointer_chasing(succ: np.ndarray, rank: np.ndarray) -> None:
+    assert succ.dtype == np.uint64 and rank.dtype == np.int64
+    if _o().oracle_local_pointer_chasing(_p(succ), _p(rank), U64(succ.size)) != 0:
+        raise ValueError("oracle: cycle without a root")
+
+
+def pointer_doubling(succ: np.ndarray, rank: np.ndarray) -> int:
+    assert succ.dtype == np.uint64 and rank.dtype == np.int64
+    return _o().oracle_pointer_doubling(_p(succ), _p(rank), U64(succ.size))
+
+
+def euler_tour(parent: np.ndarray):
+    """The reference-numbered tour: (succ, weight, src, dst, is_up)."""
+    parent = np.ascontiguousarray(parent, np.uint64)
+    n = parent.size
+    lib = _o()
+    lib.oracle_euler_tour_size.restype = ctypes.c_uint64
+    m = int(lib.oracle_euler_tour_size(_p(parent), U64(n)))
+    ts = np.empty(max(m, 1), np.uint64)
+    tw = np.empty(max(m, 1), np.int64)
+    es = np.empty(max(m, 1), np.uint64)
+    ed = np.empty(max(m, 1), np.uint64)
+    up = np.empty(max(m, 1), np.uint8)
+    lib.oracle_euler_tour(_p(parent), U64(n), _p(ts), _p(tw), _p(es), _p(ed), _p(up))
+    return ts[:m], tw[:m], es[:m], ed[:m], up[:m].astype(bool)
+
+
+def rank_via_euler_tour(succ: np.ndarray, rank: np.ndarray) -> None:
+    assert succ.dtype == np.uint64 and rank.dtype == np.int64
+    if _o().oracle_rank_via_euler_tour(_p(succ), _p(rank), U64(succ.size)) != 0:
+        raise ValueError("oracle: cycle without a root")
+
+
+def is_list(succ: np.ndarray) -> bool:
+    succ = np.ascontiguousarray(succ, np.uint64)
+    return bool(_o().oracle_is_list(_p(succ), U64(succ.size)))
+
+
+def pack(succ: np.ndarray, rank: np.ndarray, active: np.ndarray):
+    succ = np.ascontiguousarray(succ, np.uint64)
+    rank = np.ascontiguousarray(rank, np.int64)
+    active = np.ascontiguousarray(active, np.uint64)
+    sp = np.empty(active.size, np.uint64)
+    rp = np.empty(active.size, np.int64)
+    rc = _o().oracle_pack(_p(succ), _p(rank), U64(succ.size), _p(active), U64(active.size), _p(sp), _p(rp))
+    if rc != 0:
+        raise ValueError("oracle: an active element's successor is not active")
+    return sp, rp
+
+
+def unpack(sp: np.ndarray, rp: np.ndarray, active: np.ndarray, succ: np.ndarray, rank: np.ndarray) -> None:
+    assert succ.dtype == np.uint64 and rank.dtype == np.int64
+    sp = np.ascontiguousarray(sp, np.uint64)  # keep the converted arrays alive
+    rp = np.ascontiguousarray(rp, np.int64)
+    active = np.ascontiguousarray(active, np.uint64)
+    _o().oracle_unpack(_p(sp), _p(rp), _p(active), U64(active.size), _p(succ), _p(rank))
+
+
+def gen_list(n: int, seed: int, layout: int = 0) -> np.ndarray:
+    out = np.empty(n, np.uint64)
+    _o().oracle_gen_list(U64(n), U64(seed), U32(layout), _p(out))
+    return out
+
+
+def gen_weights(n: int, seed: int, wbits: int = 16) -> np.ndarray:
+    out = np.empty(n, np.uint32)
+    _o().oracle_gen_weights(U64(n), U64(seed), U32(wbits), _p(out))
+    return out
+
+
+def gen_forest(n: int, seed: int, kind: int = 0, blocks: int = 64, spine: int = 0) -> np.ndarray:
+    out = np.empty(n, np.uint64)
+    _o().oracle_gen_forest(U64(n), U64(seed), U32(kind), U64(blocks), U64(spine), _p(out))
+    return out
+
+
+def ref_gather_rank(succ: np.ndarray):
+    """The reference's own GatherRank path (set_initial_ranking_state +
+    local_pointer_chasing from lib/kascade, compiled from source)."""
+    succ = np.ascontiguousarray(succ, np.uint64)
+    root = np.empty_like(succ)
+    rank = np.empty(succ.size, np.int64)
+    _r().ref_gather_rank(_p(succ), U64(succ.size), _p(root), _p(rank))
+    return root, rank
+
+
+def ref_local_pointer_chasing(succ: np.ndarray, rank: np.ndarray) -> None:
+    """In place, the reference's lib/kascade/local_pointer_chasing.cpp."""
+    assert succ.dtype == np.uint64 and rank.dtype == np.int64
+    _r().ref_local_pointer_chasing(_p(succ), _p(rank), U64(succ.size))

@@ -1,0 +1,108 @@
+"""Tree rooting (Euler tour + ranking) on the GPU against the oracle and the
+reference's own outputs."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from gpu_util import DEEP, SPARSE, dev64, host_i64, host_u64
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def kb():
+    import kascade_b200
+
+    return kascade_b200
+
+
+def _forests(oracle_mod):
+    rng = np.random.default_rng(5)
+    out = {
+        "rrt_64": oracle_mod.gen_forest(1 << 16, 1, 0, 64),
+        "rrt_1": oracle_mod.gen_forest(100_000, 2, 0, 1),
+        "cat": oracle_mod.gen_forest(1 << 17, 3, 1, 4, 1 << 14),
+        "path": np.maximum(np.arange(-1, 40_000), 0).astype(np.uint64),
+        "heap": np.maximum((np.arange(70_000) - 1) // 2, 0).astype(np.uint64),
+        "star": np.zeros(30_000, np.uint64),
+        "all_roots": np.arange(20_000, dtype=np.uint64),
+        "single": np.array([0], np.uint64),
+    }
+    par = np.array([i if (i == 0 or rng.random() < 0.05) else rng.integers(0, i) for i in range(50_000)], np.uint64)
+    perm = rng.permutation(50_000).astype(np.uint64)
+    relab = np.empty_like(par)
+    relab[perm] = perm[par]
+    out["random_many_roots"] = relab
+    return out
+
+
+def test_golden_forests(kb, golden_cases):
+    for tuning in ({}, DEEP, SPARSE):
+        t = kb.GpuTuning(**tuning)
+        for name, c in golden_cases.items():
+            if "w" in c:
+                continue  # weighted cases are lists with weights
+            if c["kind"][0] != "forest" and not name.startswith(("list_", "single", "pair", "all_roots")):
+                continue
+            # a list is a forest of paths too
+            root, depth = kb.root_forest(dev64(c["succ"]), tuning=t)
+            np.testing.assert_array_equal(host_u64(root), c["root"], err_msg=name)
+            np.testing.assert_array_equal(host_i64(depth), c["rank"], err_msg=name)
+
+
+@pytest.mark.parametrize("tuning", [{}, DEEP, SPARSE])
+def test_forests_vs_oracle(kb, oracle_mod, tuning):
+    for name, par in _forests(oracle_mod).items():
+        root_o, depth_o = oracle_mod.root_forest(par)
+        root, depth = kb.root_forest(dev64(par), tuning=kb.GpuTuning(**tuning))
+        np.testing.assert_array_equal(host_u64(root), root_o, err_msg=name)
+        np.testing.assert_array_equal(host_u64(depth), depth_o, err_msg=name)
+
+
+@pytest.mark.parametrize("n,kind,blocks,spine", [(1 << 20, 0, 64, 0), (1 << 20, 1, 8, 1 << 16)])
+def test_generated_forests(kb, oracle_mod, n, kind, blocks, spine):
+    par_h = oracle_mod.gen_forest(n, 0xC2, kind, blocks, spine)
+    par = kb.gen_forest(n, 0xC2, kind, blocks, spine)
+    np.testing.assert_array_equal(host_u64(par), par_h)
+    root_o, depth_o = oracle_mod.root_forest(par_h)
+    root, depth = kb.root_forest(par)
+    np.testing.assert_array_equal(host_u64(root), root_o)
+    np.testing.assert_array_equal(host_u64(depth), depth_o)
+
+
+def test_compute_euler_tour_kat(kb, kat):
+    e = kat["euler_tour_small"]
+    tour = kb.compute_euler_tour(dev64(np.array(e["parent"], np.uint64)))
+    assert host_u64(tour).tolist() == e["tour_succ"]
+
+
+def test_compute_euler_tour_vs_oracle(kb, oracle_mod):
+    for name, par in _forests(oracle_mod).items():
+        if par.size > 70_000:
+            continue
+        ts, tw, es, ed, up = oracle_mod.euler_tour(par)
+        tour = kb.compute_euler_tour(dev64(par))
+        np.testing.assert_array_equal(host_u64(tour), ts, err_msg=name)
+
+
+def test_rank_via_euler_tour_in_place(kb, oracle_mod):
+    """Roots keep their input values; non-roots get root and depth."""
+    par = oracle_mod.gen_forest(50_000, 8, 0, 16)
+    s_o = par.copy()
+    r_o = np.where(par == np.arange(par.size, dtype=np.uint64), 7, 1).astype(np.int64)
+    r_in = r_o.copy()
+    oracle_mod.rank_via_euler_tour(s_o, r_o)
+    s = dev64(par)
+    r = dev64(r_in)
+    kb.rank_via_euler_tour(kb.EulerTourConfig(), s, r)
+    np.testing.assert_array_equal(host_u64(s), s_o)
+    np.testing.assert_array_equal(host_i64(r), r_o)
+
+
+def test_root_forest_host(kb, oracle_mod):
+    par = oracle_mod.gen_forest(200_000, 11, 1, 5, 10_000)
+    root_o, depth_o = oracle_mod.root_forest(par)
+    root, depth = kb.root_forest_host(par)
+    np.testing.assert_array_equal(root, root_o)
+    np.testing.assert_array_equal(depth, depth_o)

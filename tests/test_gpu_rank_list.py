@@ -1,0 +1,142 @@
+"""List ranking on the GPU against the oracle and the reference's own outputs
+(golden fixtures), bit-exact."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from gpu_util import DEEP, SPARSE, dev32, dev64, host_i64, host_u64
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def kb():
+    import kascade_b200
+
+    return kascade_b200
+
+
+TUNINGS = {"default": {}, "deep": DEEP, "sparse": SPARSE, "chains1": dict(DEEP, chains_per_thread=1),
+           "chains4": dict(DEEP, chains_per_thread=4)}
+
+
+@pytest.mark.parametrize("tuning", list(TUNINGS))
+def test_golden_lists_ruling_set(kb, golden_cases, tuning):
+    t = kb.GpuTuning(**TUNINGS[tuning])
+    for name, c in golden_cases.items():
+        if c["kind"][0] != "list":
+            continue
+        succ = dev64(c["succ"])
+        w = dev32(c["w"]) if "w" in c else None
+        root, rank = kb.rank_list(succ, w, tuning=t)
+        np.testing.assert_array_equal(host_u64(root), c["root"], err_msg=name)
+        np.testing.assert_array_equal(host_i64(rank), c["rank"], err_msg=name)
+
+
+@pytest.mark.parametrize("alg", ["PointerDoubling", "GatherChase", "AsyncPointerDoubling", "RMAPointerDoubling"])
+def test_golden_all_cases_pointer_doubling(kb, golden_cases, alg):
+    """The doubling family accepts forests of trees too (GatherChase contract)."""
+    for tuning in ({}, {"base_case_size": 16}):
+        t = kb.GpuTuning(**tuning)
+        for name, c in golden_cases.items():
+            succ = dev64(c["succ"])
+            w = dev32(c["w"]) if "w" in c else None
+            root, rank = kb.rank_list(succ, w, tuning=t, algorithm=kb.Algorithm[alg])
+            np.testing.assert_array_equal(host_u64(root), c["root"], err_msg=name)
+            np.testing.assert_array_equal(host_i64(rank), c["rank"], err_msg=name)
+
+
+@pytest.mark.parametrize("n", [8191, 8192, 8193, 65536, 1 << 20])
+@pytest.mark.parametrize("layout", [0, 1, 2])
+@pytest.mark.parametrize("weighted", [False, True])
+def test_generated_lists_vs_oracle(kb, oracle_mod, n, layout, weighted):
+    succ_h = oracle_mod.gen_list(n, 0xC0 + n, layout)
+    w_h = oracle_mod.gen_weights(n, 0xC1, 16) if weighted else None
+    root_o, rank_o = oracle_mod.rank_list(succ_h, w_h)
+    succ = kb.gen_list(n, 0xC0 + n, layout)
+    np.testing.assert_array_equal(host_u64(succ), succ_h)  # device generator == host generator
+    w = kb.gen_weights(n, 0xC1, 16) if weighted else None
+    if weighted:
+        np.testing.assert_array_equal(w.cpu().numpy().view(np.uint32), w_h)
+    root, rank = kb.rank_list(succ, w)
+    np.testing.assert_array_equal(host_u64(root), root_o)
+    np.testing.assert_array_equal(host_u64(rank), rank_o)
+
+
+@pytest.mark.parametrize("parts", [2, 37, 1000, 20000])
+def test_many_lists(kb, oracle_mod, parts):
+    rng = np.random.default_rng(parts)
+    n = 200_000
+    order = rng.permutation(n).astype(np.uint64)
+    cuts = np.sort(rng.choice(np.arange(1, n), size=parts - 1, replace=False))
+    succ_h = np.empty(n, np.uint64)
+    for seg in np.split(order, cuts):
+        succ_h[seg[:-1]] = seg[1:]
+        succ_h[seg[-1]] = seg[-1]
+    w_h = rng.integers(0, 1 << 16, n).astype(np.uint32)
+    root_o, rank_o = oracle_mod.rank_list(succ_h, w_h)
+    for tuning in ({}, DEEP, SPARSE):
+        root, rank = kb.rank_list(dev64(succ_h), dev32(w_h), tuning=kb.GpuTuning(**tuning))
+        np.testing.assert_array_equal(host_u64(root), root_o)
+        np.testing.assert_array_equal(host_u64(rank), rank_o)
+
+
+def test_edge_sizes(kb, oracle_mod):
+    for succ_h in (np.array([0], np.uint64), np.array([1, 1], np.uint64), np.array([0, 0], np.uint64),
+                   np.arange(50_000, dtype=np.uint64),  # all roots
+                   np.minimum(np.arange(1, 30_001), 29_999).astype(np.uint64),  # path 0 -> 1 -> ...
+                   np.maximum(np.arange(-1, 29_999), 0).astype(np.uint64)):  # path n-1 -> ... -> 0
+        root_o, rank_o = oracle_mod.rank_list(succ_h)
+        for tuning in ({}, DEEP):
+            root, rank = kb.rank_list(dev64(succ_h), tuning=kb.GpuTuning(**tuning))
+            np.testing.assert_array_equal(host_u64(root), root_o)
+            np.testing.assert_array_equal(host_u64(rank), rank_o)
+    empty = torch.empty(0, dtype=torch.int64, device="cuda")
+    root, rank = kb.rank_list(empty)
+    assert root.numel() == 0 and rank.numel() == 0
+
+
+def test_zero_and_max_weights(kb, oracle_mod):
+    n = 100_000
+    succ_h = oracle_mod.gen_list(n, 7, 0)
+    for w_h in (np.zeros(n, np.uint32), np.full(n, 0xFFFFFFFF, np.uint32)):
+        root_o, rank_o = oracle_mod.rank_list(succ_h, w_h)
+        for tuning in ({}, DEEP):
+            root, rank = kb.rank_list(dev64(succ_h), dev32(w_h), tuning=kb.GpuTuning(**tuning))
+            np.testing.assert_array_equal(host_u64(rank), rank_o)
+            np.testing.assert_array_equal(host_u64(root), root_o)
+
+
+def test_host_variant(kb, oracle_mod):
+    n = 300_000
+    succ_h = oracle_mod.gen_list(n, 9, 1)
+    w_h = oracle_mod.gen_weights(n, 10, 16)
+    root_o, rank_o = oracle_mod.rank_list(succ_h, w_h)
+    root, rank = kb.rank_list_host(succ_h, w_h)
+    np.testing.assert_array_equal(root, root_o)
+    np.testing.assert_array_equal(rank, rank_o)
+
+
+def test_seed_independence(kb, oracle_mod):
+    """Ruler choice cannot change the result."""
+    n = 250_000
+    succ_h = oracle_mod.gen_list(n, 3, 0)
+    w_h = oracle_mod.gen_weights(n, 4, 16)
+    root_o, rank_o = oracle_mod.rank_list(succ_h, w_h)
+    for seed in (1, 2, 3, 0xDEADBEEF):
+        root, rank = kb.rank_list(dev64(succ_h), dev32(w_h), tuning=kb.GpuTuning(seed=seed, ruler_spacing=7))
+        np.testing.assert_array_equal(host_u64(rank), rank_o)
+        np.testing.assert_array_equal(host_u64(root), root_o)
+
+
+def test_profile_and_levels(kb):
+    ctx = kb.Context()
+    succ = kb.gen_list(1 << 20, 1, 0)
+    kb.rank_list(succ, tuning=kb.GpuTuning(profile=True), ctx=ctx)
+    times = ctx.kernel_times()
+    assert "chase" in times and "propagate" in times and "prepare" in times
+    lv = ctx.levels()
+    assert lv[0] == 1 << 20 and len(lv) >= 2 and lv[1] < lv[0] // 8
+    ctx.close()

@@ -1,0 +1,115 @@
+"""The CPU oracle against the reference's own code and known answers."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+
+def test_oracle_matches_golden(oracle_mod, golden_cases):
+    """Golden outputs were produced by the reference's GatherChase."""
+    for name, c in golden_cases.items():
+        if "w" in c:
+            root, rank = oracle_mod.rank_list(c["succ"], c["w"])
+        else:
+            root, rank = oracle_mod.rank_list(c["succ"])
+        np.testing.assert_array_equal(root, c["root"], err_msg=name)
+        np.testing.assert_array_equal(rank.view(np.int64), c["rank"], err_msg=name)
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_oracle_matches_reference_chase(oracle_mod, seed):
+    if not oracle_mod.has_ref():
+        pytest.skip("oracle/_ref not built (reference source tree absent)")
+    inputs = [
+        oracle_mod.gen_list(20000, seed, 0),
+        oracle_mod.gen_list(20000, seed, 1),
+        oracle_mod.gen_forest(30000, seed, 0, 5),
+        oracle_mod.gen_forest(30000, seed, 1, 4, 3000),
+    ]
+    for succ in inputs:
+        r1, k1 = oracle_mod.root_forest(succ)
+        r2, k2 = oracle_mod.ref_gather_rank(succ)
+        np.testing.assert_array_equal(r1, r2)
+        np.testing.assert_array_equal(k1.view(np.int64), k2)
+
+
+def test_pointer_doubling_oracle_agrees(oracle_mod, golden_cases):
+    for name, c in golden_cases.items():
+        s = c["succ"].copy()
+        r = (c["w"].astype(np.int64) if "w" in c else np.ones(s.size, np.int64))
+        r[s == np.arange(s.size, dtype=np.uint64)] = 0
+        rounds = oracle_mod.pointer_doubling(s, r)
+        assert rounds >= 0, name
+        np.testing.assert_array_equal(s, c["root"], err_msg=name)
+        np.testing.assert_array_equal(r, c["rank"], err_msg=name)
+
+
+def test_pack_kat(oracle_mod, kat):
+    p = kat["pack_works"]
+    sp, rp = oracle_mod.pack(np.array(p["succ"]), np.array(p["rank"]), np.array(p["active"]))
+    assert sp.tolist() == p["packed_succ"]
+    assert rp.tolist() == p["packed_rank"]
+    succ = np.array(p["succ"], np.uint64)
+    rank = np.array(p["rank"], np.int64)
+    oracle_mod.unpack(np.array(p["ranked_packed_succ"]), np.array(p["ranked_packed_rank"]),
+                      np.array(p["active"]), succ, rank)
+    assert succ.tolist() == p["unpacked_succ"]
+    assert rank.tolist() == p["unpacked_rank"]
+    s = kat["pack_sanity"]
+    n = len(s["succ"])
+    sp, rp = oracle_mod.pack(np.array(s["succ"]), np.array(s["rank"]), np.arange(n))
+    assert sp.tolist() == s["succ"] and rp.tolist() == s["rank"]
+
+
+def test_euler_tour_kat(oracle_mod, kat):
+    e = kat["euler_tour_small"]
+    ts, tw, es, ed, up = oracle_mod.euler_tour(np.array(e["parent"], np.uint64))
+    assert ts.tolist() == e["tour_succ"]
+    s = np.array(e["parent"], np.uint64)
+    r = np.where(s == np.arange(s.size, dtype=np.uint64), 0, 1).astype(np.int64)
+    oracle_mod.rank_via_euler_tour(s, r)
+    assert s.tolist() == e["root"] and r.tolist() == e["depth"]
+
+
+@pytest.mark.parametrize("kind,blocks,spine", [(0, 3, 0), (1, 2, 50), (0, 1, 0)])
+def test_euler_tour_is_one_list_per_tree(oracle_mod, kind, blocks, spine):
+    parent = oracle_mod.gen_forest(700, 9, kind, blocks, spine)
+    ts, tw, es, ed, up = oracle_mod.euler_tour(parent)
+    m = ts.size
+    roots = int((parent == np.arange(700, dtype=np.uint64)).sum())
+    assert m == 2 * (700 - roots) + roots
+    assert oracle_mod.is_list(ts)
+    # ranking the tour with the chase gives the depths at up edges
+    s, r = oracle_mod.root_forest(parent)
+    ts2 = ts.copy()
+    tw2 = tw.copy()
+    oracle_mod.local_pointer_chasing(ts2, tw2)
+    for e in np.nonzero(up)[0]:
+        assert tw2[e] == int(r[es[e]])
+
+
+def test_generators_are_valid(oracle_mod):
+    for layout in (0, 1, 2):
+        succ = oracle_mod.gen_list(5000, 3, layout)
+        assert oracle_mod.is_list(succ)
+        assert int((succ == np.arange(5000, dtype=np.uint64)).sum()) == 1
+        root, rank = oracle_mod.rank_list(succ)
+        assert sorted(rank.tolist()) == list(range(5000))
+    parent = oracle_mod.gen_forest(6400, 4, 0, 64)
+    assert int((parent == np.arange(6400, dtype=np.uint64)).sum()) == 64
+    cat = oracle_mod.gen_forest(6000, 4, 1, 3, 1000)
+    root, depth = oracle_mod.root_forest(cat)
+    assert int(depth.max()) in (999, 1000)
+
+
+def test_generator_fixture_is_stable(oracle_mod, golden_cases):
+    """The generators behind the golden inputs have not drifted."""
+    np.testing.assert_array_equal(oracle_mod.gen_list(1000, 0xC0, 0), golden_cases["list_random_1000"]["succ"])
+    np.testing.assert_array_equal(oracle_mod.gen_weights(3000, 12, 16), golden_cases["list_weighted_3000"]["w"])
+    np.testing.assert_array_equal(oracle_mod.gen_forest(6000, 22, 1, 3, 1500), golden_cases["forest_cat_6000"]["succ"])
+
+
+def test_oracle_detects_cycle(oracle_mod):
+    succ = np.array([1, 2, 0, 3], np.uint64)  # 0->1->2->0, 3 root
+    with pytest.raises(ValueError):
+        oracle_mod.rank_list(succ)
