@@ -189,6 +189,25 @@ def cpu_reference_time(n_sample: int, wl: str, reps: int = 1) -> tuple[float, st
         f" best of {reps}")
 
 
+def calibrate(local: int) -> None:
+    """Random 16 B access rate of the device (the chase's ceiling)."""
+    import ctypes
+
+    import kascade_b200 as kb
+
+    ctx = kb.Context(local)
+    out = {}
+    names = ["independent_read", "independent_read_write", "dependent_read", "dependent_read_write"]
+    for mode, nm in enumerate(names):
+        for bps in (8, 16):
+            v = ctypes.c_double(0)
+            kb._lib.check(kb.lib.kascade_calibrate_random_access(ctx.handle, 1 << 28, mode, bps, ctypes.byref(v)),
+                          "calibrate", ctx.handle)
+            out[f"{nm}@{bps}blk"] = round(v.value, 2)
+    print(json.dumps({"calibration": "G random 16 B record accesses/s, 2^28 records (4 GiB)", **out}), flush=True)
+    ctx.close()
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return
@@ -230,10 +249,16 @@ def main():
     ap.add_argument("--no-secondary", action="store_true")
     ap.add_argument("--spacing", type=int, default=0)
     ap.add_argument("--chains", type=int, default=0)
+    ap.add_argument("--n", type=int, default=0, help="override the workload size (profiling runs)")
+    ap.add_argument("--calibrate", action="store_true",
+                    help="measure the random 16 B access rate of this GPU (2^28 records) and exit")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
     world, rank, local = dist_setup()
+    if args.calibrate:
+        calibrate(local)
+        return
     if args.impl == "reference":
         run_reference(args, world, rank)
         if world > 1:
@@ -248,6 +273,9 @@ def main():
     import kascade_b200 as kb
 
     desc, n, kind, arg, weighted = WORKLOADS[args.workload]
+    if args.n:
+        n = args.n
+        desc = f"{desc} [size overridden: n={n}]"
     dev = torch.device(f"cuda:{local}")
     ctx = kb.Context(local)
     stream = torch.cuda.current_stream(dev)

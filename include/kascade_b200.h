@@ -226,6 +226,17 @@ KASCADE_API kascade_status kascade_gen_forest(uint64_t n, uint64_t seed, uint32_
                                               uint64_t blocks, uint64_t spine, uint64_t* parent,
                                               void* stream);
 
+/* ----------------------------------------------------------------------------
+ * Measurement.  Random-access calibration: G random 16 B record accesses per
+ * second in an array of n_records (far larger than L2).  mode 0: independent
+ * reads, 1: independent read + write back, 2: dependent chains (reads),
+ * 3: dependent chains with write back.  Diagnostic with no counterpart in the
+ * reference; it measures the ceiling the ruler chase runs against.
+ * ------------------------------------------------------------------------- */
+KASCADE_API kascade_status kascade_calibrate_random_access(kascade_ctx* ctx, uint64_t n_records,
+                                                           uint32_t mode, uint32_t blocks_per_sm,
+                                                           double* gaccess_per_s);
+
 #ifdef __cplusplus
 }
 #endif
