@@ -227,6 +227,24 @@ KASCADE_API kascade_status kascade_gen_forest(uint64_t n, uint64_t seed, uint32_
                                               void* stream);
 
 /* ----------------------------------------------------------------------------
+ * Ranking without allocation -- no counterpart in the reference.
+ * For callers that may not allocate device memory (a host framework that owns
+ * all device memory through its own pool, or a latency-critical path where an
+ * allocation's possible device synchronisation is not acceptable): no
+ * context, no cudaMalloc/cudaFree; scratch is one fixed device array of the
+ * library (2 MiB, held on every GPU that loads the library until exit).
+ * Same results as kascade_rank_list (lists or forests of trees) for
+ * n <= KASCADE_NOALLOC_MAX_ELEMENTS; larger n returns KASCADE_ERR_TOO_LARGE.
+ * All calls share the array: calls that overlap on the GPU race, so order
+ * them.  The first call on a device looks up the array's address; make it
+ * before any stream capture.  Synchronises `stream` before returning.
+ * ------------------------------------------------------------------------- */
+#define KASCADE_NOALLOC_MAX_ELEMENTS 65536u
+KASCADE_API kascade_status kascade_rank_list_noalloc(const uint64_t* succ, const uint32_t* weights,
+                                                     uint64_t n, uint64_t* root_out,
+                                                     uint64_t* rank_out, void* stream);
+
+/* ----------------------------------------------------------------------------
  * Measurement.  Random-access calibration: G random 16 B record accesses per
  * second in an array of n_records (far larger than L2).  mode 0: independent
  * reads, 1: independent read + write back, 2: dependent chains (reads),

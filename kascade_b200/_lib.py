@@ -105,6 +105,7 @@ _SIGS = {
     "kascade_gen_weights": (_status, [c_u64, c_u64, c_u32, c_void_p, c_void_p]),
     "kascade_gen_forest": (_status, [c_u64, c_u64, c_u32, c_u64, c_u64, c_void_p, c_void_p]),
     "kascade_calibrate_random_access": (_status, [_ctx_p, c_u64, c_u32, c_u32, P(ctypes.c_double)]),
+    "kascade_rank_list_noalloc": (_status, [c_void_p, c_void_p, c_u64, c_void_p, c_void_p, c_void_p]),
 }
 
 for _name, (_res, _args) in _SIGS.items():
