@@ -85,6 +85,10 @@ typedef struct kascade_opts {
   uint32_t async;             /* 1: return after enqueueing; see kascade_ctx_sync   */
   uint32_t profile;           /* 1: time each kernel with CUDA events               */
   uint32_t seed;              /* ruler-sampling seed                                */
+  uint32_t level0_mode;       /* 0 auto, 1 stamping chase, 2 write-free chase
+                                 (log + windowed scatter) for the first level      */
+  uint32_t max_chain;         /* hop cap of the write-free chase before it hands
+                                 level 0 to the stamping chase (0 = 64 x spacing)  */
 } kascade_opts;
 
 typedef struct kascade_ctx kascade_ctx;

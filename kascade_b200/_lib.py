@@ -44,6 +44,8 @@ class Opts(ctypes.Structure):
         ("async_", c_u32),
         ("profile", c_u32),
         ("seed", c_u32),
+        ("level0_mode", c_u32),
+        ("max_chain", c_u32),
     ]
 
 

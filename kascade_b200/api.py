@@ -55,6 +55,8 @@ class GpuTuning:
     profile: bool = False
     seed: int = 0
     async_: bool = False
+    level0_mode: int = 0
+    max_chain: int = 0
 
     def to_opts(self, algorithm: Algorithm = Algorithm.SparseRulingSet) -> Opts:
         o = Opts()
@@ -70,6 +72,8 @@ class GpuTuning:
         o.profile = int(self.profile)
         o.seed = self.seed
         o.async_ = int(self.async_)
+        o.level0_mode = self.level0_mode
+        o.max_chain = self.max_chain
         return o
 
 

@@ -1,4 +1,5 @@
 // The C ABI of libkascade_b200.so (declared in include/kascade_b200.h).
+#include <cstddef>
 #include <cstring>
 #include <new>
 
@@ -35,7 +36,9 @@ inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s
 
 kascade_status begin_call(kascade_ctx* ctx, cudaStream_t s, const kascade_opts* o) {
   if (!ctx) return KASCADE_ERR_INVALID_ARG;
-  if (o && o->struct_size != 0 && o->struct_size < sizeof(kascade_opts)) return KASCADE_ERR_INVALID_ARG;
+  // callers built against the first version of kascade_opts (without
+  // level0_mode / max_chain) pass a smaller struct_size; both are accepted
+  if (o && o->struct_size != 0 && o->struct_size < offsetof(kascade_opts, level0_mode)) return KASCADE_ERR_INVALID_ARG;
   KS_CUDA(cudaSetDevice(ctx->device));
   if (ctx->done_event && ctx->last_stream != s) KS_CUDA(cudaStreamWaitEvent(s, ctx->done_event, 0));
   KS_TRY(arena_begin_call(*ctx, s));
@@ -193,14 +196,17 @@ KASCADE_API kascade_status kascade_ctx_reserve(kascade_ctx* c, uint64_t bytes) {
 }
 
 KASCADE_API uint64_t kascade_scratch_bytes_rank_list(uint64_t n) {
-  // level-0 records + ruler list + level-1 records/results + deeper levels
-  return 16 * n + 4 * n + (40 * n) / 16 + (64ull << 20);
+  // level-0 records (16n) + ruler list (4n) + write-free path: log (16n),
+  // partitioned results (16n), reached flags (n) + level-1 records/results
+  // and deeper levels + per-warp log chunks
+  return 16 * n + 4 * n + 16 * n + 16 * n + n + (40 * n) / 16 + (192ull << 20);
 }
 
 KASCADE_API uint64_t kascade_scratch_bytes_root_forest(uint64_t n) {
-  // sort buffers (4 x 4n) + histogram + segments (8n) + tour records (32n)
-  // + ruler list (8n) + deeper levels
-  return 16 * n + 8 * n + 32 * n + 8 * n + (80 * n) / 16 + (64ull << 20);
+  // sort buffers (16n) + histogram + segments (8n) + tour records (32n)
+  // + ruler list (8n) + write-free path on 2n tour slots: log (32n),
+  // partitioned results (16n) + deeper levels
+  return 16 * n + 8 * n + 32 * n + 8 * n + 32 * n + 16 * n + (80 * n) / 16 + (192ull << 20);
 }
 
 KASCADE_API kascade_status kascade_ctx_sync(kascade_ctx* c, void* stream) {

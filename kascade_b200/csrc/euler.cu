@@ -83,11 +83,32 @@ __global__ void __launch_bounds__(256) k_tour_build(const uint32_t* __restrict__
         rd[i].a = ~0ull;  // -1
         rd[i].b = (sg.x < sg.y) ? n + sg.x : c;
         sd[i] = slot_down;
+        // the down edge to a root's first child is the head of that tree's
+        // tour: make it a ruler so that no tour element is left unreached
+        bool head = false;
+        bool first = true;
+        if (q > 0 && keys[q - 1] == p) first = (vals[q - 1] == p) && (q < 2 || keys[q - 2] != p);
+        if (first) {
+          if (q > 0 && keys[q - 1] == p) {
+            head = true;  // preceded by p's own entry: p is a root
+          } else {
+            const uint2 sp = seg[p];  // p is a root iff its own entry (p, p) is in its segment
+            uint32_t lo = sp.x, hi = sp.y;
+            while (lo < hi) {
+              const uint32_t mid = (lo + hi) >> 1;
+              if (vals[mid] < p)
+                lo = mid + 1;
+              else
+                hi = mid;
+            }
+            head = (lo < sp.y && vals[lo] == p);
+          }
+        }
         if (sampled(c, salt, thresh)) {
           rl |= 1u << (2 * i);
           cnt++;
         }
-        if (sampled(slot_down, salt, thresh)) {
+        if (head || sampled(slot_down, salt, thresh)) {
           rl |= 2u << (2 * i);
           cnt++;
         }

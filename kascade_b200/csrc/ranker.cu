@@ -15,6 +15,7 @@
 //   propagation (pull)  ruler_propagation.hpp:148-256 -> one coalesced pass
 //   pointer doubling    pointer_doubling_generic.hpp:43-60, 171-212, 418-438,
 //                       609-700 -> double-buffered jump kernel
+#include <cstddef>
 #include <cstdio>
 
 #include "ranker.cuh"
@@ -563,6 +564,11 @@ Params make_params(const kascade_ctx& ctx, const kascade_opts* o, uint64_t n) {
     if (o->block_size) p.block = o->block_size;
     if (o->seed) p.seed = o->seed;
     p.algorithm = o->algorithm;
+    if (o->struct_size >= offsetof(kascade_opts, max_chain) + sizeof(uint32_t)) {
+      if (o->level0_mode == 1) p.level0_log_min = 0xFFFFFFFFu;
+      if (o->level0_mode == 2) p.level0_log_min = 0;
+      p.max_chain = o->max_chain;
+    }
   }
   if (p.base_max > (uint32_t)(BASE_THREADS * BASE_PER_THREAD)) p.base_max = BASE_THREADS * BASE_PER_THREAD;
   if (p.spacing0 < 2) p.spacing0 = 2;
@@ -679,6 +685,13 @@ kascade_status rank_records(kascade_ctx& ctx, Rec* rec, uint32_t n, uint32_t r0,
   if (n <= p.base_max) return launch_base(ctx, rec, n, nullptr, sink, s);
   if (p.algorithm != KASCADE_ALGO_SPARSE_RULING_SET || p.max_levels == 0 || (uint64_t)r0 * 10 > (uint64_t)n * 7)
     return pointer_double_records(ctx, rec, n, nullptr, sink, s);
+  if (n >= p.level0_log_min) {
+    const kascade_status st = rank_level0_log(ctx, rec, n, r0, ruler_elem0, sink.log_target(n), p, s);
+    if (st != KASCADE_ERR_TIMEOUT) return st;
+    // a chain exceeded the write-free path's hop cap (invalid input, or an
+    // astronomically unlikely ruler gap): redo level 0 on the stamping path
+    KS_CUDA(cudaMemsetAsync(&ctx.d_status->counter[0], 0, sizeof(unsigned long long), s));
+  }
   Rec* rec1 = alloc<Rec>(ctx, r0);
   Out* out1 = alloc<Out>(ctx, r0);
   if (!rec1 || !out1) return KASCADE_ERR_OOM;
@@ -686,6 +699,11 @@ kascade_status rank_records(kascade_ctx& ctx, Rec* rec, uint32_t n, uint32_t r0,
   // level-1 elements are level-0 rulers: their level-0 index is ruler_elem0
   KS_TRY(rank_deep(ctx, rec1, r0, ruler_elem0, SinkOut{out1}, 1, p, s));
   return launch_propagate(ctx, rec, sink.limit(n), n, out1, sink, s);
+}
+
+kascade_status rank_sublist(kascade_ctx& ctx, Rec* rec, uint32_t n, const uint32_t* elem0, Out* out, int level,
+                            const Params& p, cudaStream_t s) {
+  return rank_deep(ctx, rec, n, elem0, SinkOut{out}, level, p, s);
 }
 
 kascade_status check_is_list(kascade_ctx& ctx, const uint64_t* succ, uint64_t n, int* ok, cudaStream_t s) {

@@ -28,6 +28,8 @@ struct Params {
   uint32_t block = 256;
   uint32_t seed = 0x6b617363u;
   uint32_t algorithm = KASCADE_ALGO_SPARSE_RULING_SET;
+  uint32_t level0_log_min = 1u << 22;  // level 0 uses the write-free path from this size on
+  uint32_t max_chain = 0;              // write-free chase hop cap (0: 64 x spacing0 + 1024)
 };
 
 Params make_params(const kascade_ctx& ctx, const kascade_opts* opts, uint64_t n);
@@ -35,6 +37,15 @@ Params make_params(const kascade_ctx& ctx, const kascade_opts* opts, uint64_t n)
 // Where results of level 0 go ------------------------------------------------
 // A sink receives, for element x, its rank, its root (level-0 index) and
 // whether x itself is a root.
+
+// Level-0 output description for the write-free (log) pipeline.
+struct LogTarget {
+  uint64_t* root;
+  uint64_t* rank;
+  uint32_t limit;        // elements [0, limit) produce output
+  int keep_roots;        // leave roots' entries untouched
+  int heads_are_rulers;  // every list head is a ruler: no element is left unreached
+};
 
 // Plain arrays. keep_roots: leave root entries untouched (the reference's
 // in-place contract); otherwise roots get (x, 0).
@@ -44,6 +55,7 @@ struct SinkPlain {
   int keep_roots;
   // elements [0, limit(n)) produce output
   uint32_t limit(uint32_t n) const { return n; }
+  LogTarget log_target(uint32_t n) const { return LogTarget{root, rank, n, keep_roots, 0}; }
   __device__ __forceinline__ void put(uint32_t x, uint64_t rk, uint32_t rt, bool is_root) const {
     if (is_root) {
       if (!keep_roots) {
@@ -65,6 +77,8 @@ struct SinkTour {
   uint32_t nv;
   int keep_roots;
   uint32_t limit(uint32_t n) const { return n < nv ? n : nv; }
+  // the tour build makes every tour head a ruler
+  LogTarget log_target(uint32_t n) const { return LogTarget{root, depth, limit(n), keep_roots, 1}; }
   __device__ __forceinline__ void put(uint32_t x, uint64_t rk, uint32_t rt, bool is_root) const {
     if (x >= nv) return;
     if (is_root) {
@@ -103,6 +117,19 @@ template <class Sink>
 kascade_status rank_records(kascade_ctx& ctx, Rec* rec, uint32_t n, uint32_t r0,
                             uint32_t* ruler_elem0, const Sink& sink, const Params& p,
                             cudaStream_t s);
+
+// Rank a deeper level (records written by the chase of the level above, tags
+// unassigned); results go to out[0..n).  elem0 maps this level's elements to
+// level-0 indices.
+kascade_status rank_sublist(kascade_ctx& ctx, Rec* rec, uint32_t n, const uint32_t* elem0, Out* out,
+                            int level, const Params& p, cudaStream_t s);
+
+// Write-free level 0: read-only chase that logs (element, ruler, distance),
+// recursion on the ruler sub-list, then resolve + partition by element window
+// and a windowed scatter into the outputs.
+kascade_status rank_level0_log(kascade_ctx& ctx, const Rec* rec, uint32_t n, uint32_t r0,
+                               const uint32_t* ruler_elem0, const LogTarget& t, const Params& p,
+                               cudaStream_t s);
 
 // Pointer doubling on level-0 records (tags ignored).
 template <class Sink>

@@ -37,7 +37,7 @@ def test_status_strings_and_opts():
         assert kb.lib.kascade_status_string(code)
     o = Opts()
     kb.lib.kascade_opts_init(ctypes.byref(o))
-    assert o.struct_size == ctypes.sizeof(Opts) == 48
+    assert o.struct_size == ctypes.sizeof(Opts) == 56
     assert o.algorithm == 4
     assert kb.lib.kascade_scratch_bytes_rank_list(1 << 20) < kb.lib.kascade_scratch_bytes_rank_list(1 << 28)
 

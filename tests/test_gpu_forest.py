@@ -38,7 +38,7 @@ def _forests(oracle_mod):
 
 
 def test_golden_forests(kb, golden_cases):
-    for tuning in ({}, DEEP, SPARSE):
+    for tuning in ({}, DEEP, SPARSE, dict(DEEP, level0_mode=2)):
         t = kb.GpuTuning(**tuning)
         for name, c in golden_cases.items():
             if "w" in c:
@@ -51,7 +51,8 @@ def test_golden_forests(kb, golden_cases):
             np.testing.assert_array_equal(host_i64(depth), c["rank"], err_msg=name)
 
 
-@pytest.mark.parametrize("tuning", [{}, DEEP, SPARSE])
+@pytest.mark.parametrize("tuning", [{}, DEEP, SPARSE, dict(DEEP, level0_mode=2), dict(SPARSE, level0_mode=2),
+                                    dict(DEEP, level0_mode=2, max_chain=2)])
 def test_forests_vs_oracle(kb, oracle_mod, tuning):
     for name, par in _forests(oracle_mod).items():
         root_o, depth_o = oracle_mod.root_forest(par)

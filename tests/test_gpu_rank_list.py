@@ -19,7 +19,13 @@ def kb():
 
 
 TUNINGS = {"default": {}, "deep": DEEP, "sparse": SPARSE, "chains1": dict(DEEP, chains_per_thread=1),
-           "chains4": dict(DEEP, chains_per_thread=4)}
+           "chains4": dict(DEEP, chains_per_thread=4),
+           # the write-free level 0 (log + windowed scatter), forced at small sizes
+           "log": dict(DEEP, level0_mode=2), "log_sparse": dict(SPARSE, level0_mode=2),
+           "log_chains1": dict(DEEP, level0_mode=2, chains_per_thread=1),
+           "log_chains4": dict(DEEP, level0_mode=2, chains_per_thread=4),
+           # a hop cap so small that level 0 always falls back to the stamping chase
+           "log_fallback": dict(DEEP, level0_mode=2, max_chain=2)}
 
 
 @pytest.mark.parametrize("tuning", list(TUNINGS))
@@ -60,9 +66,26 @@ def test_generated_lists_vs_oracle(kb, oracle_mod, n, layout, weighted):
     w = kb.gen_weights(n, 0xC1, 16) if weighted else None
     if weighted:
         np.testing.assert_array_equal(w.cpu().numpy().view(np.uint32), w_h)
-    root, rank = kb.rank_list(succ, w)
+    for mode in (1, 2):
+        root, rank = kb.rank_list(succ, w, tuning=kb.GpuTuning(level0_mode=mode))
+        np.testing.assert_array_equal(host_u64(root), root_o)
+        np.testing.assert_array_equal(host_u64(rank), rank_o)
+
+
+@pytest.mark.parametrize("layout", [0, 1])
+def test_auto_write_free_size(kb, oracle_mod, layout):
+    """Above 2^22 elements level 0 takes the write-free path by default."""
+    n = (1 << 22) + 12345
+    succ_h = oracle_mod.gen_list(n, 0xD0, layout)
+    w_h = oracle_mod.gen_weights(n, 0xD1, 16)
+    root_o, rank_o = oracle_mod.rank_list(succ_h, w_h)
+    ctx = kb.Context()
+    root, rank = kb.rank_list(dev64(succ_h), dev32(w_h), tuning=kb.GpuTuning(profile=True), ctx=ctx)
     np.testing.assert_array_equal(host_u64(root), root_o)
     np.testing.assert_array_equal(host_u64(rank), rank_o)
+    times = ctx.kernel_times()
+    assert "resolve" in times and "scatter" in times
+    ctx.close()
 
 
 @pytest.mark.parametrize("parts", [2, 37, 1000, 20000])
@@ -77,7 +100,7 @@ def test_many_lists(kb, oracle_mod, parts):
         succ_h[seg[-1]] = seg[-1]
     w_h = rng.integers(0, 1 << 16, n).astype(np.uint32)
     root_o, rank_o = oracle_mod.rank_list(succ_h, w_h)
-    for tuning in ({}, DEEP, SPARSE):
+    for tuning in ({}, DEEP, SPARSE, dict(DEEP, level0_mode=2), dict(level0_mode=2, base_case_size=64)):
         root, rank = kb.rank_list(dev64(succ_h), dev32(w_h), tuning=kb.GpuTuning(**tuning))
         np.testing.assert_array_equal(host_u64(root), root_o)
         np.testing.assert_array_equal(host_u64(rank), rank_o)
@@ -89,7 +112,7 @@ def test_edge_sizes(kb, oracle_mod):
                    np.minimum(np.arange(1, 30_001), 29_999).astype(np.uint64),  # path 0 -> 1 -> ...
                    np.maximum(np.arange(-1, 29_999), 0).astype(np.uint64)):  # path n-1 -> ... -> 0
         root_o, rank_o = oracle_mod.rank_list(succ_h)
-        for tuning in ({}, DEEP):
+        for tuning in ({}, DEEP, dict(DEEP, level0_mode=2)):
             root, rank = kb.rank_list(dev64(succ_h), tuning=kb.GpuTuning(**tuning))
             np.testing.assert_array_equal(host_u64(root), root_o)
             np.testing.assert_array_equal(host_u64(rank), rank_o)
@@ -103,7 +126,7 @@ def test_zero_and_max_weights(kb, oracle_mod):
     succ_h = oracle_mod.gen_list(n, 7, 0)
     for w_h in (np.zeros(n, np.uint32), np.full(n, 0xFFFFFFFF, np.uint32)):
         root_o, rank_o = oracle_mod.rank_list(succ_h, w_h)
-        for tuning in ({}, DEEP):
+        for tuning in ({}, DEEP, dict(DEEP, level0_mode=2)):
             root, rank = kb.rank_list(dev64(succ_h), dev32(w_h), tuning=kb.GpuTuning(**tuning))
             np.testing.assert_array_equal(host_u64(rank), rank_o)
             np.testing.assert_array_equal(host_u64(root), root_o)

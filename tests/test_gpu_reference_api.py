@@ -132,6 +132,19 @@ def test_error_statuses(kb):
             with pytest.raises(kb.KascadeError) as e:
                 kb.rank_list(cyc, algorithm=alg)
             assert e.value.name == "CYCLE"
+    # the same on the write-free level 0
+    cyc = dev64(((np.arange(100_000) + 1) % 100_000).astype(np.uint64))
+    with pytest.raises(kb.KascadeError) as e:
+        kb.rank_list(cyc, tuning=kb.GpuTuning(level0_mode=2, base_case_size=64))
+    assert e.value.name == "CYCLE"
+    # a tail leading into a rootless cycle (not a list): the write-free chase
+    # stops at its hop cap and the stamping chase reports the input
+    rho = np.arange(1, 3001, dtype=np.uint64)
+    rho[-1] = 1000
+    with pytest.raises(kb.KascadeError) as e:
+        kb.rank_list(dev64(rho), tuning=kb.GpuTuning(level0_mode=2, base_case_size=16, ruler_spacing=4,
+                                                      max_chain=64))
+    assert e.value.name in ("NOT_A_LIST", "CYCLE")
     # a tree given to the list-only ranker with validation on
     tree = dev64(np.array([0, 0, 0, 1], np.uint64))
     with pytest.raises(kb.KascadeError) as e:
