@@ -189,6 +189,11 @@ __global__ void __launch_bounds__(256) k_chase_log(const Rec* __restrict__ rec, 
           // tells the two cases apart exactly.
           if (++hops[c] > max_hops) {
             atomicOr(&st->counter[0], 1ull);
+            Rec o;  // keep the next level's records in range (the level is redone anyway)
+            o.a = 0;
+            o.b = cid[c];
+            o.c = TAG_UNREACHED;
+            st_rec_cg(rec_next + cid[c], o);
             act &= ~(1u << c);
           }
         }
@@ -276,7 +281,7 @@ __global__ void __launch_bounds__(256) k_scatter(const OutEnt* __restrict__ part
     __syncthreads();
     if (it >= total) break;
     const uint32_t b = it / IPB, k = it % IPB;
-    const uint32_t cnt = bcursor[b];
+    const uint32_t cnt = min(bcursor[b], WIN);  // beyond WIN only on invalid input (reported by resolve)
     const uint32_t beg = k * SCATTER_ITEM;
     if (beg >= cnt) continue;
     const uint32_t stop = min(beg + SCATTER_ITEM, cnt);

@@ -136,6 +136,10 @@ __global__ void __launch_bounds__(256) k_prepare_level(Rec* __restrict__ rec, ui
       uint64_t x = tile + (uint64_t)i * blockDim.x + threadIdx.x;
       if (x < n) {
         rv[i] = rec[x];
+        if (rv[i].b >= n) {  // never for records the level above wrote; kept as a guard
+          set_error(st, KASCADE_ERR_OUT_OF_RANGE, x);
+          rv[i].b = (uint32_t)x;
+        }
         if (rv[i].b == (uint32_t)x || sampled((uint32_t)x, salt, thresh)) {
           rl |= 1u << i;
           cnt++;
@@ -164,6 +168,16 @@ __global__ void __launch_bounds__(256) k_prepare_level(Rec* __restrict__ rec, ui
     }
     __syncthreads();
   }
+}
+
+// A chain that ends on an error still leaves its ruler a valid next-level
+// record (a self loop), so that later levels only ever see in-range indices.
+__device__ __forceinline__ void end_chain_on_error(Rec* rec_next, uint32_t id) {
+  Rec o;
+  o.a = 0;
+  o.b = id;
+  o.c = TAG_UNREACHED;
+  st_rec_cg(rec_next + id, o);
 }
 
 // ---------------------------------------------------------------------------
@@ -261,6 +275,7 @@ __global__ void __launch_bounds__(256) k_chase(Rec* __restrict__ rec, uint32_t n
         cx[c] = rr[c].b;
         if (++hops[c] > n) {
           set_error(st, KASCADE_ERR_CYCLE, cid[c]);
+          end_chain_on_error(rec_next, cid[c]);
           act &= ~(1u << c);
         }
       } else if (tag_ruler(tg)) {
@@ -273,6 +288,7 @@ __global__ void __launch_bounds__(256) k_chase(Rec* __restrict__ rec, uint32_t n
       } else {
         // already stamped by another chase: two predecessors
         set_error(st, KASCADE_ERR_NOT_A_LIST, cx[c]);
+        end_chain_on_error(rec_next, cid[c]);
         act &= ~(1u << c);
       }
     }
@@ -358,6 +374,10 @@ __global__ void __launch_bounds__(BASE_THREADS) k_base(const Rec* __restrict__ r
   uint8_t* isroot = smem + 12ull * n;
   for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
     Rec r = rec[i];
+    if (r.b >= n) {  // guard: treat as a root and report
+      set_error(st, KASCADE_ERR_OUT_OF_RANGE, i);
+      r.b = i;
+    }
     bool root = (r.b == i);
     sc[i] = r.b;
     rk[i] = root ? 0ull : r.a;
@@ -410,9 +430,14 @@ __global__ void __launch_bounds__(BASE_THREADS) k_base(const Rec* __restrict__ r
 // pointer doubling: double-buffered jump rounds over 16 B records.
 // done bit 0: successor is a root; bit 1: the element is a root.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_pd_init(const Rec* __restrict__ rec, uint32_t n, PdRec* __restrict__ a) {
+__global__ void __launch_bounds__(256) k_pd_init(const Rec* __restrict__ rec, uint32_t n, PdRec* __restrict__ a,
+                                                 DevStatus* st) {
   for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; x < n; x += (uint64_t)gridDim.x * blockDim.x) {
     Rec r = rec[x];
+    if (r.b >= n) {  // guard: treat as a root and report
+      set_error(st, KASCADE_ERR_OUT_OF_RANGE, x);
+      r.b = (uint32_t)x;
+    }
     bool root = (r.b == (uint32_t)x);
     PdRec p;
     p.rank = root ? 0ull : r.a;
@@ -614,7 +639,7 @@ kascade_status pointer_double_records(kascade_ctx& ctx, const Rec* rec, uint32_t
   unsigned grid = grid_for(ctx, n, 256, 8);
   {
     ProfScope ps(ctx, "pd_init", s);
-    k_pd_init<<<grid, 256, 0, s>>>(rec, n, a);
+    k_pd_init<<<grid, 256, 0, s>>>(rec, n, a, ctx.d_status);
     KS_CHECK_LAUNCH();
   }
   int rounds = 0;
