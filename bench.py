@@ -250,6 +250,7 @@ def main():
     ap.add_argument("--spacing", type=int, default=0)
     ap.add_argument("--chains", type=int, default=0)
     ap.add_argument("--n", type=int, default=0, help="override the workload size (profiling runs)")
+    ap.add_argument("--level0-mode", type=int, default=0, help="0 auto, 1 stamping chase, 2 write-free chase")
     ap.add_argument("--calibrate", action="store_true",
                     help="measure the random 16 B access rate of this GPU (2^28 records) and exit")
     args = ap.parse_args()
@@ -280,7 +281,8 @@ def main():
     ctx = kb.Context(local)
     stream = torch.cuda.current_stream(dev)
     seed = 0xC1 + 1000 * rank
-    tuning = kb.GpuTuning(profile=True, ruler_spacing=args.spacing, chains_per_thread=args.chains)
+    tuning = kb.GpuTuning(profile=True, ruler_spacing=args.spacing, chains_per_thread=args.chains,
+                          level0_mode=args.level0_mode)
     if kind == "list":
         inp = kb.gen_list(n, seed, arg, device=dev)
         w = kb.gen_weights(n, seed + 1, 16, device=dev) if weighted else None
@@ -371,7 +373,8 @@ def main():
             pin_w.copy_(w.cpu())
         pin_root = torch.empty(n, dtype=torch.int64, pin_memory=True)
         pin_rank = torch.empty(n, dtype=torch.int64, pin_memory=True)
-        o = kb.GpuTuning(ruler_spacing=args.spacing, chains_per_thread=args.chains).to_opts()
+        o = kb.GpuTuning(ruler_spacing=args.spacing, chains_per_thread=args.chains,
+                         level0_mode=args.level0_mode).to_opts()
         import ctypes
 
         def e2e_step():
@@ -406,7 +409,7 @@ def main():
     if not args.no_secondary and kind == "list" and args.workload == "list" and world == 1:
         # the locality-biased layout of the same configuration
         inp2 = kb.gen_list(n, seed, 1, device=dev)
-        tun2 = kb.GpuTuning(ruler_spacing=args.spacing, chains_per_thread=args.chains)
+        tun2 = kb.GpuTuning(ruler_spacing=args.spacing, chains_per_thread=args.chains, level0_mode=args.level0_mode)
         for _ in range(2):
             kb.rank_list(inp2, w, tuning=tun2, root_out=root, rank_out=rk, ctx=ctx)
         torch.cuda.synchronize()

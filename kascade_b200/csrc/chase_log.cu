@@ -33,11 +33,12 @@ namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
 constexpr uint32_t LOG_CHUNK = 1024;  // entries per warp-owned log chunk
-constexpr uint32_t WIN_SHIFT = 21;    // 2^21 elements per output window
+constexpr uint32_t WIN_SHIFT = 19;    // 2^19 elements per output window (8.5 MB of outputs)
 constexpr uint32_t WIN = 1u << WIN_SHIFT;
-constexpr uint32_t MAX_BUCKETS = 2048;  // windows for 2^32 elements
+constexpr uint32_t MAX_BUCKETS = 8192;  // windows for 2^32 elements
+constexpr uint32_t CURSOR_STRIDE = 8;   // one 32 B sector per window cursor (spreads the atomics)
 constexpr uint32_t FLAG_ONLY = 0xFFFFFFFFu;
-constexpr uint32_t SCATTER_ITEM = 4096;
+constexpr uint32_t SCATTER_ITEM = 1024;
 
 struct __align__(16) LogEnt {
   uint32_t x;
@@ -212,8 +213,9 @@ __global__ void __launch_bounds__(256) k_resolve_partition(const LogEnt* __restr
                                                            uint32_t* __restrict__ bcursor,
                                                            unsigned long long* __restrict__ logged, DevStatus* st) {
   constexpr int PER = LOG_CHUNK / 256;
-  __shared__ uint32_t bcnt[MAX_BUCKETS];
-  __shared__ uint32_t bbase[MAX_BUCKETS];
+  extern __shared__ uint32_t dyn[];
+  uint32_t* bcnt = dyn;        // nb entries
+  uint32_t* bbase = dyn + nb;  // nb entries
   unsigned long long block_logged = 0;
   for (uint32_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
     const uint32_t fill = chunk_fill[ch];
@@ -249,7 +251,7 @@ __global__ void __launch_bounds__(256) k_resolve_partition(const LogEnt* __restr
     }
     __syncthreads();
     for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x)
-      if (bcnt[b]) bbase[b] = atomicAdd(bcursor + b, bcnt[b]);
+      if (bcnt[b]) bbase[b] = atomicAdd(bcursor + (uint64_t)b * CURSOR_STRIDE, bcnt[b]);
     __syncthreads();
 #pragma unroll
     for (int i = 0; i < PER; ++i) {
@@ -281,7 +283,7 @@ __global__ void __launch_bounds__(256) k_scatter(const OutEnt* __restrict__ part
     __syncthreads();
     if (it >= total) break;
     const uint32_t b = it / IPB, k = it % IPB;
-    const uint32_t cnt = min(bcursor[b], WIN);  // beyond WIN only on invalid input (reported by resolve)
+    const uint32_t cnt = min(bcursor[(uint64_t)b * CURSOR_STRIDE], WIN);  // beyond WIN only on invalid input
     const uint32_t beg = k * SCATTER_ITEM;
     if (beg >= cnt) continue;
     const uint32_t stop = min(beg + SCATTER_ITEM, cnt);
@@ -464,14 +466,23 @@ kascade_status rank_level0_log(kascade_ctx& ctx, const Rec* rec, uint32_t n, uin
   const uint32_t limit = t.limit < n ? t.limit : n;
   const uint32_t nb = (uint32_t)(((uint64_t)limit + WIN - 1) / WIN);
   OutEnt* part = alloc<OutEnt>(ctx, (uint64_t)(nb ? nb : 1) * WIN);
-  uint32_t* bcursor = alloc<uint32_t>(ctx, nb ? nb : 1);
+  uint32_t* bcursor = alloc<uint32_t>(ctx, (uint64_t)(nb ? nb : 1) * CURSOR_STRIDE);
   if (!part || !bcursor) return KASCADE_ERR_OOM;
-  KS_CUDA(cudaMemsetAsync(bcursor, 0, sizeof(uint32_t) * (nb ? nb : 1), s));
+  KS_CUDA(cudaMemsetAsync(bcursor, 0, sizeof(uint32_t) * (nb ? nb : 1) * CURSOR_STRIDE, s));
   {
     ProfScope ps(ctx, "resolve", s);
     const unsigned g = (unsigned)std::min<uint64_t>(nchunks, (uint64_t)ctx.sm_count * 8);
-    k_resolve_partition<<<g, 256, 0, s>>>(log, chunk_fill, nchunks, out1, limit, t.keep_roots, nb, part, bcursor,
-                                          logged, ctx.d_status);
+    const size_t smem = 2 * sizeof(uint32_t) * (nb ? nb : 1);
+    if (smem > 48 * 1024) {
+      static bool raised = false;
+      if (!raised) {
+        KS_CUDA(cudaFuncSetAttribute(k_resolve_partition, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(2 * sizeof(uint32_t) * MAX_BUCKETS)));
+        raised = true;
+      }
+    }
+    k_resolve_partition<<<g, 256, smem, s>>>(log, chunk_fill, nchunks, out1, limit, t.keep_roots, nb, part, bcursor,
+                                             logged, ctx.d_status);
     KS_CHECK_LAUNCH();
   }
   uint32_t lg[2] = {0, 0};

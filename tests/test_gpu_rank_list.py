@@ -73,14 +73,14 @@ def test_generated_lists_vs_oracle(kb, oracle_mod, n, layout, weighted):
 
 
 @pytest.mark.parametrize("layout", [0, 1])
-def test_auto_write_free_size(kb, oracle_mod, layout):
-    """Above 2^22 elements level 0 takes the write-free path by default."""
+def test_write_free_above_2_22(kb, oracle_mod, layout):
+    """The write-free level 0 at a size with several output windows."""
     n = (1 << 22) + 12345
     succ_h = oracle_mod.gen_list(n, 0xD0, layout)
     w_h = oracle_mod.gen_weights(n, 0xD1, 16)
     root_o, rank_o = oracle_mod.rank_list(succ_h, w_h)
     ctx = kb.Context()
-    root, rank = kb.rank_list(dev64(succ_h), dev32(w_h), tuning=kb.GpuTuning(profile=True), ctx=ctx)
+    root, rank = kb.rank_list(dev64(succ_h), dev32(w_h), tuning=kb.GpuTuning(profile=True, level0_mode=2), ctx=ctx)
     np.testing.assert_array_equal(host_u64(root), root_o)
     np.testing.assert_array_equal(host_u64(rank), rank_o)
     times = ctx.kernel_times()
