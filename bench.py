@@ -208,6 +208,130 @@ def calibrate(local: int) -> None:
     ctx.close()
 
 
+def measure_batched(kb, ctx, dev, steps: int = 3) -> dict:
+    """4096 independent instances (sizes log-uniform in
+    [2^6, 2^22] rescaled to sum to 2^28; 70% weighted lists, 30% random
+    recursive forests) ranked by one kascade_rank_batch call, against plain
+    per-instance calls on the same instances."""
+    import numpy as np
+    import torch
+
+    sizes, kinds = kb.batch_sizes(4096, 0xC3, lo_log2=6, hi_log2=22, total=1 << 28)
+    inputs, w = kb.gen_batch(sizes, kinds, seed=0xC3, device=dev)
+    segs = kb.make_segments(sizes, kinds)
+    total = int(sizes.sum())
+    root = torch.empty(total, dtype=torch.int64, device=dev)
+    rk = torch.empty(total, dtype=torch.int64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(2):
+        kb.rank_batch(inputs, segs, w, root_out=root, rank_out=rk, ctx=ctx)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        kb.rank_batch(inputs, segs, w, root_out=root, rank_out=rk, ctx=ctx)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    tb = e0.elapsed_time(e1) / steps / 1000.0
+    # plain per-instance launches of the same instances (one call each)
+    root2 = torch.empty_like(root)
+    rk2 = torch.empty_like(rk)
+    offs = np.concatenate([[0], np.cumsum(sizes)])
+    torch.cuda.synchronize()
+    p0 = time.perf_counter()
+    p_ev0, p_ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p_ev0.record(stream)
+    for i in range(len(sizes)):
+        a, b = int(offs[i]), int(offs[i + 1])
+        if kinds[i] == kb.SEG_LIST:
+            kb.rank_list(inputs[a:b], w[a:b], root_out=root2[a:b], rank_out=rk2[a:b], ctx=ctx)
+        else:
+            kb.root_forest(inputs[a:b], root_out=root2[a:b], depth_out=rk2[a:b], ctx=ctx)
+    p_ev1.record(stream)
+    torch.cuda.synchronize()
+    tp = max(p_ev0.elapsed_time(p_ev1) / 1000.0, time.perf_counter() - p0)
+    same = bool(torch.equal(root, root2) and torch.equal(rk, rk2))
+    return {"workload": "4096 instances, sizes log-uniform in [2^6,2^22] rescaled to sum 2^28, 70% weighted lists / "
+                        "30% random recursive forests, one kascade_rank_batch call",
+            "instances": len(sizes), "elements": total, "ms_per_batch": round(tb * 1e3, 3),
+            "req_per_s": round(len(sizes) / tb, 1), "elements_per_s": total / tb,
+            "plain_per_instance_ms": round(tp * 1e3, 1), "plain_elements_per_s": total / tp,
+            "speedup_vs_plain": round(tp / tb, 2), "results_equal_plain": same}
+
+
+def measure_served(kb, dev, n_requests: int = 1000, rate: float = 20000.0) -> dict:
+    """Poisson arrivals (mean 20k req/s) of sizes
+    log-uniform in [2^8, 2^24], 70% weighted lists / 30% random recursive
+    forests, served under a 40 GB HBM budget with device-resident inputs;
+    p50 / p99 latency and throughput, against plain per-request calls."""
+    import numpy as np
+    import torch
+
+    rng = np.random.default_rng(0xC4)
+    sizes = np.floor(2.0 ** rng.uniform(8, 24, n_requests)).astype(np.int64)
+    kinds = np.where(rng.random(n_requests) < 0.7, kb.SEG_LIST, kb.SEG_FOREST)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n_requests))
+    inputs, w = kb.gen_batch(sizes, kinds, seed=0xC4, device=dev)
+    offs = np.concatenate([[0], np.cumsum(sizes)])
+    torch.cuda.synchronize()
+    srv = kb.Server(device=dev.index or 0, hbm_budget=40 << 30, small_max=1 << 20, small_batch_elements=1 << 23)
+    # warm the lanes once
+    wid = srv.submit(int(kinds[0]), inputs[0:int(sizes[0])], w[0:int(sizes[0])] if kinds[0] == kb.SEG_LIST else None)
+    srv.wait(wid, 60.0)
+    srv.release(wid)
+    srv.reset_stats()
+    ids = []
+    t0 = time.perf_counter()
+    for i in range(n_requests):
+        delay = t0 + arrivals[i] - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        a, b = int(offs[i]), int(offs[i + 1])
+        ids.append(srv.submit(int(kinds[i]), inputs[a:b], w[a:b] if kinds[i] == kb.SEG_LIST else None))
+    for rid in ids:
+        srv.wait(rid, 300.0)
+    st = srv.stats()
+    # spot-check three results against plain calls
+    ok = True
+    for i in (0, n_requests // 2, n_requests - 1):
+        a, b = int(offs[i]), int(offs[i + 1])
+        r_dev, k_dev = srv.result_device(ids[i])
+        if kinds[i] == kb.SEG_LIST:
+            r_p, k_p = kb.rank_list(inputs[a:b], w[a:b])
+        else:
+            r_p, k_p = kb.root_forest(inputs[a:b])
+        ok &= bool(torch.equal(r_dev.view(torch.int64), r_p) and torch.equal(k_dev.view(torch.int64), k_p))
+    for rid in ids:
+        srv.release(rid)
+    srv.close()
+    # plain per-request calls of the same requests, back to back
+    ctx = kb.Context(dev.index or 0)
+    root = torch.empty(int(sizes.max()), dtype=torch.int64, device=dev)
+    rk = torch.empty_like(root)
+    torch.cuda.synchronize()
+    p0 = time.perf_counter()
+    for i in range(n_requests):
+        a, b = int(offs[i]), int(offs[i + 1])
+        n = b - a
+        if kinds[i] == kb.SEG_LIST:
+            kb.rank_list(inputs[a:b], w[a:b], root_out=root[:n], rank_out=rk[:n], ctx=ctx)
+        else:
+            kb.root_forest(inputs[a:b], root_out=root[:n], depth_out=rk[:n], ctx=ctx)
+    torch.cuda.synchronize()
+    tp = time.perf_counter() - p0
+    ctx.close()
+    total = int(sizes.sum())
+    return {"workload": f"{n_requests} requests, Poisson arrivals at {rate:.0f}/s, sizes log-uniform in [2^8,2^24], "
+                        "70% weighted lists / 30% random recursive forests, 40 GB admission budget, device-resident "
+                        "inputs",
+            "requests": n_requests, "elements": total, "req_per_s": round(st["requests_per_s"], 1),
+            "elements_per_s": st["elements_per_s"], "p50_ms": round(st["p50_ms"], 3), "p99_ms": round(st["p99_ms"], 3),
+            "p50_ms_le_2^20": round(st["p50_small_ms"], 3), "p99_ms_le_2^20": round(st["p99_small_ms"], 3),
+            "requests_le_2^20": int(st["completed_small"]), "batches": int(st["batches"]),
+            "plain_elements_per_s": total / tp, "plain_req_per_s": round(n_requests / tp, 1),
+            "throughput_vs_plain": round(st["elements_per_s"] / (total / tp), 2), "spot_check_equal": ok}
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return
@@ -426,6 +550,14 @@ def main():
                                    "pipeline_frac": round(n * b_alg / (tl / 1000.0) / 1e9 / hbm, 4)}
         del inp2
 
+    batched = served = None
+    if world == 1 and not args.no_secondary and args.workload == "list" and not args.n:
+        del inp
+        torch.cuda.empty_cache()
+        batched = measure_batched(kb, ctx, dev)
+        torch.cuda.empty_cache()
+        served = measure_served(kb, dev)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, kd, sample = cpu_reference_time(args.cpu_sample, args.workload)
@@ -443,7 +575,7 @@ def main():
             "roofline": roofline, "pipeline_roofline": pipeline, "cpu_baseline": cpu, "e2e": e2e,
             "clocks": clk, "gpu_launches": launches,
             "kernels_ms_per_step": {k: round(v, 4) for k, v in sorted(step_kernel_ms.items())},
-            "secondary": secondary or None,
+            "secondary": secondary or None, "batched": batched, "served": served,
         }
         print(json.dumps(out), flush=True)
     ctx.close()

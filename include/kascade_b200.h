@@ -231,6 +231,101 @@ KASCADE_API kascade_status kascade_gen_forest(uint64_t n, uint64_t seed, uint32_
                                               void* stream);
 
 /* ----------------------------------------------------------------------------
+ * Batched ranking: many independent lists and forests in one call, ranked by
+ * one shared ruler chase (one persistent launch, one device work queue).
+ * Instances are concatenated in `input` (instance-local successor or parent
+ * indices); segs[i] gives instance i's offset (= sum of the earlier sizes),
+ * size and kind.  Outputs are written at the same positions: for lists root
+ * and rank, for forests root and depth, roots relative to their instance.
+ * weights (optional) apply to list instances.  Each instance's ruler spacing
+ * comes from the context's size-class table unless opts->ruler_spacing is
+ * set.  No counterpart in the reference (it ranks one distributed instance
+ * per call).
+ * ------------------------------------------------------------------------- */
+#define KASCADE_SEG_LIST 0u
+#define KASCADE_SEG_FOREST 1u
+typedef struct kascade_segment {
+  uint64_t offset;
+  uint64_t size;
+  uint32_t kind; /* KASCADE_SEG_LIST or KASCADE_SEG_FOREST */
+  uint32_t reserved;
+} kascade_segment;
+
+KASCADE_API kascade_status kascade_rank_batch(kascade_ctx* ctx, const kascade_segment* segs,
+                                              uint32_t num_segs, const uint64_t* input,
+                                              const uint32_t* weights, uint64_t total_n,
+                                              uint64_t* root_out, uint64_t* rank_out,
+                                              const kascade_opts* opts, void* stream);
+
+/* Size classes: an instance of at most max_size[i] elements (tour elements
+ * for forests: twice the vertex count) uses mean ruler spacing spacing[i];
+ * classes in increasing max_size, the last one covering everything. */
+KASCADE_API kascade_status kascade_ctx_set_size_classes(kascade_ctx* ctx, const uint64_t* max_size,
+                                                        const uint32_t* spacing, uint32_t count);
+KASCADE_API int kascade_ctx_get_size_classes(kascade_ctx* ctx, uint64_t* max_size, uint32_t* spacing,
+                                             int cap);
+
+/* ----------------------------------------------------------------------------
+ * Serving: a request loop over the batched ranker (no counterpart in the
+ * reference).  Requests are admitted by HBM footprint under a budget; their
+ * inputs and results stay on the device; two lanes (requests up to small_max
+ * elements, and larger ones) each coalesce the admitted requests waiting when
+ * they become free into one batched call, so arrivals join as memory and
+ * lanes free up and both lanes' work overlaps on the device.
+ * ------------------------------------------------------------------------- */
+typedef struct kascade_server kascade_server;
+typedef struct kascade_server_config {
+  uint32_t struct_size;
+  int device;
+  uint64_t hbm_budget_bytes;     /* admission budget (default 40 GiB)             */
+  uint32_t max_batch_requests;   /* requests per batch (default 4096)             */
+  uint32_t reserved;
+  uint64_t max_batch_elements;   /* elements per batch, large lane (default 2^28) */
+  uint64_t small_max;            /* latency lane: requests up to this many
+                                    elements (default 2^20)                       */
+  uint64_t small_batch_elements; /* elements per batch, latency lane (2^23)       */
+} kascade_server_config;
+
+typedef struct kascade_server_stats {
+  uint64_t completed;
+  uint64_t completed_small;
+  uint64_t batches;
+  uint64_t elements;
+  double p50_ms, p99_ms;             /* submit-to-completion latency, all requests */
+  double p50_small_ms, p99_small_ms; /* requests up to small_max elements          */
+  double elements_per_s;             /* completed elements / (last completion -
+                                        first submission)                         */
+  double requests_per_s;
+  uint64_t bytes_in_use;
+} kascade_server_stats;
+
+KASCADE_API void kascade_server_config_init(kascade_server_config* cfg);
+KASCADE_API kascade_status kascade_server_create(const kascade_server_config* cfg, kascade_server** out);
+KASCADE_API kascade_status kascade_server_destroy(kascade_server* server);
+/* kind: KASCADE_SEG_LIST (succ + optional weights) or KASCADE_SEG_FOREST
+ * (parent array).  Host input is copied at submission; a request that does
+ * not fit the budget yet waits in arrival order. */
+KASCADE_API kascade_status kascade_server_submit(kascade_server* server, uint32_t kind, const uint64_t* input,
+                                                 const uint32_t* weights, uint64_t n, uint64_t* request_id);
+/* The same for input already in device memory (copied into the server's own
+ * buffers on admission; blocks while the budget is exhausted). */
+KASCADE_API kascade_status kascade_server_submit_device(kascade_server* server, uint32_t kind,
+                                                        const uint64_t* input, const uint32_t* weights,
+                                                        uint64_t n, uint64_t* request_id);
+/* Wait for completion (timeout_s < 0: forever); returns the request status. */
+KASCADE_API kascade_status kascade_server_wait(kascade_server* server, uint64_t request_id, double timeout_s);
+/* Device pointers to a completed request's root and rank (or depth). */
+KASCADE_API kascade_status kascade_server_result_device(kascade_server* server, uint64_t request_id,
+                                                        const uint64_t** root, const uint64_t** rank);
+/* Copy a completed request's results to host buffers of n entries. */
+KASCADE_API kascade_status kascade_server_fetch(kascade_server* server, uint64_t request_id,
+                                                uint64_t* root_out, uint64_t* rank_out);
+/* Drop a completed request and its device results. */
+KASCADE_API kascade_status kascade_server_release(kascade_server* server, uint64_t request_id);
+KASCADE_API kascade_status kascade_server_get_stats(kascade_server* server, kascade_server_stats* out);
+KASCADE_API kascade_status kascade_server_reset_stats(kascade_server* server);
+
+/* ----------------------------------------------------------------------------
  * Ranking without allocation -- no counterpart in the reference.
  * For callers that may not allocate device memory (a host framework that owns
  * all device memory through its own pool, or a latency-critical path where an

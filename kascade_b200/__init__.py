@@ -12,6 +12,8 @@ from .api import (  # noqa: F401
     LAYOUT_IDENTITY,
     LAYOUT_RANDOM,
     LAYOUT_RUNS,
+    SEG_FOREST,
+    SEG_LIST,
     Algorithm,
     B200Ranking,
     Context,
@@ -19,8 +21,15 @@ from .api import (  # noqa: F401
     GpuTuning,
     PointerDoublingConfig,
     RulerSelectionStrategy,
+    Server,
     SparseRulingSetConfig,
     async_pointer_doubling,
+    batch_sizes,
+    gen_batch,
+    get_size_classes,
+    make_segments,
+    rank_batch,
+    set_size_classes,
     compute_euler_tour,
     default_context,
     gen_forest,

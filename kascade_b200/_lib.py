@@ -28,6 +28,30 @@ c_int = ctypes.c_int
 P = ctypes.POINTER
 
 
+class Segment(ctypes.Structure):
+    """Mirror of ``kascade_segment``."""
+
+    _fields_ = [("offset", ctypes.c_uint64), ("size", ctypes.c_uint64), ("kind", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32)]
+
+
+class ServerConfig(ctypes.Structure):
+    """Mirror of ``kascade_server_config``."""
+
+    _fields_ = [("struct_size", c_u32), ("device", c_int), ("hbm_budget_bytes", c_u64),
+                ("max_batch_requests", c_u32), ("reserved", c_u32), ("max_batch_elements", c_u64),
+                ("small_max", c_u64), ("small_batch_elements", c_u64)]
+
+
+class ServerStats(ctypes.Structure):
+    """Mirror of ``kascade_server_stats``."""
+
+    _fields_ = [("completed", c_u64), ("completed_small", c_u64), ("batches", c_u64), ("elements", c_u64),
+                ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double), ("p50_small_ms", ctypes.c_double),
+                ("p99_small_ms", ctypes.c_double), ("elements_per_s", ctypes.c_double),
+                ("requests_per_s", ctypes.c_double), ("bytes_in_use", c_u64)]
+
+
 class Opts(ctypes.Structure):
     """Mirror of ``kascade_opts``."""
 
@@ -108,6 +132,23 @@ _SIGS = {
     "kascade_gen_forest": (_status, [c_u64, c_u64, c_u32, c_u64, c_u64, c_void_p, c_void_p]),
     "kascade_calibrate_random_access": (_status, [_ctx_p, c_u64, c_u32, c_u32, P(ctypes.c_double)]),
     "kascade_rank_list_noalloc": (_status, [c_void_p, c_void_p, c_u64, c_void_p, c_void_p, c_void_p]),
+    "kascade_rank_batch": (
+        _status,
+        [_ctx_p, P(Segment), c_u32, c_void_p, c_void_p, c_u64, c_void_p, c_void_p, P(Opts), c_void_p],
+    ),
+    "kascade_ctx_set_size_classes": (_status, [_ctx_p, P(c_u64), P(c_u32), c_u32]),
+    "kascade_ctx_get_size_classes": (c_int, [_ctx_p, P(c_u64), P(c_u32), c_int]),
+    "kascade_server_config_init": (None, [P(ServerConfig)]),
+    "kascade_server_create": (_status, [P(ServerConfig), P(c_void_p)]),
+    "kascade_server_destroy": (_status, [c_void_p]),
+    "kascade_server_submit": (_status, [c_void_p, c_u32, c_void_p, c_void_p, c_u64, P(c_u64)]),
+    "kascade_server_submit_device": (_status, [c_void_p, c_u32, c_void_p, c_void_p, c_u64, P(c_u64)]),
+    "kascade_server_wait": (_status, [c_void_p, c_u64, ctypes.c_double]),
+    "kascade_server_result_device": (_status, [c_void_p, c_u64, P(c_void_p), P(c_void_p)]),
+    "kascade_server_fetch": (_status, [c_void_p, c_u64, c_void_p, c_void_p]),
+    "kascade_server_release": (_status, [c_void_p, c_u64]),
+    "kascade_server_get_stats": (_status, [c_void_p, P(ServerStats)]),
+    "kascade_server_reset_stats": (_status, [c_void_p]),
 }
 
 for _name, (_res, _args) in _SIGS.items():

@@ -16,7 +16,7 @@ from typing import Optional
 import numpy as np
 import torch
 
-from ._lib import KascadeError, Opts, check, lib
+from ._lib import KascadeError, Opts, Segment, ServerConfig, ServerStats, check, lib
 
 
 class Algorithm(IntEnum):
@@ -426,6 +426,192 @@ def unpack(succ_packed: torch.Tensor, rank_packed: torch.Tensor, succ_array: tor
     check(lib.kascade_unpack(c.handle, succ_packed.data_ptr(), rank_packed.data_ptr(), active_indices.data_ptr(),
                              active_indices.numel(), succ_array.data_ptr(), rank_array.data_ptr(),
                              succ_array.numel(), _stream(succ_array)), "kascade_unpack", c.handle)
+
+
+# ---------------------------------------------------------------------------
+# Batched ranking
+# ---------------------------------------------------------------------------
+SEG_LIST, SEG_FOREST = 0, 1
+
+
+def make_segments(sizes, kinds) -> "ctypes.Array":
+    """Segment table for instances of the given sizes and kinds (SEG_LIST /
+    SEG_FOREST), concatenated in order."""
+    arr = (Segment * len(sizes))()
+    off = 0
+    for i, (sz, kd) in enumerate(zip(sizes, kinds)):
+        arr[i].offset, arr[i].size, arr[i].kind, arr[i].reserved = off, int(sz), int(kd), 0
+        off += int(sz)
+    return arr
+
+
+def rank_batch(inputs: torch.Tensor, segments, weights: Optional[torch.Tensor] = None, *,
+               tuning: Optional[GpuTuning] = None, root_out: Optional[torch.Tensor] = None,
+               rank_out: Optional[torch.Tensor] = None, ctx: Optional[Context] = None):
+    """Rank many independent lists and forests at once (kascade_rank_batch).
+    `inputs` holds every instance's successor (list) or parent (forest) array,
+    concatenated, with instance-local indices; `segments` comes from
+    make_segments.  Returns (root, rank_or_depth), roots instance-local."""
+    _dev64(inputs, "inputs")
+    n = inputs.numel()
+    if weights is not None:
+        _dev32(weights, "weights")
+    root_out = root_out if root_out is not None else torch.empty(n, dtype=torch.int64, device=inputs.device)
+    rank_out = rank_out if rank_out is not None else torch.empty(n, dtype=torch.int64, device=inputs.device)
+    c = _ctx_for(inputs, ctx)
+    o = (tuning or GpuTuning()).to_opts()
+    check(lib.kascade_rank_batch(c.handle, segments, len(segments), inputs.data_ptr(),
+                                 weights.data_ptr() if weights is not None else None, n, root_out.data_ptr(),
+                                 rank_out.data_ptr(), ctypes.byref(o), _stream(inputs)), "kascade_rank_batch",
+          c.handle)
+    return root_out, rank_out
+
+
+def set_size_classes(ctx: Context, max_sizes, spacings) -> None:
+    """Install a size-class table (max instance size -> mean ruler spacing)."""
+    k = len(max_sizes)
+    ms = (ctypes.c_uint64 * k)(*[int(x) for x in max_sizes])
+    sp = (ctypes.c_uint32 * k)(*[int(x) for x in spacings])
+    check(lib.kascade_ctx_set_size_classes(ctx.handle, ms, sp, k), "kascade_ctx_set_size_classes", ctx.handle)
+
+
+def get_size_classes(ctx: Context):
+    ms = (ctypes.c_uint64 * 64)()
+    sp = (ctypes.c_uint32 * 64)()
+    k = lib.kascade_ctx_get_size_classes(ctx.handle, ms, sp, 64)
+    return [int(ms[i]) for i in range(k)], [int(sp[i]) for i in range(k)]
+
+
+def batch_sizes(count: int, seed: int, lo_log2: int = 6, hi_log2: int = 22, total: Optional[int] = None,
+                list_share: float = 0.7):
+    """Instance sizes log-uniform in [2^lo, 2^hi] (rescaled to sum to `total`
+    when given, never below 2^lo) and kinds (list with probability
+    list_share, else forest), from a seeded generator."""
+    rng = np.random.default_rng(seed)
+    sizes = np.floor(2.0 ** rng.uniform(lo_log2, hi_log2, count)).astype(np.int64)
+    if total:
+        sizes = np.maximum((sizes * (total / sizes.sum())).astype(np.int64), 1 << lo_log2)
+    kinds = np.where(rng.random(count) < list_share, SEG_LIST, SEG_FOREST)
+    return sizes, kinds
+
+
+def gen_batch(sizes, kinds, seed: int, device=None, wbits: int = 16):
+    """Concatenated seeded instances: lists in random order, forests of
+    random recursive trees (one tree per 2^16 vertices, at least one); plus
+    uint32 weights for the whole array."""
+    total = int(np.sum(sizes))
+    dev = device or "cuda"
+    out = torch.empty(total, dtype=torch.int64, device=dev)
+    off = 0
+    for i, (sz, kd) in enumerate(zip(sizes, kinds)):
+        sz = int(sz)
+        part = out[off:off + sz]
+        if kd == SEG_LIST:
+            gen_list(sz, seed + 7919 * i, LAYOUT_RANDOM, out=part)
+        else:
+            gen_forest(sz, seed + 7919 * i, FOREST_RRT, max(1, sz >> 16), 0, out=part)
+        off += sz
+    w = gen_weights(total, seed ^ 0x5A5A, wbits, device=dev)
+    return out, w
+
+
+# ---------------------------------------------------------------------------
+# Serving
+# ---------------------------------------------------------------------------
+class _DevView:
+    """A device array described by __cuda_array_interface__ (no copy)."""
+
+    def __init__(self, ptr: int, n: int):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<u8", "data": (ptr, False), "version": 3}
+
+
+class Server:
+    """The library's request loop (kascade_server_*): admission by HBM
+    footprint, device-resident inputs and results, two lanes of continuous
+    batching.  kind: SEG_LIST (successors, optional uint32 weights) or
+    SEG_FOREST (parents)."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 40 << 30, small_max: int = 1 << 20,
+                 small_batch_elements: int = 1 << 23, max_batch_elements: int = 1 << 28,
+                 max_batch_requests: int = 4096):
+        cfg = ServerConfig()
+        lib.kascade_server_config_init(ctypes.byref(cfg))
+        cfg.device = device
+        cfg.hbm_budget_bytes = hbm_budget
+        cfg.small_max = small_max
+        cfg.small_batch_elements = small_batch_elements
+        cfg.max_batch_elements = max_batch_elements
+        cfg.max_batch_requests = max_batch_requests
+        h = ctypes.c_void_p()
+        check(lib.kascade_server_create(ctypes.byref(cfg), ctypes.byref(h)), "kascade_server_create")
+        self.handle = h
+        self.device = device
+        self._n: dict[int, int] = {}
+
+    def submit(self, kind: int, inp, weights=None) -> int:
+        rid = ctypes.c_uint64(0)
+        if isinstance(inp, torch.Tensor):
+            _dev64(inp, "input")
+            w = weights
+            if w is not None:
+                _dev32(w, "weights")
+            st = lib.kascade_server_submit_device(self.handle, kind, inp.data_ptr(),
+                                                  w.data_ptr() if w is not None else None, inp.numel(),
+                                                  ctypes.byref(rid))
+            n = inp.numel()
+        else:
+            a = np.ascontiguousarray(inp, dtype=np.uint64)
+            w = None if weights is None else np.ascontiguousarray(weights, dtype=np.uint32)
+            st = lib.kascade_server_submit(self.handle, kind, a.ctypes.data, w.ctypes.data if w is not None else None,
+                                           a.size, ctypes.byref(rid))
+            n = a.size
+        check(st, "kascade_server_submit")
+        self._n[rid.value] = n
+        return rid.value
+
+    def wait(self, rid: int, timeout: float = -1.0) -> None:
+        check(lib.kascade_server_wait(self.handle, rid, timeout), "kascade_server_wait")
+
+    def fetch(self, rid: int):
+        n = self._n[rid]
+        root = np.empty(n, np.uint64)
+        rank = np.empty(n, np.uint64)
+        check(lib.kascade_server_fetch(self.handle, rid, root.ctypes.data, rank.ctypes.data), "kascade_server_fetch")
+        return root, rank
+
+    def result_device(self, rid: int):
+        """(root, rank) as CUDA tensors viewing the server's result buffers
+        (valid until release)."""
+        r, k = ctypes.c_void_p(), ctypes.c_void_p()
+        check(lib.kascade_server_result_device(self.handle, rid, ctypes.byref(r), ctypes.byref(k)),
+              "kascade_server_result_device")
+        n = self._n[rid]
+        dev = f"cuda:{self.device}"
+        return (torch.as_tensor(_DevView(r.value or 0, n), device=dev),
+                torch.as_tensor(_DevView(k.value or 0, n), device=dev))
+
+    def release(self, rid: int) -> None:
+        check(lib.kascade_server_release(self.handle, rid), "kascade_server_release")
+        self._n.pop(rid, None)
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        check(lib.kascade_server_get_stats(self.handle, ctypes.byref(st)), "kascade_server_get_stats")
+        return {f: getattr(st, f) for f, _ in ServerStats._fields_}
+
+    def reset_stats(self) -> None:
+        check(lib.kascade_server_reset_stats(self.handle), "kascade_server_reset_stats")
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            lib.kascade_server_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 # ---------------------------------------------------------------------------

@@ -23,6 +23,9 @@ kascade_status pack_impl(kascade_ctx& ctx, const uint64_t* succ, const int64_t* 
 kascade_status unpack_impl(kascade_ctx& ctx, const uint64_t* succ_packed, const int64_t* rank_packed,
                            const uint64_t* active, uint64_t k, uint64_t* succ, int64_t* rank, uint64_t n,
                            cudaStream_t s);
+kascade_status rank_batch_impl(kascade_ctx& ctx, const kascade_segment* segs, uint32_t nseg, const uint64_t* in,
+                               const uint32_t* weights, uint64_t total, uint64_t* root_out, uint64_t* rank_out,
+                               const kascade_opts* opts, cudaStream_t s);
 }  // namespace ks
 
 using namespace ks;
@@ -444,6 +447,39 @@ KASCADE_API kascade_status kascade_unpack(kascade_ctx* c, const uint64_t* succ_p
   KS_TRY(begin_call(c, s, nullptr));
   kascade_status st = unpack_impl(*c, succ_packed, rank_packed, active, k, succ, rank, n, s);
   return end_call(c, s, st, nullptr);
+}
+
+KASCADE_API kascade_status kascade_rank_batch(kascade_ctx* c, const kascade_segment* segs, uint32_t num_segs,
+                                              const uint64_t* input, const uint32_t* weights, uint64_t total_n,
+                                              uint64_t* root_out, uint64_t* rank_out, const kascade_opts* opts,
+                                              void* stream) {
+  cudaStream_t s = as_stream(stream);
+  if (total_n && (!segs || !num_segs || !input || !root_out || !rank_out)) return KASCADE_ERR_INVALID_ARG;
+  KS_TRY(begin_call(c, s, opts));
+  kascade_status st = rank_batch_impl(*c, segs, num_segs, input, weights, total_n, root_out, rank_out, opts, s);
+  return end_call(c, s, st, opts);
+}
+
+KASCADE_API kascade_status kascade_ctx_set_size_classes(kascade_ctx* c, const uint64_t* max_size,
+                                                        const uint32_t* spacing, uint32_t count) {
+  if (!c || !max_size || !spacing || count == 0 || count > 64) return KASCADE_ERR_INVALID_ARG;
+  for (uint32_t i = 0; i < count; ++i) {
+    if (spacing[i] < 2 || (i && max_size[i] <= max_size[i - 1])) return KASCADE_ERR_INVALID_ARG;
+  }
+  c->class_max.assign(max_size, max_size + count);
+  c->class_max.back() = ~0ull;
+  c->class_spacing.assign(spacing, spacing + count);
+  return KASCADE_OK;
+}
+
+KASCADE_API int kascade_ctx_get_size_classes(kascade_ctx* c, uint64_t* max_size, uint32_t* spacing, int cap) {
+  if (!c) return 0;
+  const int n = (int)c->class_max.size();
+  for (int i = 0; i < n && i < cap; ++i) {
+    if (max_size) max_size[i] = c->class_max[i];
+    if (spacing) spacing[i] = c->class_spacing[i];
+  }
+  return n;
 }
 
 KASCADE_API kascade_status kascade_gen_list(uint64_t n, uint64_t seed, uint32_t layout, uint64_t* succ, void* stream) {

@@ -45,6 +45,10 @@ struct kascade_ctx {
   cudaEvent_t done_event = nullptr;
   cudaStream_t last_stream = nullptr;
   bool async_pending = false;
+  // size classes: instances of at most class_max[i] elements use a mean ruler
+  // spacing of class_spacing[i] (set by the autotuner)
+  std::vector<unsigned long long> class_max{1ull << 10, 1ull << 16, 1ull << 22, ~0ull};
+  std::vector<uint32_t> class_spacing{8u, 16u, 32u, 48u};
 };
 
 namespace ks {

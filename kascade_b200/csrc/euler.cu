@@ -40,12 +40,51 @@ __global__ void __launch_bounds__(256) k_seg_bounds(const uint32_t* __restrict__
   }
 }
 
+// Where the records of a forest's tour live.  A single forest of n vertices:
+// up edge of v at slot v, down edge of sorted entry q at slot n + q.  A batch
+// of forests (compacted into one vertex space with per-forest bases fd[j]):
+// up edge of compact vertex c of forest j at that vertex's position in the
+// caller's concatenated arrays (foff[j] + c - fd[j]), down edges after all
+// input elements (down_base + q).  Ruler sampling thresholds can differ per
+// forest (size classes).
+struct SlotsSingle {
+  uint32_t n;
+  uint32_t th;
+  __device__ __forceinline__ uint32_t seg_of(uint32_t) const { return 0; }
+  __device__ __forceinline__ uint32_t up(uint32_t v, uint32_t) const { return v; }
+  __device__ __forceinline__ uint32_t down(uint64_t q) const { return n + (uint32_t)q; }
+  __device__ __forceinline__ uint32_t thresh(uint32_t) const { return th; }
+};
+
+struct SlotsBatch {
+  const uint32_t* fd;       // nf + 1 compact starts
+  const uint32_t* foff;     // nf concatenated offsets
+  const uint32_t* fthresh;  // nf sampling thresholds
+  uint32_t nf;
+  uint32_t down_base;
+  __device__ __forceinline__ uint32_t seg_of(uint32_t c) const {
+    uint32_t lo = 0, hi = nf;  // last j with fd[j] <= c
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (__ldg(fd + mid) <= c)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    return lo;
+  }
+  __device__ __forceinline__ uint32_t up(uint32_t c, uint32_t j) const { return c - __ldg(fd + j) + __ldg(foff + j); }
+  __device__ __forceinline__ uint32_t down(uint64_t q) const { return down_base + (uint32_t)q; }
+  __device__ __forceinline__ uint32_t thresh(uint32_t j) const { return __ldg(fthresh + j); }
+};
+
 // Writes both tour records of every sorted entry q, samples rulers among the
 // written slots and numbers them (one atomic per tile, as in prepare).
+template <class Slots>
 __global__ void __launch_bounds__(256) k_tour_build(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
                                                     uint32_t n, const uint2* __restrict__ seg, Rec* __restrict__ rec,
                                                     uint32_t* __restrict__ ruler_elem, uint32_t* __restrict__ counter,
-                                                    uint32_t salt, uint32_t thresh, DevStatus* st) {
+                                                    uint32_t salt, Slots slots, DevStatus* st) {
   __shared__ uint32_t sm[33];
   __shared__ uint32_t sbase;
   const uint64_t tile_sz = (uint64_t)blockDim.x * TB_ITEMS;
@@ -59,12 +98,15 @@ __global__ void __launch_bounds__(256) k_tour_build(const uint32_t* __restrict__
       su[i] = sd[i] = 0;
       if (q >= n) continue;
       const uint32_t p = keys[q], c = vals[q];
-      const uint32_t slot_down = n + (uint32_t)q;
+      const uint32_t j = slots.seg_of(p);  // p and c belong to the same forest
+      const uint32_t th = slots.thresh(j);
+      const uint32_t slot_down = slots.down(q);
       if (p == c) {
-        // root r = p: terminal slot r and the unused down slot, both self loops
+        // root r = p: terminal slot of r and the unused down slot, both self loops
+        const uint32_t slot_root = slots.up(p, j);
         ru[i].a = 0;
-        ru[i].b = p;
-        su[i] = p;
+        ru[i].b = slot_root;
+        su[i] = slot_root;
         rd[i].a = 0;
         rd[i].b = slot_down;
         sd[i] = slot_down;
@@ -74,14 +116,15 @@ __global__ void __launch_bounds__(256) k_tour_build(const uint32_t* __restrict__
         // up edge c -> p: continue with p's next child, else leave p
         uint64_t q1 = q + 1;
         if (q1 < n && keys[q1] == p && vals[q1] == p) q1++;
-        const uint32_t succ_up = (q1 < n && keys[q1] == p) ? n + (uint32_t)q1 : p;
+        const uint32_t succ_up = (q1 < n && keys[q1] == p) ? slots.down(q1) : slots.up(p, j);
+        const uint32_t slot_up = slots.up(c, j);
         ru[i].a = 1ull;
         ru[i].b = succ_up;
-        su[i] = c;
+        su[i] = slot_up;
         // down edge p -> c: descend to c's first child, else come back up
         const uint2 sg = seg[c];
         rd[i].a = ~0ull;  // -1
-        rd[i].b = (sg.x < sg.y) ? n + sg.x : c;
+        rd[i].b = (sg.x < sg.y) ? slots.down(sg.x) : slot_up;
         sd[i] = slot_down;
         // the down edge to a root's first child is the head of that tree's
         // tour: make it a ruler so that no tour element is left unreached
@@ -104,11 +147,11 @@ __global__ void __launch_bounds__(256) k_tour_build(const uint32_t* __restrict__
             head = (lo < sp.y && vals[lo] == p);
           }
         }
-        if (sampled(c, salt, thresh)) {
+        if (sampled(slot_up, salt, th)) {
           rl |= 1u << (2 * i);
           cnt++;
         }
-        if (head || sampled(slot_down, salt, thresh)) {
+        if (head || sampled(slot_down, salt, th)) {
           rl |= 2u << (2 * i);
           cnt++;
         }
@@ -245,15 +288,34 @@ kascade_status root_forest_impl(kascade_ctx& ctx, const uint64_t* parent, uint32
   {
     ProfScope ps(ctx, "tour_build", s);
     const unsigned grid = grid_for(ctx, ((uint64_t)n + 256 * TB_ITEMS - 1) / (256 * TB_ITEMS) * 256, 256, 8);
-    k_tour_build<<<grid, 256, 0, s>>>(keys, vals, n, seg, rec, ruler_elem, ctr, mix32(p.seed ^ 0x70757254u),
-                                      (uint32_t)(4294967296.0 / (double)(p.spacing0 < 2 ? 2 : p.spacing0)),
-                                      ctx.d_status);
+    SlotsSingle slots{n, (uint32_t)(4294967296.0 / (double)(p.spacing0 < 2 ? 2 : p.spacing0))};
+    k_tour_build<SlotsSingle><<<grid, 256, 0, s>>>(keys, vals, n, seg, rec, ruler_elem, ctr,
+                                                   mix32(p.seed ^ 0x70757254u), slots, ctx.d_status);
     KS_CHECK_LAUNCH();
   }
   uint32_t r = 0;
   KS_TRY(read_u32(ctx, ctr, &r, s));
   SinkTour sink{root_out, depth_out, n, keep_roots};
   return rank_records(ctx, rec, m, r, ruler_elem, sink, p, s);
+}
+
+// Tours of a batch of forests whose parents are given in one compact vertex
+// space (fpar[c] = compact parent of compact vertex c); records go to the
+// slots described by SlotsBatch, ruler ids continue `counter`.
+kascade_status batch_tours(kascade_ctx& ctx, const uint64_t* fpar, uint32_t F, const uint32_t* fd, const uint32_t* foff,
+                           const uint32_t* fthresh, uint32_t nf, uint32_t down_base, Rec* rec, uint32_t* ruler_elem,
+                           uint32_t* counter, uint32_t salt, cudaStream_t s) {
+  if (F == 0) return KASCADE_OK;
+  uint32_t *keys, *vals;
+  uint2* seg;
+  KS_TRY(sort_children(ctx, fpar, F, &keys, &vals, &seg, s));
+  SlotsBatch slots{fd, foff, fthresh, nf, down_base};
+  ProfScope ps(ctx, "tour_build", s);
+  const unsigned grid = grid_for(ctx, ((uint64_t)F + 256 * TB_ITEMS - 1) / (256 * TB_ITEMS) * 256, 256, 8);
+  k_tour_build<SlotsBatch><<<grid, 256, 0, s>>>(keys, vals, F, seg, rec, ruler_elem, counter, salt, slots,
+                                                ctx.d_status);
+  KS_CHECK_LAUNCH();
+  return KASCADE_OK;
 }
 
 kascade_status compute_euler_tour_impl(kascade_ctx& ctx, const uint64_t* parent, uint32_t n, uint64_t* tour,

@@ -572,14 +572,11 @@ kascade_status rank_deep(kascade_ctx& ctx, Rec* rec, uint32_t n, const uint32_t*
 // Public (library-internal) entry points
 // ---------------------------------------------------------------------------
 Params make_params(const kascade_ctx& ctx, const kascade_opts* o, uint64_t n) {
-  (void)ctx;
   Params p;
   // Spacing trades chase critical path (~ spacing * ln(n/spacing) hops)
   // against ruler-table size; these defaults are the tuned values for
   // random lists on B200 (see the autotune table in the batch path).
-  if (n <= (1u << 16)) p.spacing0 = 16;
-  else if (n <= (1u << 22)) p.spacing0 = 32;
-  else p.spacing0 = 48;
+  p.spacing0 = spacing_for(ctx, n);
   if (o) {
     if (o->ruler_spacing) p.spacing0 = o->ruler_spacing;
     if (o->ruler_spacing_deep) p.spacing_deep = o->ruler_spacing_deep;
@@ -710,7 +707,7 @@ kascade_status rank_records(kascade_ctx& ctx, Rec* rec, uint32_t n, uint32_t r0,
   if (n <= p.base_max) return launch_base(ctx, rec, n, nullptr, sink, s);
   if (p.algorithm != KASCADE_ALGO_SPARSE_RULING_SET || p.max_levels == 0 || (uint64_t)r0 * 10 > (uint64_t)n * 7)
     return pointer_double_records(ctx, rec, n, nullptr, sink, s);
-  if (n >= p.level0_log_min) {
+  if (Sink::kWriteFree && n >= p.level0_log_min) {
     const kascade_status st = rank_level0_log(ctx, rec, n, r0, ruler_elem0, sink.log_target(n), p, s);
     if (st != KASCADE_ERR_TIMEOUT) return st;
     // a chain exceeded the write-free path's hop cap (invalid input, or an
@@ -755,6 +752,10 @@ template kascade_status rank_records<SinkPlain>(kascade_ctx&, Rec*, uint32_t, ui
                                                 const Params&, cudaStream_t);
 template kascade_status rank_records<SinkTour>(kascade_ctx&, Rec*, uint32_t, uint32_t, uint32_t*, const SinkTour&,
                                                const Params&, cudaStream_t);
+template kascade_status rank_records<SinkBatch>(kascade_ctx&, Rec*, uint32_t, uint32_t, uint32_t*, const SinkBatch&,
+                                                const Params&, cudaStream_t);
+template kascade_status pointer_double_records<SinkBatch>(kascade_ctx&, const Rec*, uint32_t, const uint32_t*,
+                                                          const SinkBatch&, cudaStream_t);
 template kascade_status pointer_double_records<SinkPlain>(kascade_ctx&, const Rec*, uint32_t, const uint32_t*,
                                                           const SinkPlain&, cudaStream_t);
 template kascade_status pointer_double_records<SinkTour>(kascade_ctx&, const Rec*, uint32_t, const uint32_t*,

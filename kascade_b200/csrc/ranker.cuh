@@ -34,6 +34,9 @@ struct Params {
 
 Params make_params(const kascade_ctx& ctx, const kascade_opts* opts, uint64_t n);
 
+// Mean ruler spacing for an instance of n elements (the size-class table).
+uint32_t spacing_for(const kascade_ctx& ctx, uint64_t n);
+
 // Where results of level 0 go ------------------------------------------------
 // A sink receives, for element x, its rank, its root (level-0 index) and
 // whether x itself is a root.
@@ -50,6 +53,7 @@ struct LogTarget {
 // Plain arrays. keep_roots: leave root entries untouched (the reference's
 // in-place contract); otherwise roots get (x, 0).
 struct SinkPlain {
+  static constexpr bool kWriteFree = true;
   uint64_t* root;
   uint64_t* rank;
   int keep_roots;
@@ -72,6 +76,7 @@ struct SinkPlain {
 // Euler tour: elements 0..nv-1 are the vertices' up edges (roots: the tour's
 // terminal element), so only those produce output.
 struct SinkTour {
+  static constexpr bool kWriteFree = true;
   uint64_t* root;
   uint64_t* depth;
   uint32_t nv;
@@ -93,8 +98,41 @@ struct SinkTour {
   }
 };
 
+// A batch of independent instances concatenated into one index space:
+// roots are reported relative to their instance.  seg_off holds the nseg
+// instance offsets (non-decreasing), hint[k] the instance containing element
+// k * 4096.  Elements at or beyond `total` (tour down edges) give no output.
+struct SinkBatch {
+  static constexpr bool kWriteFree = false;
+  uint64_t* root;
+  uint64_t* rank;
+  uint32_t total;
+  const uint64_t* seg_off;
+  const uint32_t* hint;
+  uint32_t nseg;
+  uint32_t limit(uint32_t n) const { return n < total ? n : total; }
+  LogTarget log_target(uint32_t n) const { return LogTarget{root, rank, limit(n), 0, 0}; }
+  __device__ __forceinline__ uint64_t base_of(uint32_t x) const {
+    uint32_t j = __ldg(hint + (x >> 12));
+    while (j + 1 < nseg && __ldg(seg_off + j + 1) <= x) ++j;
+    return __ldg(seg_off + j);
+  }
+  __device__ __forceinline__ void put(uint32_t x, uint64_t rk, uint32_t rt, bool is_root) const {
+    if (x >= total) return;
+    const uint64_t b = base_of(x);
+    if (is_root) {
+      __stcs(root + x, (unsigned long long)(x - b));
+      __stcs(rank + x, 0ull);
+      return;
+    }
+    __stcs(root + x, (unsigned long long)(rt - b));
+    __stcs(rank + x, (unsigned long long)rk);
+  }
+};
+
 // Deeper levels write Out records.
 struct SinkOut {
+  static constexpr bool kWriteFree = false;
   Out* out;
   uint32_t limit(uint32_t n) const { return n; }
   __device__ __forceinline__ void put(uint32_t x, uint64_t rk, uint32_t rt, bool is_root) const {

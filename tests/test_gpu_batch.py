@@ -1,0 +1,87 @@
+"""Batched ranking of many lists and forests in one call, instance by
+instance against the oracle (bit-exact)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from gpu_util import DEEP, host_i64, host_u64
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def kb():
+    import kascade_b200
+
+    return kascade_b200
+
+
+def _check(kb, oracle_mod, inputs, w, sizes, kinds, root, rank):
+    inp = host_u64(inputs)
+    wh = w.cpu().numpy().view(np.uint32) if w is not None else None
+    r_all, k_all = host_u64(root), host_u64(rank)
+    off = 0
+    for i, (sz, kd) in enumerate(zip(sizes, kinds)):
+        sz = int(sz)
+        sl = slice(off, off + sz)
+        if kd == kb.SEG_LIST:
+            r_o, k_o = oracle_mod.rank_list(inp[sl], None if wh is None else wh[sl])
+        else:
+            r_o, k_o = oracle_mod.root_forest(inp[sl])
+        np.testing.assert_array_equal(r_all[sl], r_o, err_msg=f"instance {i} kind {kd} size {sz}")
+        np.testing.assert_array_equal(k_all[sl], k_o, err_msg=f"instance {i} kind {kd} size {sz}")
+        off += sz
+
+
+@pytest.mark.parametrize("tuning", [{}, DEEP, dict(base_case_size=64), dict(ruler_spacing=5)])
+@pytest.mark.parametrize("weighted", [False, True])
+def test_batch_mixed(kb, oracle_mod, tuning, weighted):
+    sizes, kinds = kb.batch_sizes(300, seed=7, lo_log2=0, hi_log2=14)
+    inputs, w = kb.gen_batch(sizes, kinds, seed=0xC3)
+    segs = kb.make_segments(sizes, kinds)
+    root, rank = kb.rank_batch(inputs, segs, w if weighted else None, tuning=kb.GpuTuning(**tuning))
+    _check(kb, oracle_mod, inputs, w if weighted else None, sizes, kinds, root, rank)
+
+
+def test_batch_large_instances(kb, oracle_mod):
+    sizes = np.array([1 << 20, 64, 3000, 1 << 19, 1, 2, 70000], np.int64)
+    kinds = np.array([0, 1, 0, 1, 1, 0, 0])
+    inputs, w = kb.gen_batch(sizes, kinds, seed=11)
+    segs = kb.make_segments(sizes, kinds)
+    root, rank = kb.rank_batch(inputs, segs, w)
+    _check(kb, oracle_mod, inputs, w, sizes, kinds, root, rank)
+
+
+def test_batch_only_lists_and_only_forests(kb, oracle_mod):
+    for kind in (0, 1):
+        sizes = np.array([5000, 1, 7, 20000, 333], np.int64)
+        kinds = np.full(sizes.size, kind)
+        inputs, w = kb.gen_batch(sizes, kinds, seed=13 + kind)
+        root, rank = kb.rank_batch(inputs, kb.make_segments(sizes, kinds), w)
+        _check(kb, oracle_mod, inputs, w, sizes, kinds, root, rank)
+
+
+def test_batch_size_classes_and_errors(kb, oracle_mod):
+    ctx = kb.Context()
+    kb.set_size_classes(ctx, [1 << 8, 1 << 12, 1 << 40], [4, 9, 40])
+    ms, sp = kb.get_size_classes(ctx)
+    assert sp == [4, 9, 40] and ms[-1] == (1 << 64) - 1
+    sizes, kinds = kb.batch_sizes(100, seed=3, lo_log2=2, hi_log2=13)
+    inputs, w = kb.gen_batch(sizes, kinds, seed=17)
+    root, rank = kb.rank_batch(inputs, kb.make_segments(sizes, kinds), w, ctx=ctx)
+    _check(kb, oracle_mod, inputs, w, sizes, kinds, root, rank)
+    # an instance-local index out of its instance
+    bad = inputs.clone()
+    bad[0] = int(sizes[0]) + 5
+    with pytest.raises(kb.KascadeError) as e:
+        kb.rank_batch(bad, kb.make_segments(sizes, kinds), w, ctx=ctx)
+    assert e.value.name == "OUT_OF_RANGE"
+    # a segment table that does not tile the input
+    segs = kb.make_segments(sizes, kinds)
+    segs[1].offset += 1
+    with pytest.raises(kb.KascadeError) as e:
+        kb.rank_batch(inputs, segs, w, ctx=ctx)
+    assert e.value.name == "INVALID_ARG"
+    ctx.close()
