@@ -259,7 +259,7 @@ def measure_batched(kb, ctx, dev, steps: int = 3) -> dict:
             "speedup_vs_plain": round(tp / tb, 2), "results_equal_plain": same}
 
 
-def measure_served(kb, dev, n_requests: int = 1000, rate: float = 20000.0) -> dict:
+def measure_served(kb, dev, n_requests: int = 1000, rate: float = 20000.0, **server_kw) -> dict:
     """Poisson arrivals (mean 20k req/s) of sizes
     log-uniform in [2^8, 2^24], 70% weighted lists / 30% random recursive
     forests, served under a 40 GB HBM budget with device-resident inputs;
@@ -274,36 +274,61 @@ def measure_served(kb, dev, n_requests: int = 1000, rate: float = 20000.0) -> di
     inputs, w = kb.gen_batch(sizes, kinds, seed=0xC4, device=dev)
     offs = np.concatenate([[0], np.cumsum(sizes)])
     torch.cuda.synchronize()
-    srv = kb.Server(device=dev.index or 0, hbm_budget=40 << 30, small_max=1 << 20, small_batch_elements=1 << 23)
+    kw = dict(hbm_budget=40 << 30, small_max=1 << 20, small_batch_elements=1 << 23)
+    kw.update(server_kw)
+    srv = kb.Server(device=dev.index or 0, **kw)
     # warm the lanes once
     wid = srv.submit(int(kinds[0]), inputs[0:int(sizes[0])], w[0:int(sizes[0])] if kinds[0] == kb.SEG_LIST else None)
     srv.wait(wid, 60.0)
     srv.release(wid)
     srv.reset_stats()
-    ids = []
+    import queue
+    import threading
+
+    ids = [None] * n_requests
+    done_q: "queue.Queue" = queue.Queue()
+    check_at = {0, n_requests // 2, n_requests - 1}
+    checks = {}
+    errors = []
+
+    def collector():
+        # waits in submission order and releases each result once read, so
+        # the budget holds only requests in flight
+        for i in range(n_requests):
+            rid = done_q.get()
+            try:
+                srv.wait(rid, 300.0)
+                if i in check_at:
+                    r_dev, k_dev = srv.result_device(rid)
+                    checks[i] = (r_dev.clone(), k_dev.clone())
+                srv.release(rid)
+            except Exception as e:  # noqa: BLE001
+                errors.append(e)
+
+    th = threading.Thread(target=collector, daemon=True)
+    th.start()
     t0 = time.perf_counter()
     for i in range(n_requests):
         delay = t0 + arrivals[i] - time.perf_counter()
         if delay > 0:
             time.sleep(delay)
         a, b = int(offs[i]), int(offs[i + 1])
-        ids.append(srv.submit(int(kinds[i]), inputs[a:b], w[a:b] if kinds[i] == kb.SEG_LIST else None))
-    for rid in ids:
-        srv.wait(rid, 300.0)
+        ids[i] = srv.submit(int(kinds[i]), inputs[a:b], w[a:b] if kinds[i] == kb.SEG_LIST else None)
+        done_q.put(ids[i])
+    th.join(timeout=600.0)
+    if th.is_alive() or errors:
+        raise RuntimeError(f"served run did not complete: {errors[:1]}")
     st = srv.stats()
+    srv.close()
     # spot-check three results against plain calls
     ok = True
-    for i in (0, n_requests // 2, n_requests - 1):
+    for i, (r_dev, k_dev) in checks.items():
         a, b = int(offs[i]), int(offs[i + 1])
-        r_dev, k_dev = srv.result_device(ids[i])
         if kinds[i] == kb.SEG_LIST:
             r_p, k_p = kb.rank_list(inputs[a:b], w[a:b])
         else:
             r_p, k_p = kb.root_forest(inputs[a:b])
         ok &= bool(torch.equal(r_dev.view(torch.int64), r_p) and torch.equal(k_dev.view(torch.int64), k_p))
-    for rid in ids:
-        srv.release(rid)
-    srv.close()
     # plain per-request calls of the same requests, back to back
     ctx = kb.Context(dev.index or 0)
     root = torch.empty(int(sizes.max()), dtype=torch.int64, device=dev)
@@ -329,7 +354,8 @@ def measure_served(kb, dev, n_requests: int = 1000, rate: float = 20000.0) -> di
             "p50_ms_le_2^20": round(st["p50_small_ms"], 3), "p99_ms_le_2^20": round(st["p99_small_ms"], 3),
             "requests_le_2^20": int(st["completed_small"]), "batches": int(st["batches"]),
             "plain_elements_per_s": total / tp, "plain_req_per_s": round(n_requests / tp, 1),
-            "throughput_vs_plain": round(st["elements_per_s"] / (total / tp), 2), "spot_check_equal": ok}
+            "throughput_vs_plain": round(st["elements_per_s"] / (total / tp), 2), "spot_check_equal": ok,
+            "lanes": {k: st[k] for k in ("lane_batches", "lane_elements", "lane_busy_ms", "lane_max_batch_ms")}}
 
 
 def run_reference(args, world, rank):

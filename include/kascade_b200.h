@@ -264,6 +264,10 @@ KASCADE_API kascade_status kascade_ctx_set_size_classes(kascade_ctx* ctx, const 
                                                         const uint32_t* spacing, uint32_t count);
 KASCADE_API int kascade_ctx_get_size_classes(kascade_ctx* ctx, uint64_t* max_size, uint32_t* spacing,
                                              int cap);
+/* Size this context's grids for `sms` SMs (0 = all SMs): its persistent and
+ * grid-stride kernels then hold that many SMs' worth of block slots, and
+ * work on other streams (the server's latency lane) finds the rest free. */
+KASCADE_API kascade_status kascade_ctx_set_sm_budget(kascade_ctx* ctx, int sms);
 
 /* ----------------------------------------------------------------------------
  * Serving: a request loop over the batched ranker (no counterpart in the
@@ -280,10 +284,16 @@ typedef struct kascade_server_config {
   uint64_t hbm_budget_bytes;     /* admission budget (default 40 GiB)             */
   uint32_t max_batch_requests;   /* requests per batch (default 4096)             */
   uint32_t reserved;
-  uint64_t max_batch_elements;   /* elements per batch, large lane (default 2^28) */
+  uint64_t max_batch_elements;   /* elements per batch, large lane (default 2^26) */
   uint64_t small_max;            /* latency lane: requests up to this many
                                     elements (default 2^20)                       */
   uint64_t small_batch_elements; /* elements per batch, latency lane (2^23)       */
+  uint32_t latency_sms;          /* SMs the throughput lane's persistent kernels
+                                    leave free for the latency lane (default 16)  */
+  uint32_t reserved2;
+  uint64_t result_heap_bytes;    /* device memory set aside at creation for
+                                    results (default hbm_budget_bytes / 2); a
+                                    batch that finds no room there allocates   */
 } kascade_server_config;
 
 typedef struct kascade_server_stats {
@@ -297,6 +307,11 @@ typedef struct kascade_server_stats {
                                         first submission)                         */
   double requests_per_s;
   uint64_t bytes_in_use;
+  /* per lane (0 latency, 1 throughput) */
+  uint64_t lane_batches[2];
+  uint64_t lane_elements[2];
+  double lane_busy_ms[2];      /* wall time spent running batches              */
+  double lane_max_batch_ms[2]; /* longest batch                                */
 } kascade_server_stats;
 
 KASCADE_API void kascade_server_config_init(kascade_server_config* cfg);
@@ -307,8 +322,12 @@ KASCADE_API kascade_status kascade_server_destroy(kascade_server* server);
  * not fit the budget yet waits in arrival order. */
 KASCADE_API kascade_status kascade_server_submit(kascade_server* server, uint32_t kind, const uint64_t* input,
                                                  const uint32_t* weights, uint64_t n, uint64_t* request_id);
-/* The same for input already in device memory (copied into the server's own
- * buffers on admission; blocks while the budget is exhausted). */
+/* The same for input already in device memory: it is copied into the
+ * server's batch buffer when its batch runs, so it must stay valid until the
+ * request completes.  A request holds its whole footprint while it waits or
+ * runs and only its result bytes (16 per element) from completion until
+ * release.  Requests up to small_max elements may pass larger ones that wait
+ * for memory. */
 KASCADE_API kascade_status kascade_server_submit_device(kascade_server* server, uint32_t kind,
                                                         const uint64_t* input, const uint32_t* weights,
                                                         uint64_t n, uint64_t* request_id);
@@ -320,7 +339,9 @@ KASCADE_API kascade_status kascade_server_result_device(kascade_server* server, 
 /* Copy a completed request's results to host buffers of n entries. */
 KASCADE_API kascade_status kascade_server_fetch(kascade_server* server, uint64_t request_id,
                                                 uint64_t* root_out, uint64_t* rank_out);
-/* Drop a completed request and its device results. */
+/* Drop a completed request and its device results.  The result memory is
+ * reused by later batches at once: device work that reads the pointers from
+ * kascade_server_result_device must have finished before this call. */
 KASCADE_API kascade_status kascade_server_release(kascade_server* server, uint64_t request_id);
 KASCADE_API kascade_status kascade_server_get_stats(kascade_server* server, kascade_server_stats* out);
 KASCADE_API kascade_status kascade_server_reset_stats(kascade_server* server);

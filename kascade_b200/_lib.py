@@ -40,7 +40,8 @@ class ServerConfig(ctypes.Structure):
 
     _fields_ = [("struct_size", c_u32), ("device", c_int), ("hbm_budget_bytes", c_u64),
                 ("max_batch_requests", c_u32), ("reserved", c_u32), ("max_batch_elements", c_u64),
-                ("small_max", c_u64), ("small_batch_elements", c_u64)]
+                ("small_max", c_u64), ("small_batch_elements", c_u64), ("latency_sms", c_u32),
+                ("reserved2", c_u32), ("result_heap_bytes", c_u64)]
 
 
 class ServerStats(ctypes.Structure):
@@ -49,7 +50,9 @@ class ServerStats(ctypes.Structure):
     _fields_ = [("completed", c_u64), ("completed_small", c_u64), ("batches", c_u64), ("elements", c_u64),
                 ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double), ("p50_small_ms", ctypes.c_double),
                 ("p99_small_ms", ctypes.c_double), ("elements_per_s", ctypes.c_double),
-                ("requests_per_s", ctypes.c_double), ("bytes_in_use", c_u64)]
+                ("requests_per_s", ctypes.c_double), ("bytes_in_use", c_u64), ("lane_batches", c_u64 * 2),
+                ("lane_elements", c_u64 * 2), ("lane_busy_ms", ctypes.c_double * 2),
+                ("lane_max_batch_ms", ctypes.c_double * 2)]
 
 
 class Opts(ctypes.Structure):
@@ -138,6 +141,7 @@ _SIGS = {
     ),
     "kascade_ctx_set_size_classes": (_status, [_ctx_p, P(c_u64), P(c_u32), c_u32]),
     "kascade_ctx_get_size_classes": (c_int, [_ctx_p, P(c_u64), P(c_u32), c_int]),
+    "kascade_ctx_set_sm_budget": (_status, [_ctx_p, c_int]),
     "kascade_server_config_init": (None, [P(ServerConfig)]),
     "kascade_server_create": (_status, [P(ServerConfig), P(c_void_p)]),
     "kascade_server_destroy": (_status, [c_void_p]),

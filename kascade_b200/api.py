@@ -532,8 +532,8 @@ class Server:
     SEG_FOREST (parents)."""
 
     def __init__(self, device: int = 0, hbm_budget: int = 40 << 30, small_max: int = 1 << 20,
-                 small_batch_elements: int = 1 << 23, max_batch_elements: int = 1 << 28,
-                 max_batch_requests: int = 4096):
+                 small_batch_elements: int = 1 << 23, max_batch_elements: int = 1 << 26,
+                 max_batch_requests: int = 4096, latency_sms: int = 16):
         cfg = ServerConfig()
         lib.kascade_server_config_init(ctypes.byref(cfg))
         cfg.device = device
@@ -542,11 +542,13 @@ class Server:
         cfg.small_batch_elements = small_batch_elements
         cfg.max_batch_elements = max_batch_elements
         cfg.max_batch_requests = max_batch_requests
+        cfg.latency_sms = latency_sms
         h = ctypes.c_void_p()
         check(lib.kascade_server_create(ctypes.byref(cfg), ctypes.byref(h)), "kascade_server_create")
         self.handle = h
         self.device = device
         self._n: dict[int, int] = {}
+        self._viewed: set[int] = set()
 
     def submit(self, kind: int, inp, weights=None) -> int:
         rid = ctypes.c_uint64(0)
@@ -587,17 +589,28 @@ class Server:
               "kascade_server_result_device")
         n = self._n[rid]
         dev = f"cuda:{self.device}"
+        self._viewed.add(rid)
         return (torch.as_tensor(_DevView(r.value or 0, n), device=dev),
                 torch.as_tensor(_DevView(k.value or 0, n), device=dev))
 
     def release(self, rid: int) -> None:
+        """Drop a completed request.  Its result memory is reused by later
+        batches at once, so work queued on the views from result_device must
+        finish first: the current stream is synchronised for such requests."""
+        if rid in self._viewed:
+            torch.cuda.current_stream(self.device).synchronize()
+            self._viewed.discard(rid)
         check(lib.kascade_server_release(self.handle, rid), "kascade_server_release")
         self._n.pop(rid, None)
 
     def stats(self) -> dict:
         st = ServerStats()
         check(lib.kascade_server_get_stats(self.handle, ctypes.byref(st)), "kascade_server_get_stats")
-        return {f: getattr(st, f) for f, _ in ServerStats._fields_}
+        out = {}
+        for f, _ in ServerStats._fields_:
+            v = getattr(st, f)
+            out[f] = list(v) if isinstance(v, ctypes.Array) else v
+        return out
 
     def reset_stats(self) -> None:
         check(lib.kascade_server_reset_stats(self.handle), "kascade_server_reset_stats")

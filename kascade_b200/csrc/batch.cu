@@ -217,7 +217,7 @@ kascade_status rank_batch_impl(kascade_ctx& ctx, const kascade_segment* segs, ui
   const uint32_t salt = mix32(p.seed ^ 0x62617463u);
   {
     ProfScope ps(ctx, "batch_prepare", s);
-    const unsigned grid = (unsigned)std::min<uint64_t>(items.size(), (uint64_t)ctx.sm_count * 8);
+    const unsigned grid = (unsigned)std::min<uint64_t>(items.size(), (uint64_t)ctx.usable_sms() * 8);
     if (weights)
       k_batch_prepare<BWU32><<<grid, BP_THREADS, 0, s>>>(d_items, (uint32_t)items.size(), d_segs, in, BWU32{weights},
                                                          rec, fpar, ruler_elem, ctr, salt, ctx.d_status);

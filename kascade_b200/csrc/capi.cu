@@ -472,6 +472,12 @@ KASCADE_API kascade_status kascade_ctx_set_size_classes(kascade_ctx* c, const ui
   return KASCADE_OK;
 }
 
+KASCADE_API kascade_status kascade_ctx_set_sm_budget(kascade_ctx* c, int sms) {
+  if (!c || sms < 0) return KASCADE_ERR_INVALID_ARG;
+  c->sm_budget = sms;
+  return KASCADE_OK;
+}
+
 KASCADE_API int kascade_ctx_get_size_classes(kascade_ctx* c, uint64_t* max_size, uint32_t* spacing, int cap) {
   if (!c) return 0;
   const int n = (int)c->class_max.size();

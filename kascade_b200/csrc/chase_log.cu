@@ -410,7 +410,7 @@ unsigned chase_grid(const kascade_ctx& ctx, uint32_t r) {
     }
     g_chase_occ[C] = nb < 1 ? 1 : nb;
   }
-  unsigned grid = (unsigned)(ctx.sm_count * g_chase_occ[C]);
+  unsigned grid = (unsigned)(ctx.usable_sms() * g_chase_occ[C]);
   const uint64_t need = ((uint64_t)r + 32ull * C - 1) / (32ull * C);
   const uint64_t need_blocks = (need + 7) / 8;
   if (need_blocks < grid) grid = (unsigned)(need_blocks ? need_blocks : 1);
@@ -471,7 +471,7 @@ kascade_status rank_level0_log(kascade_ctx& ctx, const Rec* rec, uint32_t n, uin
   KS_CUDA(cudaMemsetAsync(bcursor, 0, sizeof(uint32_t) * (nb ? nb : 1) * CURSOR_STRIDE, s));
   {
     ProfScope ps(ctx, "resolve", s);
-    const unsigned g = (unsigned)std::min<uint64_t>(nchunks, (uint64_t)ctx.sm_count * 8);
+    const unsigned g = (unsigned)std::min<uint64_t>(nchunks, (uint64_t)ctx.usable_sms() * 8);
     const size_t smem = 2 * sizeof(uint32_t) * (nb ? nb : 1);
     if (smem > 48 * 1024) {
       static bool raised = false;
@@ -500,7 +500,7 @@ kascade_status rank_level0_log(kascade_ctx& ctx, const Rec* rec, uint32_t n, uin
   }
   {
     ProfScope ps(ctx, "scatter", s);
-    k_scatter<<<ctx.sm_count * 8, 256, 0, s>>>(part, bcursor, nb, scatter_work, t.root, t.rank, flags);
+    k_scatter<<<ctx.usable_sms() * 8, 256, 0, s>>>(part, bcursor, nb, scatter_work, t.root, t.rank, flags);
     KS_CHECK_LAUNCH();
   }
   if (need_heads) {
@@ -511,7 +511,7 @@ kascade_status rank_level0_log(kascade_ctx& ctx, const Rec* rec, uint32_t n, uin
     const uint64_t groups = ((uint64_t)n + 15) / 16;
     k_find_unreached<<<grid_for(ctx, groups, 256, 8), 256, 0, s>>>(flags, n, ulist, ucount, ucap, ctx.d_status);
     KS_CHECK_LAUNCH();
-    k_walk_unreached<<<ctx.sm_count * 4, 256, 0, s>>>(rec, flags, ulist, ucount, ucap, n, t.root, t.rank,
+    k_walk_unreached<<<ctx.usable_sms() * 4, 256, 0, s>>>(rec, flags, ulist, ucount, ucap, n, t.root, t.rank,
                                                       ctx.d_status);
     KS_CHECK_LAUNCH();
   }

@@ -49,6 +49,11 @@ struct kascade_ctx {
   // spacing of class_spacing[i] (set by the autotuner)
   std::vector<unsigned long long> class_max{1ull << 10, 1ull << 16, 1ull << 22, ~0ull};
   std::vector<uint32_t> class_spacing{8u, 16u, 32u, 48u};
+  // SMs' worth of block slots this context's kernels may occupy (0 = all):
+  // grids are sized for this many SMs, so that work on other streams (a
+  // server's latency lane) always finds free slots
+  int sm_budget = 0;
+  int usable_sms() const { return (sm_budget > 0 && sm_budget < sm_count) ? sm_budget : sm_count; }
 };
 
 namespace ks {
@@ -84,7 +89,7 @@ struct ProfScope {
 
 inline unsigned grid_for(const kascade_ctx& ctx, uint64_t work, unsigned block, unsigned per_sm_cap) {
   uint64_t g = (work + block - 1) / block;
-  uint64_t cap = (uint64_t)ctx.sm_count * per_sm_cap;
+  uint64_t cap = (uint64_t)ctx.usable_sms() * per_sm_cap;
   if (g > cap) g = cap;
   if (g == 0) g = 1;
   return (unsigned)g;

@@ -511,7 +511,7 @@ kascade_status launch_chase_c(kascade_ctx& ctx, Rec* rec, uint32_t n, const uint
                               Rec* rec_next, uint32_t* work, cudaStream_t s) {
   static int occ = -1;
   if (occ < 0) occ = occupancy(k_chase<C>, 256, 0);
-  unsigned grid = (unsigned)(ctx.sm_count * occ);
+  unsigned grid = (unsigned)(ctx.usable_sms() * occ);
   uint64_t need = ((uint64_t)r + 32ull * C - 1) / (32ull * C);  // warps worth of work
   uint64_t need_blocks = (need + 7) / 8;
   if (need_blocks < grid) grid = (unsigned)(need_blocks ? need_blocks : 1);

@@ -1,17 +1,25 @@
 // Serving: a request loop over the batched ranker.
 //
 //  - submit: a request (list ranking or tree rooting, host or device input)
-//    is admitted when its HBM footprint fits the budget; admission copies its
-//    input to the device, where input and result stay until released.
-//    Requests that do not fit wait in arrival order and are admitted as
-//    memory frees up.
+//    is admitted when its HBM footprint fits the budget.  Requests that do
+//    not fit wait in arrival order and are admitted as memory frees up;
+//    requests for the latency lane may pass larger ones that wait.  Host
+//    inputs are held in host memory until their batch runs; the lane copies
+//    every input of a batch straight into the batch's concatenated buffer.
 //  - lanes: each lane is a worker thread with its own library context and
 //    CUDA stream.  A lane takes every admitted request of its class that is
 //    waiting when it becomes free (continuous batching), gathers their inputs
 //    into one concatenated buffer and ranks them with one kascade_rank_batch
 //    call.  Lane 0 serves requests up to `small_max` elements (the latency
 //    lane, small batches, higher stream priority), lane 1 the larger ones;
-//    both lanes' batches run concurrently on the device.
+//    both lanes' batches run concurrently on the device, and lane 1's
+//    persistent kernels leave `latency_sms` SMs free for lane 0.
+//  - memory: nothing is allocated per batch on the normal path.  Each lane
+//    stages its batch input in buffers sized for a full batch, and results
+//    go to a result heap set aside at creation (first fit, coalescing free
+//    list kept on the host).  Only a request larger than a lane's batch limit,
+//    or a batch that finds no room in the heap, allocates from the server's
+//    memory pool (pool growth can stall the device for milliseconds).
 //  - results: each request's root and rank live in its batch's output
 //    buffers until the request is released.
 //  - stats: per-request latency (submit to completion), p50 / p99, throughput.
@@ -19,8 +27,11 @@
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <thread>
@@ -35,24 +46,67 @@ using Clock = std::chrono::steady_clock;
 
 double now_s() { return std::chrono::duration<double>(Clock::now().time_since_epoch()).count(); }
 
+constexpr uint64_t NO_CHUNK = ~0ull;
+
 struct BatchBuf {
-  uint64_t* d_in = nullptr;
-  uint32_t* d_w = nullptr;
-  uint64_t* d_root = nullptr;
+  uint64_t* d_root = nullptr;  // results: root, then rank, in one chunk
   uint64_t* d_rank = nullptr;
   uint64_t n = 0;
-  uint64_t bytes = 0;
+  uint64_t heap_off = NO_CHUNK;  // offset in the result heap, or pool memory
+  uint64_t heap_bytes = 0;
   int refs = 0;
+};
+
+// First-fit allocator over one device range, with coalescing on free.
+struct ResultHeap {
+  char* base = nullptr;
+  uint64_t size = 0;
+  std::map<uint64_t, uint64_t> free_blocks;  // offset -> bytes
+
+  void init(char* p, uint64_t bytes) {
+    base = p;
+    size = bytes;
+    free_blocks.clear();
+    if (bytes) free_blocks.emplace(0, bytes);
+  }
+  uint64_t alloc(uint64_t bytes) {
+    bytes = (bytes + 255) & ~255ull;
+    for (auto it = free_blocks.begin(); it != free_blocks.end(); ++it) {
+      if (it->second < bytes) continue;
+      const uint64_t off = it->first, left = it->second - bytes;
+      free_blocks.erase(it);
+      if (left) free_blocks.emplace(off + bytes, left);
+      return off;
+    }
+    return NO_CHUNK;
+  }
+  void release(uint64_t off, uint64_t bytes) {
+    bytes = (bytes + 255) & ~255ull;
+    auto it = free_blocks.emplace(off, bytes).first;
+    auto nx = std::next(it);
+    if (nx != free_blocks.end() && it->first + it->second == nx->first) {
+      it->second += nx->second;
+      free_blocks.erase(nx);
+    }
+    if (it != free_blocks.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first) {
+        pv->second += it->second;
+        free_blocks.erase(it);
+      }
+    }
+  }
 };
 
 struct Request {
   uint64_t id = 0;
   uint32_t kind = 0;
   uint64_t n = 0;
-  uint64_t* d_in = nullptr;  // owned until the request runs
-  uint32_t* d_w = nullptr;
-  std::vector<uint64_t> h_in;  // host submissions wait here until admitted
+  std::vector<uint64_t> h_in;  // host submissions wait here until their batch runs
   std::vector<uint32_t> h_w;
+  const uint64_t* src_in = nullptr;  // device submissions: copied from here when the batch runs
+  const uint32_t* src_w = nullptr;
+  uint64_t result_bytes = 0;  // the share of the footprint held until release
   bool has_w = false;
   bool admitted = false;
   int state = 0;  // 0 waiting for memory, 1 admitted, 2 running, 3 done, 4 failed
@@ -79,6 +133,14 @@ uint64_t footprint_of(uint32_t kind, uint64_t n, bool w) {
 
 }  // namespace
 
+// One finished batch, for the optional trace (KASCADE_SERVER_TRACE=<file>).
+struct BatchTrace {
+  int lane;
+  uint32_t requests;
+  uint64_t elements;
+  double t_start, t_alloc, t_gathered, t_end;
+};
+
 struct kascade_server {
   kascade_server_config cfg{};
   std::mutex mu;
@@ -91,60 +153,77 @@ struct kascade_server {
   uint64_t bytes_in_use = 0;
   uint64_t elements_done = 0;
   uint64_t batches = 0;
+  uint64_t lane_batches[2] = {0, 0}, lane_elements[2] = {0, 0};
+  double lane_busy[2] = {0, 0}, lane_max[2] = {0, 0};
   double t_first_submit = 0, t_last_done = 0;
   bool stop = false;
   struct Lane {
     kascade_ctx* ctx = nullptr;
     cudaStream_t stream = nullptr;
     std::thread th;
+    uint64_t* d_in = nullptr;  // staging for a full batch
+    uint32_t* d_w = nullptr;
+    uint64_t cap = 0;
   };
   Lane lanes[2];
   cudaStream_t copy_stream = nullptr;
+  // batch buffers come from a pool that keeps freed memory (no release to
+  // the driver, hence no device-wide synchronisation on reuse)
+  cudaMemPool_t pool = nullptr;
+  ResultHeap heap;
+
+  std::vector<BatchTrace> trace;
+  bool tracing = false;
 
   void admit_locked();
   void lane_loop(int lane);
-  kascade_status admit_one(Request* r);
+  kascade_status warm_lane(int lane, uint64_t n_list, uint64_t n_forest);
 };
 
-// Copy a request's input to the device (caller holds no lock).
-kascade_status kascade_server::admit_one(Request* r) {
-  cudaSetDevice(cfg.device);
-  const size_t in_bytes = r->n * sizeof(uint64_t), w_bytes = r->n * sizeof(uint32_t);
-  if (cudaMallocAsync(reinterpret_cast<void**>(&r->d_in), in_bytes ? in_bytes : 8, copy_stream) != cudaSuccess)
-    return cudaGetLastError(), KASCADE_ERR_OOM;
-  if (r->has_w &&
-      cudaMallocAsync(reinterpret_cast<void**>(&r->d_w), w_bytes ? w_bytes : 8, copy_stream) != cudaSuccess)
-    return cudaGetLastError(), KASCADE_ERR_OOM;
-  if (!r->h_in.empty()) {
-    if (cudaMemcpyAsync(r->d_in, r->h_in.data(), in_bytes, cudaMemcpyHostToDevice, copy_stream) != cudaSuccess)
-      return cudaGetLastError(), KASCADE_ERR_CUDA;
-    if (r->has_w &&
-        cudaMemcpyAsync(r->d_w, r->h_w.data(), w_bytes, cudaMemcpyHostToDevice, copy_stream) != cudaSuccess)
-      return cudaGetLastError(), KASCADE_ERR_CUDA;
+// Run one synthetic batch (a list and a forest) on a lane before serving, so
+// that the first requests pay for no kernel loading and no pool growth.
+kascade_status kascade_server::warm_lane(int lane, uint64_t n_list, uint64_t n_forest) {
+  Lane& L = lanes[lane];
+  const uint64_t n = n_list + n_forest;
+  if (n > L.cap || 16 * n > heap.size) return KASCADE_OK;  // nothing to warm with
+  uint64_t* in = L.d_in;
+  uint32_t* w = L.d_w;
+  uint64_t* root = reinterpret_cast<uint64_t*>(heap.base);
+  uint64_t* rank = root + n;
+  kascade_status st = KASCADE_OK;
+  if (st == KASCADE_OK) st = kascade_gen_list(n_list, 0x5e7e, 0, in, L.stream);
+  if (st == KASCADE_OK) st = kascade_gen_weights(n, 0x5e7e, 16, w, L.stream);
+  if (st == KASCADE_OK) st = kascade_gen_forest(n_forest, 0x5e7e, 0, 16, 0, in + n_list, L.stream);
+  if (st == KASCADE_OK) {
+    kascade_segment segs[2] = {{0, n_list, KASCADE_SEG_LIST, 0}, {n_list, n_forest, KASCADE_SEG_FOREST, 0}};
+    kascade_opts o;
+    kascade_opts_init(&o);
+    st = kascade_rank_batch(L.ctx, segs, 2, in, w, n, root, rank, &o, L.stream);
   }
-  if (cudaStreamSynchronize(copy_stream) != cudaSuccess) return cudaGetLastError(), KASCADE_ERR_CUDA;
-  std::vector<uint64_t>().swap(r->h_in);
-  std::vector<uint32_t>().swap(r->h_w);
-  return KASCADE_OK;
+  if (cudaStreamSynchronize(L.stream) != cudaSuccess && st == KASCADE_OK) st = KASCADE_ERR_CUDA;
+  cudaGetLastError();
+  return st;
 }
 
-// Admit waiting host requests in arrival order while they fit the budget.
+// Admit waiting requests while they fit the budget: arrival order, except
+// that requests for the latency lane may pass larger ones that do not fit
+// yet.  Admission is accounting only; the lane copies the input when it runs.
 void kascade_server::admit_locked() {
-  while (!waiting.empty()) {
-    Request* r = waiting.front();
-    if (bytes_in_use + r->footprint > cfg.hbm_budget_bytes && bytes_in_use > 0) break;
-    waiting.pop_front();
-    bytes_in_use += r->footprint;
-    mu.unlock();
-    kascade_status st = admit_one(r);
-    mu.lock();
-    if (st != KASCADE_OK) {
-      r->state = 4;
-      r->status = st;
-      bytes_in_use -= r->footprint;
-      cv_done.notify_all();
+  bool blocked_large = false;
+  for (auto it = waiting.begin(); it != waiting.end();) {
+    Request* r = *it;
+    const bool small = r->n <= cfg.small_max;
+    if (blocked_large && !small) {
+      ++it;
       continue;
     }
+    if (bytes_in_use + r->footprint > cfg.hbm_budget_bytes && bytes_in_use > 0) {
+      if (!small) blocked_large = true;
+      ++it;
+      continue;
+    }
+    it = waiting.erase(it);
+    bytes_in_use += r->footprint;
     r->admitted = true;
     r->state = 1;
     ready.push_back(r);
@@ -184,38 +263,58 @@ void kascade_server::lane_loop(int lane) {
       if (stop) break;
       continue;
     }
-    lk.unlock();
-    // gather into one concatenated batch and rank it
     const double t0 = now_s();
     auto b = std::make_shared<BatchBuf>();
     b->n = elems;
+    b->heap_bytes = 16 * elems;
+    b->heap_off = heap.alloc(b->heap_bytes);
+    lk.unlock();
+    // gather into one concatenated batch and rank it
     bool any_w = false;
     for (Request* r : take) any_w |= r->has_w;
     kascade_status st = KASCADE_OK;
-    if (cudaMallocAsync(reinterpret_cast<void**>(&b->d_in), elems * 8, L.stream) != cudaSuccess ||
-        cudaMallocAsync(reinterpret_cast<void**>(&b->d_root), elems * 8, L.stream) != cudaSuccess ||
-        cudaMallocAsync(reinterpret_cast<void**>(&b->d_rank), elems * 8, L.stream) != cudaSuccess ||
-        (any_w && cudaMallocAsync(reinterpret_cast<void**>(&b->d_w), elems * 4, L.stream) != cudaSuccess)) {
+    uint64_t* d_in = L.d_in;
+    uint32_t* d_w = L.d_w;
+    const bool staged = elems <= L.cap;
+    if (!staged) {
+      d_in = nullptr;
+      d_w = nullptr;
+      if (cudaMallocFromPoolAsync(reinterpret_cast<void**>(&d_in), elems * 8, pool, L.stream) != cudaSuccess ||
+          (any_w && cudaMallocFromPoolAsync(reinterpret_cast<void**>(&d_w), elems * 4, pool, L.stream) != cudaSuccess)) {
+        cudaGetLastError();
+        st = KASCADE_ERR_OOM;
+      }
+    }
+    if (b->heap_off != NO_CHUNK) {
+      b->d_root = reinterpret_cast<uint64_t*>(heap.base + b->heap_off);
+      b->d_rank = b->d_root + elems;
+    } else if (cudaMallocFromPoolAsync(reinterpret_cast<void**>(&b->d_root), elems * 16, pool, L.stream) ==
+               cudaSuccess) {
+      b->d_rank = b->d_root + elems;
+    } else {
       cudaGetLastError();
       st = KASCADE_ERR_OOM;
     }
+    const double t_alloc = now_s();
     std::vector<kascade_segment> segs(take.size());
     uint64_t off = 0;
     for (size_t i = 0; i < take.size() && st == KASCADE_OK; ++i) {
       Request* r = take[i];
       r->t_start = t0;
       segs[i] = kascade_segment{off, r->n, r->kind, 0};
+      const void* in_src = r->src_in ? static_cast<const void*>(r->src_in) : static_cast<const void*>(r->h_in.data());
+      const void* w_src = r->src_w ? static_cast<const void*>(r->src_w) : static_cast<const void*>(r->h_w.data());
       if (r->n) {
-        if (cudaMemcpyAsync(b->d_in + off, r->d_in, r->n * 8, cudaMemcpyDeviceToDevice, L.stream) != cudaSuccess)
+        if (cudaMemcpyAsync(d_in + off, in_src, r->n * 8, cudaMemcpyDefault, L.stream) != cudaSuccess)
           st = KASCADE_ERR_CUDA;
         if (any_w) {
           // lists without weights rank with unit weights; forests ignore weights
           cudaError_t e = cudaSuccess;
           if (r->has_w) {
-            e = cudaMemcpyAsync(b->d_w + off, r->d_w, r->n * 4, cudaMemcpyDeviceToDevice, L.stream);
+            e = cudaMemcpyAsync(d_w + off, w_src, r->n * 4, cudaMemcpyDefault, L.stream);
           } else {
             k_fill_u32<<<(unsigned)std::min<uint64_t>((r->n + 255) / 256, 4096), 256, 0, L.stream>>>(
-                b->d_w + off, r->n, r->kind == KASCADE_SEG_LIST ? 1u : 0u);
+                d_w + off, r->n, r->kind == KASCADE_SEG_LIST ? 1u : 0u);
             e = cudaGetLastError();
           }
           if (e != cudaSuccess) st = KASCADE_ERR_CUDA;
@@ -224,24 +323,24 @@ void kascade_server::lane_loop(int lane) {
       r->off = off;
       off += r->n;
     }
+    const double t_gathered = now_s();
     if (st == KASCADE_OK) {
       kascade_opts o;
       kascade_opts_init(&o);
-      st = kascade_rank_batch(L.ctx, segs.data(), (uint32_t)segs.size(), b->d_in, any_w ? b->d_w : nullptr, elems,
+      st = kascade_rank_batch(L.ctx, segs.data(), (uint32_t)segs.size(), d_in, any_w ? d_w : nullptr, elems,
                               b->d_root, b->d_rank, &o, L.stream);
     }
-    // inputs are no longer needed: free them and the batch's concatenated input
-    for (Request* r : take) {
-      if (r->d_in) cudaFreeAsync(r->d_in, L.stream);
-      if (r->d_w) cudaFreeAsync(r->d_w, L.stream);
-      r->d_in = nullptr;
-      r->d_w = nullptr;
+    // the staged input is free for the next batch once the stream is done;
+    // host submissions drop their copies then too
+    if (!staged) {
+      if (d_in) cudaFreeAsync(d_in, L.stream);
+      if (d_w) cudaFreeAsync(d_w, L.stream);
     }
-    if (b->d_in) cudaFreeAsync(b->d_in, L.stream);
-    if (b->d_w) cudaFreeAsync(b->d_w, L.stream);
-    b->d_in = nullptr;
-    b->d_w = nullptr;
     cudaStreamSynchronize(L.stream);
+    for (Request* r : take) {
+      std::vector<uint64_t>().swap(r->h_in);
+      std::vector<uint32_t>().swap(r->h_w);
+    }
     const double t1 = now_s();
     lk.lock();
     b->refs = (int)take.size();
@@ -250,15 +349,23 @@ void kascade_server::lane_loop(int lane) {
       r->t_done = t1;
       r->status = st;
       r->state = (st == KASCADE_OK) ? 3 : 4;
-      // the input share of the footprint is released now; the result share
-      // stays until the request is released
+      // input and scratch shares of the footprint return to the budget now;
+      // the result share stays until the request is released
+      bytes_in_use -= (r->footprint - r->result_bytes);
+      r->footprint = r->result_bytes;
       const double lat = r->t_done - r->t_submit;
       latencies_all.push_back(lat);
       if (r->n <= cfg.small_max) latencies_small.push_back(lat);
       elements_done += r->n;
     }
     batches++;
+    lane_batches[lane]++;
+    lane_elements[lane] += elems;
+    lane_busy[lane] += t1 - t0;
+    lane_max[lane] = std::max(lane_max[lane], t1 - t0);
+    if (tracing) trace.push_back(BatchTrace{lane, (uint32_t)take.size(), elems, t0, t_alloc, t_gathered, t1});
     t_last_done = t1;
+    admit_locked();
     cv_done.notify_all();
   }
 }
@@ -272,9 +379,11 @@ KASCADE_API void kascade_server_config_init(kascade_server_config* c) {
   c->device = 0;
   c->hbm_budget_bytes = 40ull << 30;
   c->max_batch_requests = 4096;
-  c->max_batch_elements = 1ull << 28;
+  c->max_batch_elements = 1ull << 26;
   c->small_max = 1ull << 20;
   c->small_batch_elements = 1ull << 23;
+  c->latency_sms = 16;
+  c->result_heap_bytes = 0;
 }
 
 KASCADE_API kascade_status kascade_server_create(const kascade_server_config* cfg, kascade_server** out) {
@@ -285,7 +394,7 @@ KASCADE_API kascade_status kascade_server_create(const kascade_server_config* cf
   kascade_server_config_init(&s->cfg);
   if (cfg) s->cfg = *cfg;
   if (s->cfg.max_batch_requests == 0) s->cfg.max_batch_requests = 4096;
-  if (s->cfg.max_batch_elements == 0) s->cfg.max_batch_elements = 1ull << 28;
+  if (s->cfg.max_batch_elements == 0) s->cfg.max_batch_elements = 1ull << 26;
   if (s->cfg.hbm_budget_bytes == 0) s->cfg.hbm_budget_bytes = 40ull << 30;
   if (s->cfg.small_batch_elements == 0) s->cfg.small_batch_elements = 1ull << 23;
   if (cudaSetDevice(s->cfg.device) != cudaSuccess ||
@@ -293,6 +402,19 @@ KASCADE_API kascade_status kascade_server_create(const kascade_server_config* cf
     cudaGetLastError();
     delete s;
     return KASCADE_ERR_CUDA;
+  }
+  {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = s->cfg.device;
+    uint64_t keep_all = ~0ull;
+    if (cudaMemPoolCreate(&s->pool, &props) != cudaSuccess ||
+        cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep_all) != cudaSuccess) {
+      cudaGetLastError();
+      kascade_server_destroy(s);
+      return KASCADE_ERR_CUDA;
+    }
   }
   for (int i = 0; i < 2; ++i) {
     int lo = 0, hi = 0;
@@ -305,6 +427,43 @@ KASCADE_API kascade_status kascade_server_create(const kascade_server_config* cf
       return KASCADE_ERR_CUDA;
     }
   }
+  {
+    // the throughput lane's persistent kernels leave SMs to the latency lane
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->cfg.device);
+    const int keep = (int)s->cfg.latency_sms;
+    if (keep > 0 && keep < sms) kascade_ctx_set_sm_budget(s->lanes[1].ctx, sms - keep);
+  }
+  // scratch and input staging for a full batch of each lane, so that no
+  // batch grows an arena (growing synchronises the device and would stall
+  // the other lane), and the result heap
+  {
+    const uint64_t cap[2] = {s->cfg.small_batch_elements, s->cfg.max_batch_elements};
+    bool ok = true;
+    for (int i = 0; i < 2 && ok; ++i) {
+      kascade_server::Lane& L = s->lanes[i];
+      L.cap = cap[i];
+      ok = kascade_ctx_reserve(L.ctx, kascade_scratch_bytes_root_forest(cap[i])) == KASCADE_OK &&
+           cudaMalloc(reinterpret_cast<void**>(&L.d_in), cap[i] * 8) == cudaSuccess &&
+           cudaMalloc(reinterpret_cast<void**>(&L.d_w), cap[i] * 4) == cudaSuccess;
+    }
+    uint64_t hb = s->cfg.result_heap_bytes ? s->cfg.result_heap_bytes : s->cfg.hbm_budget_bytes / 2;
+    hb = (hb + 255) & ~255ull;
+    char* hp = nullptr;
+    ok = ok && cudaMalloc(reinterpret_cast<void**>(&hp), hb) == cudaSuccess;
+    if (!ok) {
+      cudaGetLastError();
+      if (hp) cudaFree(hp);
+      kascade_server_destroy(s);
+      return KASCADE_ERR_OOM;
+    }
+    s->heap.init(hp, hb);
+  }
+  if (s->warm_lane(0, 1ull << 20, 1ull << 19) != KASCADE_OK || s->warm_lane(1, 1ull << 22, 1ull << 21) != KASCADE_OK) {
+    kascade_server_destroy(s);
+    return KASCADE_ERR_CUDA;
+  }
+  s->tracing = std::getenv("KASCADE_SERVER_TRACE") != nullptr;
   for (int i = 0; i < 2; ++i) s->lanes[i].th = std::thread([s, i] { s->lane_loop(i); });
   *out = s;
   return KASCADE_OK;
@@ -319,13 +478,19 @@ KASCADE_API kascade_status kascade_server_destroy(kascade_server* s) {
   }
   for (auto& L : s->lanes)
     if (L.th.joinable()) L.th.join();
+  if (s->tracing) {
+    // one line per batch: lane, requests, elements, start, buffers
+    // allocated, inputs issued, end (seconds on the steady clock)
+    if (FILE* f = std::fopen(std::getenv("KASCADE_SERVER_TRACE"), "w")) {
+      std::fprintf(f, "lane,requests,elements,t_start,t_alloc,t_gathered,t_end\n");
+      for (const BatchTrace& b : s->trace)
+        std::fprintf(f, "%d,%u,%llu,%.6f,%.6f,%.6f,%.6f\n", b.lane, b.requests, (unsigned long long)b.elements,
+                     b.t_start, b.t_alloc, b.t_gathered, b.t_end);
+      std::fclose(f);
+    }
+  }
   cudaSetDevice(s->cfg.device);
   cudaDeviceSynchronize();
-  for (auto& kv : s->reqs) {
-    Request* r = kv.second.get();
-    if (r->d_in) cudaFree(r->d_in);
-    if (r->d_w) cudaFree(r->d_w);
-  }
   std::vector<std::shared_ptr<BatchBuf>> bufs;
   for (auto& kv : s->reqs)
     if (kv.second->batch) bufs.push_back(kv.second->batch);
@@ -333,15 +498,18 @@ KASCADE_API kascade_status kascade_server_destroy(kascade_server* s) {
   std::sort(bufs.begin(), bufs.end());
   bufs.erase(std::unique(bufs.begin(), bufs.end()), bufs.end());
   for (auto& b : bufs) {
-    if (b->d_root) cudaFree(b->d_root);
-    if (b->d_rank) cudaFree(b->d_rank);
+    if (b->heap_off == NO_CHUNK && b->d_root) cudaFree(b->d_root);
     b->d_root = b->d_rank = nullptr;
   }
+  if (s->heap.base) cudaFree(s->heap.base);
   for (auto& L : s->lanes) {
     if (L.ctx) kascade_ctx_destroy(L.ctx);
     if (L.stream) cudaStreamDestroy(L.stream);
+    if (L.d_in) cudaFree(L.d_in);
+    if (L.d_w) cudaFree(L.d_w);
   }
   if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
+  if (s->pool) cudaMemPoolDestroy(s->pool);
   cudaGetLastError();
   delete s;
   return KASCADE_OK;
@@ -363,45 +531,17 @@ static kascade_status submit(kascade_server* s, uint32_t kind, const uint64_t* i
     r->h_in.assign(input, input + n);
     if (r->has_w) r->h_w.assign(weights, weights + n);
   }
+  if (device) {
+    r->src_in = input;
+    r->src_w = r->has_w ? weights : nullptr;
+  }
+  r->result_bytes = 16 * n;
   std::unique_lock<std::mutex> lk(s->mu);
   if (r->footprint > s->cfg.hbm_budget_bytes) return KASCADE_ERR_TOO_LARGE;
   r->id = s->next_id++;
   *request_id = r->id;
   if (s->t_first_submit == 0) s->t_first_submit = r->t_submit;
   s->reqs.emplace(r->id, std::move(req));
-  if (device) {
-    // device input: copy into the server's own buffers at admission
-    if (s->bytes_in_use + r->footprint > s->cfg.hbm_budget_bytes && s->bytes_in_use > 0) {
-      // wait for memory: admission happens in order as requests are released
-      s->cv_done.wait(lk, [&] { return s->bytes_in_use + r->footprint <= s->cfg.hbm_budget_bytes || s->bytes_in_use == 0; });
-    }
-    s->bytes_in_use += r->footprint;
-    lk.unlock();
-    cudaSetDevice(s->cfg.device);
-    kascade_status st = KASCADE_OK;
-    if (cudaMallocAsync(reinterpret_cast<void**>(&r->d_in), n ? n * 8 : 8, s->copy_stream) != cudaSuccess ||
-        (n && cudaMemcpyAsync(r->d_in, input, n * 8, cudaMemcpyDeviceToDevice, s->copy_stream) != cudaSuccess))
-      st = KASCADE_ERR_CUDA;
-    if (st == KASCADE_OK && r->has_w &&
-        (cudaMallocAsync(reinterpret_cast<void**>(&r->d_w), n ? n * 4 : 8, s->copy_stream) != cudaSuccess ||
-         (n && cudaMemcpyAsync(r->d_w, weights, n * 4, cudaMemcpyDeviceToDevice, s->copy_stream) != cudaSuccess)))
-      st = KASCADE_ERR_CUDA;
-    if (cudaStreamSynchronize(s->copy_stream) != cudaSuccess) st = KASCADE_ERR_CUDA;
-    lk.lock();
-    if (st != KASCADE_OK) {
-      cudaGetLastError();
-      r->state = 4;
-      r->status = st;
-      s->bytes_in_use -= r->footprint;
-      s->cv_done.notify_all();
-      return st;
-    }
-    r->admitted = true;
-    r->state = 1;
-    s->ready.push_back(r);
-    s->cv_work.notify_all();
-    return KASCADE_OK;
-  }
   s->waiting.push_back(r);
   s->admit_locked();
   return KASCADE_OK;
@@ -473,7 +613,14 @@ KASCADE_API kascade_status kascade_server_release(kascade_server* s, uint64_t id
     if (it == s->reqs.end() || it->second->state < 3) return KASCADE_ERR_INVALID_ARG;
     Request* r = it->second.get();
     s->bytes_in_use -= r->footprint;
-    if (r->batch && --r->batch->refs == 0) drop = r->batch;
+    if (r->batch && --r->batch->refs == 0) {
+      if (r->batch->heap_off != NO_CHUNK) {
+        s->heap.release(r->batch->heap_off, r->batch->heap_bytes);
+        r->batch->d_root = r->batch->d_rank = nullptr;
+      } else {
+        drop = r->batch;
+      }
+    }
     s->reqs.erase(it);
     s->admit_locked();
     s->cv_done.notify_all();
@@ -481,7 +628,6 @@ KASCADE_API kascade_status kascade_server_release(kascade_server* s, uint64_t id
   if (drop) {
     cudaSetDevice(s->cfg.device);
     if (drop->d_root) cudaFreeAsync(drop->d_root, s->copy_stream);
-    if (drop->d_rank) cudaFreeAsync(drop->d_rank, s->copy_stream);
     drop->d_root = drop->d_rank = nullptr;
   }
   return KASCADE_OK;
@@ -512,6 +658,12 @@ KASCADE_API kascade_status kascade_server_get_stats(kascade_server* s, kascade_s
   out->elements_per_s = span > 0 ? (double)s->elements_done / span : 0.0;
   out->requests_per_s = span > 0 ? (double)s->latencies_all.size() / span : 0.0;
   out->bytes_in_use = s->bytes_in_use;
+  for (int i = 0; i < 2; ++i) {
+    out->lane_batches[i] = s->lane_batches[i];
+    out->lane_elements[i] = s->lane_elements[i];
+    out->lane_busy_ms[i] = 1e3 * s->lane_busy[i];
+    out->lane_max_batch_ms[i] = 1e3 * s->lane_max[i];
+  }
   return KASCADE_OK;
 }
 
@@ -522,6 +674,10 @@ KASCADE_API kascade_status kascade_server_reset_stats(kascade_server* s) {
   s->latencies_small.clear();
   s->elements_done = 0;
   s->batches = 0;
+  for (int i = 0; i < 2; ++i) {
+    s->lane_batches[i] = s->lane_elements[i] = 0;
+    s->lane_busy[i] = s->lane_max[i] = 0;
+  }
   s->t_first_submit = 0;
   s->t_last_done = 0;
   return KASCADE_OK;

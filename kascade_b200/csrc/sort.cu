@@ -243,8 +243,8 @@ kascade_status radix_sort_pairs(kascade_ctx& ctx, const SortSource& src, uint32_
     *vals_out = vb[0];
     return KASCADE_OK;
   }
-  const unsigned grid = (unsigned)std::min<uint64_t>(num_tiles, (uint64_t)ctx.sm_count * 8);
-  const unsigned grid_scatter = (unsigned)std::min<uint64_t>(num_tiles, (uint64_t)ctx.sm_count * 4);
+  const unsigned grid = (unsigned)std::min<uint64_t>(num_tiles, (uint64_t)ctx.usable_sms() * 8);
+  const unsigned grid_scatter = (unsigned)std::min<uint64_t>(num_tiles, (uint64_t)ctx.usable_sms() * 4);
   int cur = 0;
   const int passes = (key_bits + 7) / 8;
   for (int p = 0; p < passes; ++p) {
