@@ -288,7 +288,11 @@ def measure_served(kb, dev, n_requests: int = 1000, rate: float = 20000.0, **ser
     ids = [None] * n_requests
     done_q: "queue.Queue" = queue.Queue()
     check_at = {0, n_requests // 2, n_requests - 1}
-    checks = {}
+    # destinations for the spot checks, allocated before the run: an
+    # allocation inside it could synchronise the device and stall the lanes
+    checks = {i: (torch.empty(int(sizes[i]), dtype=torch.int64, device=dev),
+                  torch.empty(int(sizes[i]), dtype=torch.int64, device=dev)) for i in check_at}
+    torch.cuda.synchronize()
     errors = []
 
     def collector():
@@ -300,7 +304,8 @@ def measure_served(kb, dev, n_requests: int = 1000, rate: float = 20000.0, **ser
                 srv.wait(rid, 300.0)
                 if i in check_at:
                     r_dev, k_dev = srv.result_device(rid)
-                    checks[i] = (r_dev.clone(), k_dev.clone())
+                    checks[i][0].copy_(r_dev.view(torch.int64))
+                    checks[i][1].copy_(k_dev.view(torch.int64))
                 srv.release(rid)
             except Exception as e:  # noqa: BLE001
                 errors.append(e)
@@ -328,7 +333,7 @@ def measure_served(kb, dev, n_requests: int = 1000, rate: float = 20000.0, **ser
             r_p, k_p = kb.rank_list(inputs[a:b], w[a:b])
         else:
             r_p, k_p = kb.root_forest(inputs[a:b])
-        ok &= bool(torch.equal(r_dev.view(torch.int64), r_p) and torch.equal(k_dev.view(torch.int64), k_p))
+        ok &= bool(torch.equal(r_dev, r_p) and torch.equal(k_dev, k_p))
     # plain per-request calls of the same requests, back to back
     ctx = kb.Context(dev.index or 0)
     root = torch.empty(int(sizes.max()), dtype=torch.int64, device=dev)
@@ -355,7 +360,8 @@ def measure_served(kb, dev, n_requests: int = 1000, rate: float = 20000.0, **ser
             "requests_le_2^20": int(st["completed_small"]), "batches": int(st["batches"]),
             "plain_elements_per_s": total / tp, "plain_req_per_s": round(n_requests / tp, 1),
             "throughput_vs_plain": round(st["elements_per_s"] / (total / tp), 2), "spot_check_equal": ok,
-            "lanes": {k: st[k] for k in ("lane_batches", "lane_elements", "lane_busy_ms", "lane_max_batch_ms")}}
+            "lanes": {k: st[k] for k in ("lane_batches", "lane_elements", "lane_busy_ms", "lane_max_batch_ms",
+                                         "partition_sms", "partition_batches")}}
 
 
 def run_reference(args, world, rank):

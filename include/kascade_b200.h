@@ -288,8 +288,11 @@ typedef struct kascade_server_config {
   uint64_t small_max;            /* latency lane: requests up to this many
                                     elements (default 2^20)                       */
   uint64_t small_batch_elements; /* elements per batch, latency lane (2^23)       */
-  uint32_t latency_sms;          /* SMs the throughput lane's persistent kernels
-                                    leave free for the latency lane (default 16)  */
+  uint32_t latency_sms;          /* SMs the throughput lane leaves free while the
+                                    latency lane has work (default 80): its
+                                    batches then run in an SM partition (a green
+                                    context) of the other SMs, rounded down to a
+                                    multiple of 8; 0 = no partition             */
   uint32_t reserved2;
   uint64_t result_heap_bytes;    /* device memory set aside at creation for
                                     results (default hbm_budget_bytes / 2); a
@@ -312,6 +315,9 @@ typedef struct kascade_server_stats {
   uint64_t lane_elements[2];
   double lane_busy_ms[2];      /* wall time spent running batches              */
   double lane_max_batch_ms[2]; /* longest batch                                */
+  uint64_t partition_sms;      /* SMs of the throughput lane's partition (0: the
+                                  driver offers none; grid budgets only)        */
+  uint64_t partition_batches;  /* throughput-lane batches run in the partition  */
 } kascade_server_stats;
 
 KASCADE_API void kascade_server_config_init(kascade_server_config* cfg);

@@ -52,7 +52,8 @@ class ServerStats(ctypes.Structure):
                 ("p99_small_ms", ctypes.c_double), ("elements_per_s", ctypes.c_double),
                 ("requests_per_s", ctypes.c_double), ("bytes_in_use", c_u64), ("lane_batches", c_u64 * 2),
                 ("lane_elements", c_u64 * 2), ("lane_busy_ms", ctypes.c_double * 2),
-                ("lane_max_batch_ms", ctypes.c_double * 2)]
+                ("lane_max_batch_ms", ctypes.c_double * 2), ("partition_sms", c_u64),
+                ("partition_batches", c_u64)]
 
 
 class Opts(ctypes.Structure):

@@ -42,7 +42,7 @@ kascade_status begin_call(kascade_ctx* ctx, cudaStream_t s, const kascade_opts* 
   // callers built against the first version of kascade_opts (without
   // level0_mode / max_chain) pass a smaller struct_size; both are accepted
   if (o && o->struct_size != 0 && o->struct_size < offsetof(kascade_opts, level0_mode)) return KASCADE_ERR_INVALID_ARG;
-  KS_CUDA(cudaSetDevice(ctx->device));
+  KS_CUDA(ensure_device(ctx->device));
   if (ctx->done_event && ctx->last_stream != s) KS_CUDA(cudaStreamWaitEvent(s, ctx->done_event, 0));
   KS_TRY(arena_begin_call(*ctx, s));
   KS_TRY(status_reset(*ctx, s));
@@ -139,7 +139,7 @@ KASCADE_API kascade_status kascade_ctx_create(int device, kascade_ctx** out) {
   int count = 0;
   KS_CUDA(cudaGetDeviceCount(&count));
   if (device < 0 || device >= count) return KASCADE_ERR_INVALID_ARG;
-  KS_CUDA(cudaSetDevice(device));
+  KS_CUDA(ensure_device(device));
   kascade_ctx* c = new (std::nothrow) kascade_ctx();
   if (!c) return KASCADE_ERR_OOM;
   c->device = device;
@@ -163,9 +163,10 @@ KASCADE_API kascade_status kascade_ctx_create(int device, kascade_ctx** out) {
 
 KASCADE_API kascade_status kascade_ctx_destroy(kascade_ctx* c) {
   if (!c) return KASCADE_OK;
-  cudaSetDevice(c->device);
+  ensure_device(c->device);
   cudaDeviceSynchronize();
-  for (auto& b : c->blocks) cudaFree(b.ptr);
+  for (auto& b : c->blocks)
+    if (b.owned) cudaFree(b.ptr);
   for (auto& p : c->pending) {
     cudaEventDestroy(p.a);
     cudaEventDestroy(p.b);
@@ -181,13 +182,14 @@ KASCADE_API kascade_status kascade_ctx_destroy(kascade_ctx* c) {
 
 KASCADE_API kascade_status kascade_ctx_reserve(kascade_ctx* c, uint64_t bytes) {
   if (!c) return KASCADE_ERR_INVALID_ARG;
-  KS_CUDA(cudaSetDevice(c->device));
+  KS_CUDA(ensure_device(c->device));
   KS_CUDA(cudaDeviceSynchronize());
   size_t have = 0;
   for (auto& b : c->blocks) have += b.cap;
   c->reserve_bytes = bytes;
   if (have >= bytes && c->blocks.size() == 1) return KASCADE_OK;
-  for (auto& b : c->blocks) cudaFree(b.ptr);
+  for (auto& b : c->blocks)
+    if (b.owned) cudaFree(b.ptr);
   c->blocks.clear();
   char* p = nullptr;
   if (cudaMalloc(&p, bytes) != cudaSuccess) {
@@ -474,7 +476,7 @@ KASCADE_API kascade_status kascade_ctx_set_size_classes(kascade_ctx* c, const ui
 
 KASCADE_API kascade_status kascade_ctx_set_sm_budget(kascade_ctx* c, int sms) {
   if (!c || sms < 0) return KASCADE_ERR_INVALID_ARG;
-  c->sm_budget = sms;
+  c->sm_budget.store(sms, std::memory_order_relaxed);
   return KASCADE_OK;
 }
 

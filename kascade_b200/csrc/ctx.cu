@@ -19,7 +19,7 @@ kascade_status arena_begin_call(kascade_ctx& ctx, cudaStream_t s) {
     size_t total = 0;
     for (auto& b : ctx.blocks) {
       total += b.cap;
-      cudaFree(b.ptr);
+      if (b.owned) cudaFree(b.ptr);
     }
     ctx.blocks.clear();
     char* p = nullptr;
@@ -58,8 +58,22 @@ void* arena_alloc(kascade_ctx& ctx, size_t bytes) {
     }
     cap = bytes;
   }
-  ctx.blocks.push_back({p, cap, bytes});
+  ctx.blocks.push_back({p, cap, bytes, true});
   return p;
+}
+
+void arena_adopt(kascade_ctx& ctx, char* p, size_t bytes) {
+  for (auto& b : ctx.blocks)
+    if (b.owned) cudaFree(b.ptr);
+  ctx.blocks.clear();
+  ctx.blocks.push_back({p, bytes, 0, false});
+  ctx.reserve_bytes = bytes;
+}
+
+cudaError_t ensure_device(int device) {
+  int cur = -1;
+  if (cudaGetDevice(&cur) == cudaSuccess && cur == device) return cudaSuccess;
+  return cudaSetDevice(device);
 }
 
 kascade_status status_reset(kascade_ctx& ctx, cudaStream_t s) {

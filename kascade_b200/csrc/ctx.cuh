@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <map>
 #include <string>
 #include <vector>
@@ -23,6 +24,7 @@ struct kascade_ctx {
     char* ptr;
     size_t cap;
     size_t used;
+    bool owned = true;  // false: memory lent by the caller (arena_adopt)
   };
   std::vector<Block> blocks;
   size_t reserve_bytes = 0;
@@ -51,9 +53,13 @@ struct kascade_ctx {
   std::vector<uint32_t> class_spacing{8u, 16u, 32u, 48u};
   // SMs' worth of block slots this context's kernels may occupy (0 = all):
   // grids are sized for this many SMs, so that work on other streams (a
-  // server's latency lane) always finds free slots
-  int sm_budget = 0;
-  int usable_sms() const { return (sm_budget > 0 && sm_budget < sm_count) ? sm_budget : sm_count; }
+  // server's latency lane) always finds free slots.  Read at every launch;
+  // another thread may change it between launches.
+  std::atomic<int> sm_budget{0};
+  int usable_sms() const {
+    const int b = sm_budget.load(std::memory_order_relaxed);
+    return (b > 0 && b < sm_count) ? b : sm_count;
+  }
 };
 
 namespace ks {
@@ -62,6 +68,12 @@ constexpr int KS_PINNED_WORDS = 64;
 
 // Arena -------------------------------------------------------------------
 kascade_status arena_begin_call(kascade_ctx& ctx, cudaStream_t s);
+// Use `bytes` of caller-owned device memory as the arena (the caller frees
+// it after the context); contexts that never run concurrently may share one.
+void arena_adopt(kascade_ctx& ctx, char* p, size_t bytes);
+// Make `device` current unless the current context already belongs to it
+// (which keeps a context the caller made current, e.g. an SM partition).
+cudaError_t ensure_device(int device);
 void* arena_alloc(kascade_ctx& ctx, size_t bytes);  // nullptr on OOM
 template <class T>
 T* alloc(kascade_ctx& ctx, size_t count) {

@@ -12,8 +12,9 @@
 //    into one concatenated buffer and ranks them with one kascade_rank_batch
 //    call.  Lane 0 serves requests up to `small_max` elements (the latency
 //    lane, small batches, higher stream priority), lane 1 the larger ones;
-//    both lanes' batches run concurrently on the device, and lane 1's
-//    persistent kernels leave `latency_sms` SMs free for lane 0.
+//    both lanes' batches run concurrently on the device, and while lane 0
+//    has work, lane 1's kernels are sized to leave `latency_sms` SMs free.
+//    A batch's device-resident inputs are gathered by one kernel launch.
 //  - memory: nothing is allocated per batch on the normal path.  Each lane
 //    stages its batch input in buffers sized for a full batch, and results
 //    go to a result heap set aside at creation (first fit, coalescing free
@@ -34,9 +35,12 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <string>
 #include <thread>
 #include <unordered_map>
 #include <vector>
+
+#include <cuda.h>
 
 #include "ctx.cuh"
 
@@ -117,9 +121,32 @@ struct Request {
   double t_submit = 0, t_start = 0, t_done = 0;
 };
 
-__global__ void k_fill_u32(uint32_t* __restrict__ p, uint64_t n, uint32_t v) {
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
-    p[i] = v;
+// One piece of a batch's input gather: up to PIECE elements of one request.
+struct __align__(16) Piece {
+  const uint64_t* src_in;  // nullptr: input already in place (host submission)
+  const uint32_t* src_w;   // nullptr: fill the weights with `fill`
+  uint64_t dst;            // offset in the batch
+  uint32_t n;
+  uint32_t fill;
+};
+constexpr uint32_t PIECE = 16384;
+constexpr int LATENCY_HOLD_MS = 20;
+
+// Gather device-resident request inputs (and weights, or their unit / zero
+// fill) into the batch's concatenated buffers: one launch per batch.
+__global__ void __launch_bounds__(256) k_gather(const Piece* __restrict__ pieces, uint32_t npieces,
+                                                uint64_t* __restrict__ d_in, uint32_t* __restrict__ d_w) {
+  for (uint32_t p = blockIdx.x; p < npieces; p += gridDim.x) {
+    const Piece pc = pieces[p];
+    if (pc.src_in)
+      for (uint32_t i = threadIdx.x; i < pc.n; i += blockDim.x) d_in[pc.dst + i] = __ldcs(pc.src_in + i);
+    if (d_w) {
+      if (pc.src_w)
+        for (uint32_t i = threadIdx.x; i < pc.n; i += blockDim.x) d_w[pc.dst + i] = __ldcs(pc.src_w + i);
+      else
+        for (uint32_t i = threadIdx.x; i < pc.n; i += blockDim.x) d_w[pc.dst + i] = pc.fill;
+    }
+  }
 }
 
 uint64_t footprint_of(uint32_t kind, uint64_t n, bool w) {
@@ -136,9 +163,12 @@ uint64_t footprint_of(uint32_t kind, uint64_t n, bool w) {
 // One finished batch, for the optional trace (KASCADE_SERVER_TRACE=<file>).
 struct BatchTrace {
   int lane;
+  int part;  // 1: ran in lane 1's SM partition
   uint32_t requests;
   uint64_t elements;
   double t_start, t_alloc, t_gathered, t_end;
+  double gpu_ms, chase_ms;  // kernel time of the batch (trace runs profile it)
+  char top[96];             // the batch's three longest kernels
 };
 
 struct kascade_server {
@@ -164,6 +194,12 @@ struct kascade_server {
     uint64_t* d_in = nullptr;  // staging for a full batch
     uint32_t* d_w = nullptr;
     uint64_t cap = 0;
+    Piece* h_pieces = nullptr;  // gather table (pinned) and its device copy
+    Piece* d_pieces = nullptr;
+    uint64_t piece_cap = 0;
+    // lane 1 only: a second context and stream inside the SM partition
+    kascade_ctx* pctx = nullptr;
+    cudaStream_t pstream = nullptr;
   };
   Lane lanes[2];
   cudaStream_t copy_stream = nullptr;
@@ -171,19 +207,122 @@ struct kascade_server {
   // the driver, hence no device-wide synchronisation on reuse)
   cudaMemPool_t pool = nullptr;
   ResultHeap heap;
+  int lane1_busy_sms = 0;  // lane 1's SM budget while lane 0 has work (0 = all)
+  // SM partition (green context) for lane 1 while lane 0 is active; lane 1
+  // runs on the whole device otherwise
+  CUgreenCtx green = nullptr;
+  CUcontext green_cu = nullptr, primary_cu = nullptr;
+  int partition_sms = 0;
+  char* lane1_arena = nullptr;  // shared by lane 1's two contexts
+  bool lane0_running = false;
+  double lane0_last = -1e9;
+  uint64_t partition_batches = 0;
+  struct Driver {
+    CUresult (*DeviceGet)(CUdevice*, int) = nullptr;
+    CUresult (*DeviceGetDevResource)(CUdevice, CUdevResource*, CUdevResourceType) = nullptr;
+    CUresult (*DevSmResourceSplitByCount)(CUdevResource*, unsigned int*, const CUdevResource*, CUdevResource*,
+                                          unsigned int, unsigned int) = nullptr;
+    CUresult (*DevResourceGenerateDesc)(CUdevResourceDesc*, CUdevResource*, unsigned int) = nullptr;
+    CUresult (*GreenCtxCreate)(CUgreenCtx*, CUdevResourceDesc, CUdevice, unsigned int) = nullptr;
+    CUresult (*GreenCtxDestroy)(CUgreenCtx) = nullptr;
+    CUresult (*CtxFromGreenCtx)(CUcontext*, CUgreenCtx) = nullptr;
+    CUresult (*CtxGetCurrent)(CUcontext*) = nullptr;
+    CUresult (*CtxSetCurrent)(CUcontext) = nullptr;
+  } drv;
 
   std::vector<BatchTrace> trace;
   bool tracing = false;
 
   void admit_locked();
   void lane_loop(int lane);
-  kascade_status warm_lane(int lane, uint64_t n_list, uint64_t n_forest);
+  kascade_status warm_lane(kascade_ctx* ctx, cudaStream_t stream, const Lane& L, uint64_t n_list, uint64_t n_forest);
+  bool setup_partition();
+  void drop_partition();
 };
+
+template <class F>
+static bool driver_fn(const char* name, F*& fn) {
+  void* p = nullptr;
+  cudaDriverEntryPointQueryResult q{};
+  if (cudaGetDriverEntryPoint(name, &p, cudaEnableDefault, &q) != cudaSuccess || q != cudaDriverEntryPointSuccess ||
+      !p) {
+    cudaGetLastError();
+    return false;
+  }
+  fn = reinterpret_cast<F*>(p);
+  return true;
+}
+
+// Carve an SM partition of (all SMs - latency_sms, rounded down to the
+// partition granularity of 8) as a green context, and give lane 1 a second
+// library context and stream inside it.  Work in the partition cannot use
+// the other SMs, so lane 0 always finds latency_sms SMs that lane 1 does not
+// hold.  Returns false (and leaves lane 1 on the whole device, with grid
+// budgets only) where the driver offers no green contexts.
+bool kascade_server::setup_partition() {
+  if (cfg.latency_sms == 0) return false;
+  Driver& d = drv;
+  if (!driver_fn("cuDeviceGet", d.DeviceGet) || !driver_fn("cuDeviceGetDevResource", d.DeviceGetDevResource) ||
+      !driver_fn("cuDevSmResourceSplitByCount", d.DevSmResourceSplitByCount) ||
+      !driver_fn("cuDevResourceGenerateDesc", d.DevResourceGenerateDesc) ||
+      !driver_fn("cuGreenCtxCreate", d.GreenCtxCreate) || !driver_fn("cuGreenCtxDestroy", d.GreenCtxDestroy) ||
+      !driver_fn("cuCtxFromGreenCtx", d.CtxFromGreenCtx) || !driver_fn("cuCtxGetCurrent", d.CtxGetCurrent) ||
+      !driver_fn("cuCtxSetCurrent", d.CtxSetCurrent))
+    return false;
+  CUdevice dev = 0;
+  if (d.DeviceGet(&dev, cfg.device) != CUDA_SUCCESS || d.CtxGetCurrent(&primary_cu) != CUDA_SUCCESS || !primary_cu)
+    return false;
+  CUdevResource all{}, grp{}, rest{};
+  if (d.DeviceGetDevResource(dev, &all, CU_DEV_RESOURCE_TYPE_SM) != CUDA_SUCCESS) return false;
+  const int want = ((int)all.sm.smCount - (int)cfg.latency_sms) & ~7;
+  if (want < 8) return false;
+  unsigned int nb = 1;
+  CUdevResourceDesc desc = nullptr;
+  if (d.DevSmResourceSplitByCount(&grp, &nb, &all, &rest, 0, (unsigned)want) != CUDA_SUCCESS || nb < 1 ||
+      d.DevResourceGenerateDesc(&desc, &grp, 1) != CUDA_SUCCESS ||
+      d.GreenCtxCreate(&green, desc, dev, CU_GREEN_CTX_DEFAULT_STREAM) != CUDA_SUCCESS)
+    return false;
+  partition_sms = (int)grp.sm.smCount;
+  Lane& L = lanes[1];
+  bool ok = d.CtxFromGreenCtx(&green_cu, green) == CUDA_SUCCESS && d.CtxSetCurrent(green_cu) == CUDA_SUCCESS;
+  if (ok) {
+    int lo = 0, hi = 0;
+    cudaDeviceGetStreamPriorityRange(&lo, &hi);
+    ok = cudaStreamCreateWithPriority(&L.pstream, cudaStreamNonBlocking, lo) == cudaSuccess &&
+         kascade_ctx_create(cfg.device, &L.pctx) == KASCADE_OK;
+  }
+  if (ok) {
+    kascade_ctx_set_sm_budget(L.pctx, partition_sms);
+    ks::arena_adopt(*L.pctx, lane1_arena, kascade_scratch_bytes_root_forest(L.cap));
+    ok = warm_lane(L.pctx, L.pstream, L, 1ull << 22, 1ull << 21) == KASCADE_OK;
+  }
+  d.CtxSetCurrent(primary_cu);
+  cudaGetLastError();
+  if (!ok) drop_partition();
+  return ok;
+}
+
+void kascade_server::drop_partition() {
+  Lane& L = lanes[1];
+  if (green_cu && drv.CtxSetCurrent) {
+    drv.CtxSetCurrent(green_cu);
+    if (L.pctx) kascade_ctx_destroy(L.pctx);
+    if (L.pstream) cudaStreamDestroy(L.pstream);
+    drv.CtxSetCurrent(primary_cu);
+  }
+  L.pctx = nullptr;
+  L.pstream = nullptr;
+  if (green && drv.GreenCtxDestroy) drv.GreenCtxDestroy(green);
+  green = nullptr;
+  green_cu = nullptr;
+  partition_sms = 0;
+  cudaGetLastError();
+}
 
 // Run one synthetic batch (a list and a forest) on a lane before serving, so
 // that the first requests pay for no kernel loading and no pool growth.
-kascade_status kascade_server::warm_lane(int lane, uint64_t n_list, uint64_t n_forest) {
-  Lane& L = lanes[lane];
+kascade_status kascade_server::warm_lane(kascade_ctx* ctx, cudaStream_t stream, const Lane& L, uint64_t n_list,
+                                         uint64_t n_forest) {
   const uint64_t n = n_list + n_forest;
   if (n > L.cap || 16 * n > heap.size) return KASCADE_OK;  // nothing to warm with
   uint64_t* in = L.d_in;
@@ -191,16 +330,21 @@ kascade_status kascade_server::warm_lane(int lane, uint64_t n_list, uint64_t n_f
   uint64_t* root = reinterpret_cast<uint64_t*>(heap.base);
   uint64_t* rank = root + n;
   kascade_status st = KASCADE_OK;
-  if (st == KASCADE_OK) st = kascade_gen_list(n_list, 0x5e7e, 0, in, L.stream);
-  if (st == KASCADE_OK) st = kascade_gen_weights(n, 0x5e7e, 16, w, L.stream);
-  if (st == KASCADE_OK) st = kascade_gen_forest(n_forest, 0x5e7e, 0, 16, 0, in + n_list, L.stream);
+  if (st == KASCADE_OK) st = kascade_gen_list(n_list, 0x5e7e, 0, in, stream);
+  if (st == KASCADE_OK) st = kascade_gen_weights(n, 0x5e7e, 16, w, stream);
+  if (st == KASCADE_OK) st = kascade_gen_forest(n_forest, 0x5e7e, 0, 16, 0, in + n_list, stream);
+  if (st == KASCADE_OK) {
+    // an empty gather, to load the gather kernel in this context too
+    k_gather<<<1, 256, 0, stream>>>(L.d_pieces, 0, in, w);
+    if (cudaGetLastError() != cudaSuccess) st = KASCADE_ERR_CUDA;
+  }
   if (st == KASCADE_OK) {
     kascade_segment segs[2] = {{0, n_list, KASCADE_SEG_LIST, 0}, {n_list, n_forest, KASCADE_SEG_FOREST, 0}};
     kascade_opts o;
     kascade_opts_init(&o);
-    st = kascade_rank_batch(L.ctx, segs, 2, in, w, n, root, rank, &o, L.stream);
+    st = kascade_rank_batch(ctx, segs, 2, in, w, n, root, rank, &o, stream);
   }
-  if (cudaStreamSynchronize(L.stream) != cudaSuccess && st == KASCADE_OK) st = KASCADE_ERR_CUDA;
+  if (cudaStreamSynchronize(stream) != cudaSuccess && st == KASCADE_OK) st = KASCADE_ERR_CUDA;
   cudaGetLastError();
   return st;
 }
@@ -241,12 +385,19 @@ void kascade_server::lane_loop(int lane) {
     uint64_t elems = 0;
     auto mine = [&](const Request* r) { return lane == 0 ? r->n <= cfg.small_max : r->n > cfg.small_max; };
     const uint64_t max_elems = lane == 0 ? cfg.small_batch_elements : cfg.max_batch_elements;
-    cv_work.wait(lk, [&] {
-      if (stop) return true;
+    auto have_work = [&] {
       for (Request* r : ready)
         if (mine(r)) return true;
       return false;
-    });
+    };
+    if (lane == 0 && !have_work() && !stop) {
+      // give lane 1 all SMs back only after the latency lane has been idle
+      // for a while: arrivals are bursty, and a full-width launch of lane 1
+      // holds its SMs until it ends
+      if (!cv_work.wait_for(lk, std::chrono::milliseconds(LATENCY_HOLD_MS), [&] { return stop || have_work(); }))
+        kascade_ctx_set_sm_budget(lanes[1].ctx, 0);
+    }
+    cv_work.wait(lk, [&] { return stop || have_work(); });
     if (stop && ready.empty()) break;
     for (auto it = ready.begin(); it != ready.end();) {
       Request* r = *it;
@@ -263,12 +414,28 @@ void kascade_server::lane_loop(int lane) {
       if (stop) break;
       continue;
     }
+    // while the latency lane has work, the throughput lane's next launches
+    // leave it latency_sms SMs, and its next batch runs in the partition
     const double t0 = now_s();
+    if (lane == 0) {
+      kascade_ctx_set_sm_budget(lanes[1].ctx, lane1_busy_sms);
+      lane0_running = true;
+    }
+    bool in_part = false;
+    if (lane == 1 && L.pctx) {
+      bool small_waiting = false;
+      for (Request* r : ready) small_waiting |= r->n <= cfg.small_max;
+      in_part = lane0_running || small_waiting || t0 - lane0_last < 1e-3 * LATENCY_HOLD_MS;
+      if (in_part) partition_batches++;
+    }
+    kascade_ctx* C = in_part ? L.pctx : L.ctx;
+    cudaStream_t S = in_part ? L.pstream : L.stream;
     auto b = std::make_shared<BatchBuf>();
     b->n = elems;
     b->heap_bytes = 16 * elems;
     b->heap_off = heap.alloc(b->heap_bytes);
     lk.unlock();
+    if (lane == 1 && green_cu) drv.CtxSetCurrent(in_part ? green_cu : primary_cu);
     // gather into one concatenated batch and rank it
     bool any_w = false;
     for (Request* r : take) any_w |= r->has_w;
@@ -279,8 +446,8 @@ void kascade_server::lane_loop(int lane) {
     if (!staged) {
       d_in = nullptr;
       d_w = nullptr;
-      if (cudaMallocFromPoolAsync(reinterpret_cast<void**>(&d_in), elems * 8, pool, L.stream) != cudaSuccess ||
-          (any_w && cudaMallocFromPoolAsync(reinterpret_cast<void**>(&d_w), elems * 4, pool, L.stream) != cudaSuccess)) {
+      if (cudaMallocFromPoolAsync(reinterpret_cast<void**>(&d_in), elems * 8, pool, S) != cudaSuccess ||
+          (any_w && cudaMallocFromPoolAsync(reinterpret_cast<void**>(&d_w), elems * 4, pool, S) != cudaSuccess)) {
         cudaGetLastError();
         st = KASCADE_ERR_OOM;
       }
@@ -288,7 +455,7 @@ void kascade_server::lane_loop(int lane) {
     if (b->heap_off != NO_CHUNK) {
       b->d_root = reinterpret_cast<uint64_t*>(heap.base + b->heap_off);
       b->d_rank = b->d_root + elems;
-    } else if (cudaMallocFromPoolAsync(reinterpret_cast<void**>(&b->d_root), elems * 16, pool, L.stream) ==
+    } else if (cudaMallocFromPoolAsync(reinterpret_cast<void**>(&b->d_root), elems * 16, pool, S) ==
                cudaSuccess) {
       b->d_rank = b->d_root + elems;
     } else {
@@ -298,51 +465,86 @@ void kascade_server::lane_loop(int lane) {
     const double t_alloc = now_s();
     std::vector<kascade_segment> segs(take.size());
     uint64_t off = 0;
+    uint64_t np = 0;
+    std::vector<Piece> big;  // table overflow (a request beyond the lane's batch limit)
+    auto add_piece = [&](const Piece& pc) {
+      if (np < L.piece_cap) L.h_pieces[np] = pc;
+      else big.push_back(pc);
+      ++np;
+    };
     for (size_t i = 0; i < take.size() && st == KASCADE_OK; ++i) {
       Request* r = take[i];
       r->t_start = t0;
       segs[i] = kascade_segment{off, r->n, r->kind, 0};
-      const void* in_src = r->src_in ? static_cast<const void*>(r->src_in) : static_cast<const void*>(r->h_in.data());
-      const void* w_src = r->src_w ? static_cast<const void*>(r->src_w) : static_cast<const void*>(r->h_w.data());
-      if (r->n) {
-        if (cudaMemcpyAsync(d_in + off, in_src, r->n * 8, cudaMemcpyDefault, L.stream) != cudaSuccess)
+      // lists without weights rank with unit weights; forests ignore weights
+      const uint32_t fill = r->kind == KASCADE_SEG_LIST ? 1u : 0u;
+      if (r->n && !r->src_in) {
+        // host submission: copy now, the gather kernel fills missing weights
+        if (cudaMemcpyAsync(d_in + off, r->h_in.data(), r->n * 8, cudaMemcpyHostToDevice, S) != cudaSuccess ||
+            (any_w && r->has_w &&
+             cudaMemcpyAsync(d_w + off, r->h_w.data(), r->n * 4, cudaMemcpyHostToDevice, S) != cudaSuccess))
           st = KASCADE_ERR_CUDA;
-        if (any_w) {
-          // lists without weights rank with unit weights; forests ignore weights
-          cudaError_t e = cudaSuccess;
-          if (r->has_w) {
-            e = cudaMemcpyAsync(d_w + off, w_src, r->n * 4, cudaMemcpyDefault, L.stream);
-          } else {
-            k_fill_u32<<<(unsigned)std::min<uint64_t>((r->n + 255) / 256, 4096), 256, 0, L.stream>>>(
-                d_w + off, r->n, r->kind == KASCADE_SEG_LIST ? 1u : 0u);
-            e = cudaGetLastError();
-          }
-          if (e != cudaSuccess) st = KASCADE_ERR_CUDA;
-        }
+        if (any_w && !r->has_w)
+          for (uint64_t k = 0; k < r->n; k += PIECE)
+            add_piece(Piece{nullptr, nullptr, off + k, (uint32_t)std::min<uint64_t>(PIECE, r->n - k), fill});
+      } else {
+        for (uint64_t k = 0; k < r->n; k += PIECE)
+          add_piece(Piece{r->src_in + k, r->src_w ? r->src_w + k : nullptr, off + k,
+                          (uint32_t)std::min<uint64_t>(PIECE, r->n - k), fill});
       }
       r->off = off;
       off += r->n;
+    }
+    if (st == KASCADE_OK && np) {
+      Piece* table = L.d_pieces;
+      bool own_table = false;
+      if (!big.empty()) {
+        // rare: a table larger than the lane's; copy it whole from pageable memory
+        std::vector<Piece> all(L.h_pieces, L.h_pieces + L.piece_cap);
+        all.insert(all.end(), big.begin(), big.end());
+        table = nullptr;
+        own_table = true;
+        if (cudaMallocFromPoolAsync(reinterpret_cast<void**>(&table), np * sizeof(Piece), pool, S) !=
+                cudaSuccess ||
+            cudaMemcpyAsync(table, all.data(), np * sizeof(Piece), cudaMemcpyHostToDevice, S) != cudaSuccess)
+          st = KASCADE_ERR_CUDA;
+      } else if (cudaMemcpyAsync(table, L.h_pieces, np * sizeof(Piece), cudaMemcpyHostToDevice, S) !=
+                 cudaSuccess) {
+        st = KASCADE_ERR_CUDA;
+      }
+      if (st == KASCADE_OK) {
+        const unsigned grid = (unsigned)std::min<uint64_t>(np, 148ull * 8);
+        k_gather<<<grid, 256, 0, S>>>(table, (uint32_t)np, d_in, any_w ? d_w : nullptr);
+        if (cudaGetLastError() != cudaSuccess) st = KASCADE_ERR_CUDA;
+      }
+      if (own_table && table) cudaFreeAsync(table, S);
+      cudaGetLastError();
     }
     const double t_gathered = now_s();
     if (st == KASCADE_OK) {
       kascade_opts o;
       kascade_opts_init(&o);
-      st = kascade_rank_batch(L.ctx, segs.data(), (uint32_t)segs.size(), d_in, any_w ? d_w : nullptr, elems,
-                              b->d_root, b->d_rank, &o, L.stream);
+      o.profile = tracing ? 1 : 0;
+      st = kascade_rank_batch(C, segs.data(), (uint32_t)segs.size(), d_in, any_w ? d_w : nullptr, elems,
+                              b->d_root, b->d_rank, &o, S);
     }
     // the staged input is free for the next batch once the stream is done;
     // host submissions drop their copies then too
     if (!staged) {
-      if (d_in) cudaFreeAsync(d_in, L.stream);
-      if (d_w) cudaFreeAsync(d_w, L.stream);
+      if (d_in) cudaFreeAsync(d_in, S);
+      if (d_w) cudaFreeAsync(d_w, S);
     }
-    cudaStreamSynchronize(L.stream);
+    cudaStreamSynchronize(S);
     for (Request* r : take) {
       std::vector<uint64_t>().swap(r->h_in);
       std::vector<uint32_t>().swap(r->h_w);
     }
     const double t1 = now_s();
     lk.lock();
+    if (lane == 0) {
+      lane0_running = false;
+      lane0_last = t1;
+    }
     b->refs = (int)take.size();
     for (Request* r : take) {
       r->batch = b;
@@ -363,7 +565,26 @@ void kascade_server::lane_loop(int lane) {
     lane_elements[lane] += elems;
     lane_busy[lane] += t1 - t0;
     lane_max[lane] = std::max(lane_max[lane], t1 - t0);
-    if (tracing) trace.push_back(BatchTrace{lane, (uint32_t)take.size(), elems, t0, t_alloc, t_gathered, t1});
+    if (tracing) {
+      double gpu = 0, chase = 0;
+      std::vector<std::pair<double, std::string>> ks;
+      for (auto& kv : C->times) {
+        gpu += kv.second.first;
+        if (kv.first == "chase") chase += kv.second.first;
+        ks.emplace_back(kv.second.first, kv.first);
+      }
+      C->times.clear();
+      std::sort(ks.rbegin(), ks.rend());
+      BatchTrace bt{lane, in_part ? 1 : 0, (uint32_t)take.size(), elems, t0, t_alloc, t_gathered, t1, gpu, chase, {0}};
+      std::string top;
+      for (size_t i = 0; i < ks.size() && i < 3; ++i) {
+        char buf[48];
+        std::snprintf(buf, sizeof(buf), "%s%s=%.2f", i ? " " : "", ks[i].second.c_str(), ks[i].first);
+        top += buf;
+      }
+      std::snprintf(bt.top, sizeof(bt.top), "%s", top.c_str());
+      trace.push_back(bt);
+    }
     t_last_done = t1;
     admit_locked();
     cv_done.notify_all();
@@ -382,7 +603,7 @@ KASCADE_API void kascade_server_config_init(kascade_server_config* c) {
   c->max_batch_elements = 1ull << 26;
   c->small_max = 1ull << 20;
   c->small_batch_elements = 1ull << 23;
-  c->latency_sms = 16;
+  c->latency_sms = 80;
   c->result_heap_bytes = 0;
 }
 
@@ -432,7 +653,7 @@ KASCADE_API kascade_status kascade_server_create(const kascade_server_config* cf
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->cfg.device);
     const int keep = (int)s->cfg.latency_sms;
-    if (keep > 0 && keep < sms) kascade_ctx_set_sm_budget(s->lanes[1].ctx, sms - keep);
+    if (keep > 0 && keep < sms) s->lane1_busy_sms = sms - keep;
   }
   // scratch and input staging for a full batch of each lane, so that no
   // batch grows an arena (growing synchronises the device and would stall
@@ -443,9 +664,18 @@ KASCADE_API kascade_status kascade_server_create(const kascade_server_config* cf
     for (int i = 0; i < 2 && ok; ++i) {
       kascade_server::Lane& L = s->lanes[i];
       L.cap = cap[i];
-      ok = kascade_ctx_reserve(L.ctx, kascade_scratch_bytes_root_forest(cap[i])) == KASCADE_OK &&
-           cudaMalloc(reinterpret_cast<void**>(&L.d_in), cap[i] * 8) == cudaSuccess &&
-           cudaMalloc(reinterpret_cast<void**>(&L.d_w), cap[i] * 4) == cudaSuccess;
+      L.piece_cap = cap[i] / PIECE + s->cfg.max_batch_requests + 1;
+      const uint64_t scratch = kascade_scratch_bytes_root_forest(cap[i]);
+      if (i == 1) {
+        ok = cudaMalloc(reinterpret_cast<void**>(&s->lane1_arena), scratch) == cudaSuccess;
+        if (ok) ks::arena_adopt(*L.ctx, s->lane1_arena, scratch);
+      } else {
+        ok = kascade_ctx_reserve(L.ctx, scratch) == KASCADE_OK;
+      }
+      ok = ok && cudaMalloc(reinterpret_cast<void**>(&L.d_in), cap[i] * 8) == cudaSuccess &&
+           cudaMalloc(reinterpret_cast<void**>(&L.d_w), cap[i] * 4) == cudaSuccess &&
+           cudaMallocHost(reinterpret_cast<void**>(&L.h_pieces), L.piece_cap * sizeof(Piece)) == cudaSuccess &&
+           cudaMalloc(reinterpret_cast<void**>(&L.d_pieces), L.piece_cap * sizeof(Piece)) == cudaSuccess;
     }
     uint64_t hb = s->cfg.result_heap_bytes ? s->cfg.result_heap_bytes : s->cfg.hbm_budget_bytes / 2;
     hb = (hb + 255) & ~255ull;
@@ -459,10 +689,12 @@ KASCADE_API kascade_status kascade_server_create(const kascade_server_config* cf
     }
     s->heap.init(hp, hb);
   }
-  if (s->warm_lane(0, 1ull << 20, 1ull << 19) != KASCADE_OK || s->warm_lane(1, 1ull << 22, 1ull << 21) != KASCADE_OK) {
+  if (s->warm_lane(s->lanes[0].ctx, s->lanes[0].stream, s->lanes[0], 1ull << 20, 1ull << 19) != KASCADE_OK ||
+      s->warm_lane(s->lanes[1].ctx, s->lanes[1].stream, s->lanes[1], 1ull << 22, 1ull << 21) != KASCADE_OK) {
     kascade_server_destroy(s);
     return KASCADE_ERR_CUDA;
   }
+  s->setup_partition();
   s->tracing = std::getenv("KASCADE_SERVER_TRACE") != nullptr;
   for (int i = 0; i < 2; ++i) s->lanes[i].th = std::thread([s, i] { s->lane_loop(i); });
   *out = s;
@@ -479,18 +711,21 @@ KASCADE_API kascade_status kascade_server_destroy(kascade_server* s) {
   for (auto& L : s->lanes)
     if (L.th.joinable()) L.th.join();
   if (s->tracing) {
-    // one line per batch: lane, requests, elements, start, buffers
-    // allocated, inputs issued, end (seconds on the steady clock)
+    // one line per batch: lane, in the partition, requests, elements, start, buffers
+    // allocated, inputs issued, end (seconds on the steady clock), summed
+    // kernel time and chase kernel time (ms), the three longest kernels
     if (FILE* f = std::fopen(std::getenv("KASCADE_SERVER_TRACE"), "w")) {
-      std::fprintf(f, "lane,requests,elements,t_start,t_alloc,t_gathered,t_end\n");
+      std::fprintf(f, "lane,part,requests,elements,t_start,t_alloc,t_gathered,t_end,gpu_ms,chase_ms,top\n");
       for (const BatchTrace& b : s->trace)
-        std::fprintf(f, "%d,%u,%llu,%.6f,%.6f,%.6f,%.6f\n", b.lane, b.requests, (unsigned long long)b.elements,
-                     b.t_start, b.t_alloc, b.t_gathered, b.t_end);
+        std::fprintf(f, "%d,%d,%u,%llu,%.6f,%.6f,%.6f,%.6f,%.4f,%.4f,%s\n", b.lane, b.part, b.requests,
+                     (unsigned long long)b.elements, b.t_start, b.t_alloc, b.t_gathered, b.t_end, b.gpu_ms, b.chase_ms,
+                     b.top);
       std::fclose(f);
     }
   }
   cudaSetDevice(s->cfg.device);
   cudaDeviceSynchronize();
+  s->drop_partition();
   std::vector<std::shared_ptr<BatchBuf>> bufs;
   for (auto& kv : s->reqs)
     if (kv.second->batch) bufs.push_back(kv.second->batch);
@@ -507,7 +742,10 @@ KASCADE_API kascade_status kascade_server_destroy(kascade_server* s) {
     if (L.stream) cudaStreamDestroy(L.stream);
     if (L.d_in) cudaFree(L.d_in);
     if (L.d_w) cudaFree(L.d_w);
+    if (L.h_pieces) cudaFreeHost(L.h_pieces);
+    if (L.d_pieces) cudaFree(L.d_pieces);
   }
+  if (s->lane1_arena) cudaFree(s->lane1_arena);
   if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
   if (s->pool) cudaMemPoolDestroy(s->pool);
   cudaGetLastError();
@@ -664,6 +902,8 @@ KASCADE_API kascade_status kascade_server_get_stats(kascade_server* s, kascade_s
     out->lane_busy_ms[i] = 1e3 * s->lane_busy[i];
     out->lane_max_batch_ms[i] = 1e3 * s->lane_max[i];
   }
+  out->partition_sms = (uint64_t)s->partition_sms;
+  out->partition_batches = s->partition_batches;
   return KASCADE_OK;
 }
 
@@ -678,6 +918,7 @@ KASCADE_API kascade_status kascade_server_reset_stats(kascade_server* s) {
     s->lane_batches[i] = s->lane_elements[i] = 0;
     s->lane_busy[i] = s->lane_max[i] = 0;
   }
+  s->partition_batches = 0;
   s->t_first_submit = 0;
   s->t_last_done = 0;
   return KASCADE_OK;
