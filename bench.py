@@ -120,6 +120,14 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def dist_backend() -> str:
+    """nccl on GPUs; gloo where there are none (the host-side multi-rank
+    tests), or when KASCADE_BENCH_BACKEND says so."""
+    import torch
+
+    return os.environ.get("KASCADE_BENCH_BACKEND") or ("nccl" if torch.cuda.is_available() else "gloo")
+
+
 def dist_setup():
     import torch
 
@@ -131,11 +139,14 @@ def dist_setup():
 
         import torch.distributed as dist
 
+        if dist_backend() == "nccl":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                    device_id=torch.device(f"cuda:{local}"))
+        else:
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
+    elif torch.cuda.is_available():
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device(f"cuda:{local}"))
-    else:
-        torch.cuda.set_device(0 if not torch.cuda.is_available() else local)
     return world, rank, local
 
 
@@ -152,9 +163,17 @@ def max_over_ranks(x: float, world: int) -> float:
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if dist_backend() == "nccl" else "cpu")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def whole_job(n_per_rank: int, t_ms_local: float, steps: int, world: int) -> tuple[float, float]:
+    """(ms per step, whole-job elements/s): the slowest rank's time, every
+    rank's elements (each rank ranks its own replica)."""
+    t_ms = max_over_ranks(t_ms_local, world)
+    ms_per_step = t_ms / steps
+    return ms_per_step, n_per_rank * world / (ms_per_step / 1000.0)
 
 
 def cpu_reference_time(n_sample: int, wl: str, reps: int = 1) -> tuple[float, str, str]:
@@ -479,10 +498,7 @@ def main():
     torch.cuda.synchronize()
     barrier(world)
     clk = clocks.stop()
-    t_ms = ev0.elapsed_time(ev1)
-    t_ms = max_over_ranks(t_ms, world)
-    ms_per_step = t_ms / args.steps
-    value = n * world / (ms_per_step / 1000.0)
+    ms_per_step, value = whole_job(n, ev0.elapsed_time(ev1), args.steps, world)
     ktimes = ctx.kernel_times()
     launches = sum(c for (_, c) in ktimes.values())
     step_kernel_ms = {k: v[0] / args.steps for k, v in ktimes.items()}

@@ -120,6 +120,24 @@ __device__ __forceinline__ Out ld_out(const Out* p) {
   o.pad = v.w;
   return o;
 }
+// The same load, with the line kept in L2 ahead of streaming traffic: for
+// small tables read at random by every element (a level's ruler results).
+__device__ __forceinline__ uint64_t l2_keep_policy() {
+  uint64_t pol;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+__device__ __forceinline__ Out ld_out_keep(const Out* p, uint64_t pol) {
+  uint32_t a, b, c, d;
+  asm volatile("ld.global.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
+               : "=r"(a), "=r"(b), "=r"(c), "=r"(d)
+               : "l"(p), "l"(pol));
+  Out o;
+  o.rank = (uint64_t)a | ((uint64_t)b << 32);
+  o.root = c;
+  o.pad = d;
+  return o;
+}
 __device__ __forceinline__ void st_out(Out* p, uint64_t rank, uint32_t root) {
   __stcg(reinterpret_cast<uint4*>(p), make_uint4((uint32_t)rank, (uint32_t)(rank >> 32), root, 0u));
 }

@@ -26,20 +26,25 @@ namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int PREP_ITEMS = 8;
-constexpr int PROP_ITEMS = 4;
+constexpr int PROP_ITEMS = 8;
 constexpr int BASE_THREADS = 1024;
 constexpr int BASE_PER_THREAD = 8;  // base_max <= BASE_THREADS * BASE_PER_THREAD
 
+// Weight sources; T is the narrowest type that holds one weight (fewer live
+// registers in the prepare kernel).
 struct WUnit {
-  __device__ __forceinline__ uint64_t operator()(uint64_t) const { return 1ull; }
+  using T = uint32_t;
+  __device__ __forceinline__ T operator()(uint64_t) const { return 1u; }
 };
 struct WU32 {
+  using T = uint32_t;
   const uint32_t* p;
-  __device__ __forceinline__ uint64_t operator()(uint64_t x) const { return (uint64_t)__ldcs(p + x); }
+  __device__ __forceinline__ T operator()(uint64_t x) const { return __ldcs(p + x); }
 };
 struct WI64 {
+  using T = uint64_t;
   const int64_t* p;
-  __device__ __forceinline__ uint64_t operator()(uint64_t x) const {
+  __device__ __forceinline__ T operator()(uint64_t x) const {
     return (uint64_t)__ldcs(reinterpret_cast<const long long*>(p) + x);
   }
 };
@@ -56,7 +61,7 @@ inline uint32_t salt_for(uint32_t seed, int level) { return mix32(seed + 0x9E377
 // One atomicAdd per 2048-element tile hands out dense ruler ids.
 // ---------------------------------------------------------------------------
 template <class W>
-__global__ void __launch_bounds__(256) k_prepare_arrays(const uint64_t* __restrict__ succ, W w, uint32_t n,
+__global__ void __launch_bounds__(256, 4) k_prepare_arrays(const uint64_t* __restrict__ succ, W w, uint32_t n,
                                                         Rec* __restrict__ rec, uint32_t* __restrict__ ruler_elem,
                                                         uint32_t* __restrict__ counter, uint32_t salt,
                                                         uint32_t thresh, DevStatus* st) {
@@ -65,7 +70,7 @@ __global__ void __launch_bounds__(256) k_prepare_arrays(const uint64_t* __restri
   const uint64_t tile_sz = (uint64_t)blockDim.x * PREP_ITEMS;
   for (uint64_t tile = (uint64_t)blockIdx.x * tile_sz; tile < n; tile += (uint64_t)gridDim.x * tile_sz) {
     uint32_t sv[PREP_ITEMS];
-    uint64_t wv[PREP_ITEMS];
+    typename W::T wv[PREP_ITEMS];
     uint32_t rl = 0, cnt = 0;
 #pragma unroll
     for (int i = 0; i < PREP_ITEMS; ++i) {
@@ -304,6 +309,7 @@ template <class Sink>
 __global__ void __launch_bounds__(256) k_propagate(const Rec* __restrict__ rec, uint32_t n_out, uint32_t n_all,
                                                    const Out* __restrict__ out_next, Sink sink, DevStatus* st) {
   const uint32_t stride = gridDim.x * blockDim.x;
+  const uint64_t pol = l2_keep_policy();
   for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x * PROP_ITEMS + threadIdx.x; base < n_out;
        base += (uint64_t)stride * PROP_ITEMS) {
     Rec rv[PROP_ITEMS];
@@ -312,11 +318,22 @@ __global__ void __launch_bounds__(256) k_propagate(const Rec* __restrict__ rec, 
       uint64_t x = base + (uint64_t)i * blockDim.x;
       if (x < n_out) rv[i] = ld_rec_cs(rec + x);
     }
+    // every stamped element's ruler result, all loads in flight together
+    // (they would otherwise wait behind the previous element's stores)
+    Out ov[PROP_ITEMS];
+#pragma unroll
+    for (int i = 0; i < PROP_ITEMS; ++i) {
+      uint64_t x = base + (uint64_t)i * blockDim.x;
+      ov[i] = Out{0, 0, 0};
+      if (x < n_out && !tag_unreached(rv[i].c))
+        ov[i] = ld_out_keep(out_next + (tag_ruler(rv[i].c) ? tag_id(rv[i].c) : rv[i].c), pol);
+    }
 #pragma unroll
     for (int i = 0; i < PROP_ITEMS; ++i) {
       uint64_t x = base + (uint64_t)i * blockDim.x;
       if (x >= n_out) continue;
       Rec r = rv[i];
+      Out o = ov[i];
       bool is_root = false;
       uint64_t acc = 0;
       if (tag_unreached(r.c)) {
@@ -342,17 +359,16 @@ __global__ void __launch_bounds__(256) k_propagate(const Rec* __restrict__ rec, 
           set_error(st, KASCADE_ERR_CYCLE, x);
           continue;
         }
+        o = ld_out(out_next + (tag_ruler(r.c) ? tag_id(r.c) : r.c));
       } else if (tag_ruler(r.c)) {
         is_root = (r.b == (uint32_t)x);
       }
       uint64_t rank;
       uint32_t root;
       if (tag_ruler(r.c)) {
-        Out o = ld_out(out_next + tag_id(r.c));
         rank = o.rank + acc;
         root = o.root;
       } else {
-        Out o = ld_out(out_next + r.c);
         rank = o.rank - r.a + acc;
         root = o.root;
       }
