@@ -26,7 +26,10 @@ from .api import (  # noqa: F401
     async_pointer_doubling,
     batch_sizes,
     gen_batch,
+    get_class_launch,
     get_size_classes,
+    load_tuning,
+    set_class_launch,
     make_segments,
     rank_batch,
     set_size_classes,

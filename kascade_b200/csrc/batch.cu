@@ -154,6 +154,7 @@ kascade_status rank_batch_impl(kascade_ctx& ctx, const kascade_segment* segs, ui
   std::vector<uint32_t> fd, foff, fth;
   std::vector<unsigned long long> seg_off(nseg);
   uint64_t expect = 0, F = 0;
+  std::vector<uint64_t> class_elems(ctx.class_max.size(), 0);
   items.reserve(total / ITEM + nseg);
   for (uint32_t i = 0; i < nseg; ++i) {
     const kascade_segment& g = segs[i];
@@ -161,8 +162,9 @@ kascade_status rank_batch_impl(kascade_ctx& ctx, const kascade_segment* segs, ui
       return KASCADE_ERR_INVALID_ARG;
     expect += g.size;
     const bool forest = g.kind == KASCADE_SEG_FOREST;
-    const uint32_t spacing =
-        (opts && opts->ruler_spacing) ? opts->ruler_spacing : spacing_for(ctx, forest ? 2 * g.size : g.size);
+    const uint64_t records = forest ? 2 * g.size : g.size;
+    const uint32_t spacing = (opts && opts->ruler_spacing) ? opts->ruler_spacing : spacing_for(ctx, records);
+    class_elems[ctx.class_of(records)] += records;
     dsegs[i] = DSeg{g.offset, (uint32_t)g.size, g.kind, thresh_of(spacing), (uint32_t)F};
     seg_off[i] = g.offset;
     if (forest) {
@@ -214,6 +216,14 @@ kascade_status rank_batch_impl(kascade_ctx& ctx, const kascade_segment* segs, ui
   KS_CUDA(cudaMemsetAsync(ctr, 0, sizeof(uint32_t), s));
 
   Params p = make_params(ctx, opts, M);
+  {
+    // one chase launch serves every instance: its chains and block size come
+    // from the class that holds most of the batch's elements
+    const size_t k = std::max_element(class_elems.begin(), class_elems.end()) - class_elems.begin();
+    if (!(opts && opts->chains_per_thread)) p.chains = ctx.class_chains[k];
+    if (!(opts && opts->block_size)) p.block = (ctx.class_block[k] == 128 || ctx.class_block[k] == 512)
+                                                   ? ctx.class_block[k] : 256u;
+  }
   const uint32_t salt = mix32(p.seed ^ 0x62617463u);
   {
     ProfScope ps(ctx, "batch_prepare", s);

@@ -88,7 +88,7 @@ __device__ __forceinline__ void log_append(bool emit, uint32_t x, uint32_t id, u
 }
 
 template <int C>
-__global__ void __launch_bounds__(256) k_chase_log(const Rec* __restrict__ rec, uint32_t n,
+__global__ void __launch_bounds__(512) k_chase_log(const Rec* __restrict__ rec, uint32_t n,
                                                    const uint32_t* __restrict__ ruler_elem, uint32_t r,
                                                    Rec* __restrict__ rec_next, uint32_t* __restrict__ work,
                                                    LogEnt* __restrict__ log, uint32_t* __restrict__ chunk_fill,
@@ -386,33 +386,35 @@ __global__ void __launch_bounds__(256) k_walk_unreached(const Rec* __restrict__ 
   }
 }
 
-int g_chase_occ[5] = {-1, -1, -1, -1, -1};
+int g_chase_occ[5][3] = {{-1, -1, -1}, {-1, -1, -1}, {-1, -1, -1}, {-1, -1, -1}, {-1, -1, -1}};
 
 template <int C>
 kascade_status launch_chase_log_c(kascade_ctx& ctx, const Rec* rec, uint32_t n, const uint32_t* ruler_elem, uint32_t r,
                                   Rec* rec_next, uint32_t* work, LogEnt* log, uint32_t* chunk_fill,
                                   uint32_t* chunk_cursor, uint32_t nchunks, uint32_t max_hops, unsigned grid,
-                                  cudaStream_t s) {
+                                  uint32_t block, cudaStream_t s) {
   ProfScope ps(ctx, "chase", s);
-  k_chase_log<C><<<grid, 256, 0, s>>>(rec, n, ruler_elem, r, rec_next, work, log, chunk_fill, chunk_cursor, nchunks,
+  k_chase_log<C><<<grid, block, 0, s>>>(rec, n, ruler_elem, r, rec_next, work, log, chunk_fill, chunk_cursor, nchunks,
                                       max_hops, ctx.d_status);
   KS_CHECK_LAUNCH();
   return KASCADE_OK;
 }
 
 template <int C>
-unsigned chase_grid(const kascade_ctx& ctx, uint32_t r) {
-  if (g_chase_occ[C] < 0) {
+unsigned chase_grid(const kascade_ctx& ctx, uint32_t r, uint32_t block) {
+  const int bi = block == 128 ? 0 : block == 512 ? 2 : 1;
+  if (g_chase_occ[C][bi] < 0) {
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_chase_log<C>, 256, 0) != cudaSuccess) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_chase_log<C>, (int)block, 0) != cudaSuccess) {
       cudaGetLastError();
       nb = 1;
     }
-    g_chase_occ[C] = nb < 1 ? 1 : nb;
+    g_chase_occ[C][bi] = nb < 1 ? 1 : nb;
   }
-  unsigned grid = (unsigned)(ctx.usable_sms() * g_chase_occ[C]);
+  unsigned grid = (unsigned)(ctx.usable_sms() * g_chase_occ[C][bi]);
+  const uint64_t warps_per_block = block / 32;
   const uint64_t need = ((uint64_t)r + 32ull * C - 1) / (32ull * C);
-  const uint64_t need_blocks = (need + 7) / 8;
+  const uint64_t need_blocks = (need + warps_per_block - 1) / warps_per_block;
   if (need_blocks < grid) grid = (unsigned)(need_blocks ? need_blocks : 1);
   return grid;
 }
@@ -422,8 +424,11 @@ unsigned chase_grid(const kascade_ctx& ctx, uint32_t r) {
 kascade_status rank_level0_log(kascade_ctx& ctx, const Rec* rec, uint32_t n, uint32_t r0, const uint32_t* ruler_elem0,
                                const LogTarget& t, const Params& p, cudaStream_t s) {
   const int C = (p.chains == 1 || p.chains == 4) ? (int)p.chains : 2;
-  const unsigned grid = C == 1 ? chase_grid<1>(ctx, r0) : C == 4 ? chase_grid<4>(ctx, r0) : chase_grid<2>(ctx, r0);
-  const uint64_t warps = (uint64_t)grid * 8;
+  const uint32_t block = p.block;
+  const unsigned grid = C == 1   ? chase_grid<1>(ctx, r0, block)
+                        : C == 4 ? chase_grid<4>(ctx, r0, block)
+                                 : chase_grid<2>(ctx, r0, block);
+  const uint64_t warps = (uint64_t)grid * (block / 32);
   const uint32_t nchunks = (uint32_t)(((uint64_t)n + LOG_CHUNK - 1) / LOG_CHUNK + warps + 1);
   LogEnt* log = alloc<LogEnt>(ctx, (uint64_t)nchunks * LOG_CHUNK);
   uint32_t* chunk_fill = alloc<uint32_t>(ctx, nchunks);
@@ -444,15 +449,15 @@ kascade_status rank_level0_log(kascade_ctx& ctx, const Rec* rec, uint32_t n, uin
   switch (C) {
     case 1:
       KS_TRY(launch_chase_log_c<1>(ctx, rec, n, ruler_elem0, r0, rec1, chase_work, log, chunk_fill, chunk_cursor,
-                                   nchunks, max_hops, grid, s));
+                                   nchunks, max_hops, grid, block, s));
       break;
     case 4:
       KS_TRY(launch_chase_log_c<4>(ctx, rec, n, ruler_elem0, r0, rec1, chase_work, log, chunk_fill, chunk_cursor,
-                                   nchunks, max_hops, grid, s));
+                                   nchunks, max_hops, grid, block, s));
       break;
     default:
       KS_TRY(launch_chase_log_c<2>(ctx, rec, n, ruler_elem0, r0, rec1, chase_work, log, chunk_fill, chunk_cursor,
-                                   nchunks, max_hops, grid, s));
+                                   nchunks, max_hops, grid, block, s));
   }
   {
     // a chain hit the hop cap: let the caller rerun level 0 on the stamping path

@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "tuned_classes.h"
 
 struct kascade_ctx {
   int device = 0;
@@ -48,9 +49,18 @@ struct kascade_ctx {
   cudaStream_t last_stream = nullptr;
   bool async_pending = false;
   // size classes: instances of at most class_max[i] elements use a mean ruler
-  // spacing of class_spacing[i] (set by the autotuner)
-  std::vector<unsigned long long> class_max{1ull << 10, 1ull << 16, 1ull << 22, ~0ull};
-  std::vector<uint32_t> class_spacing{8u, 16u, 32u, 48u};
+  // spacing of class_spacing[i]; a call (or a batch, by the class holding
+  // most of its elements) chases with class_chains[i] chains per thread in
+  // blocks of class_block[i] threads.  Defaults: the autotuner's table.
+  std::vector<unsigned long long> class_max = KS_TUNED_MAX;
+  std::vector<uint32_t> class_spacing = KS_TUNED_SPACING;
+  std::vector<uint32_t> class_chains = KS_TUNED_CHAINS;
+  std::vector<uint32_t> class_block = KS_TUNED_BLOCK;
+  int class_of(unsigned long long n) const {
+    for (size_t i = 0; i < class_max.size(); ++i)
+      if (n <= class_max[i]) return (int)i;
+    return (int)class_max.size() - 1;
+  }
   // SMs' worth of block slots this context's kernels may occupy (0 = all):
   // grids are sized for this many SMs, so that work on other streams (a
   // server's latency lane) always finds free slots.  Read at every launch;

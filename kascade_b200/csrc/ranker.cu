@@ -194,7 +194,7 @@ __device__ __forceinline__ void end_chain_on_error(Rec* rec_next, uint32_t id) {
 // (weight = distance to that ruler, successor = that ruler's id).
 // ---------------------------------------------------------------------------
 template <int C>
-__global__ void __launch_bounds__(256) k_chase(Rec* __restrict__ rec, uint32_t n,
+__global__ void __launch_bounds__(512) k_chase(Rec* __restrict__ rec, uint32_t n,
                                                const uint32_t* __restrict__ ruler_elem, uint32_t r,
                                                Rec* __restrict__ rec_next, uint32_t* __restrict__ work,
                                                DevStatus* st) {
@@ -524,15 +524,17 @@ int occupancy(K kernel, int block, size_t smem) {
 
 template <int C>
 kascade_status launch_chase_c(kascade_ctx& ctx, Rec* rec, uint32_t n, const uint32_t* ruler_elem, uint32_t r,
-                              Rec* rec_next, uint32_t* work, cudaStream_t s) {
-  static int occ = -1;
-  if (occ < 0) occ = occupancy(k_chase<C>, 256, 0);
-  unsigned grid = (unsigned)(ctx.usable_sms() * occ);
+                              Rec* rec_next, uint32_t* work, uint32_t block, cudaStream_t s) {
+  static int occ[3] = {-1, -1, -1};  // blocks of 128, 256, 512 threads
+  const int bi = block == 128 ? 0 : block == 512 ? 2 : 1;
+  if (occ[bi] < 0) occ[bi] = occupancy(k_chase<C>, (int)block, 0);
+  unsigned grid = (unsigned)(ctx.usable_sms() * occ[bi]);
+  const uint64_t warps_per_block = block / 32;
   uint64_t need = ((uint64_t)r + 32ull * C - 1) / (32ull * C);  // warps worth of work
-  uint64_t need_blocks = (need + 7) / 8;
+  uint64_t need_blocks = (need + warps_per_block - 1) / warps_per_block;
   if (need_blocks < grid) grid = (unsigned)(need_blocks ? need_blocks : 1);
   ProfScope ps(ctx, "chase", s);
-  k_chase<C><<<grid, 256, 0, s>>>(rec, n, ruler_elem, r, rec_next, work, ctx.d_status);
+  k_chase<C><<<grid, block, 0, s>>>(rec, n, ruler_elem, r, rec_next, work, ctx.d_status);
   KS_CHECK_LAUNCH();
   return KASCADE_OK;
 }
@@ -544,11 +546,11 @@ kascade_status launch_chase(kascade_ctx& ctx, Rec* rec, uint32_t n, const uint32
   KS_CUDA(cudaMemsetAsync(work, 0, sizeof(uint32_t), s));
   switch (p.chains) {
     case 1:
-      return launch_chase_c<1>(ctx, rec, n, ruler_elem, r, rec_next, work, s);
+      return launch_chase_c<1>(ctx, rec, n, ruler_elem, r, rec_next, work, p.block, s);
     case 4:
-      return launch_chase_c<4>(ctx, rec, n, ruler_elem, r, rec_next, work, s);
+      return launch_chase_c<4>(ctx, rec, n, ruler_elem, r, rec_next, work, p.block, s);
     default:
-      return launch_chase_c<2>(ctx, rec, n, ruler_elem, r, rec_next, work, s);
+      return launch_chase_c<2>(ctx, rec, n, ruler_elem, r, rec_next, work, p.block, s);
   }
 }
 
@@ -593,6 +595,11 @@ Params make_params(const kascade_ctx& ctx, const kascade_opts* o, uint64_t n) {
   // against ruler-table size; these defaults are the tuned values for
   // random lists on B200 (see the autotune table in the batch path).
   p.spacing0 = spacing_for(ctx, n);
+  {
+    const int k = ctx.class_of(n);
+    p.chains = ctx.class_chains[k];
+    p.block = ctx.class_block[k];
+  }
   if (o) {
     if (o->ruler_spacing) p.spacing0 = o->ruler_spacing;
     if (o->ruler_spacing_deep) p.spacing_deep = o->ruler_spacing_deep;
@@ -609,6 +616,7 @@ Params make_params(const kascade_ctx& ctx, const kascade_opts* o, uint64_t n) {
     }
   }
   if (p.base_max > (uint32_t)(BASE_THREADS * BASE_PER_THREAD)) p.base_max = BASE_THREADS * BASE_PER_THREAD;
+  if (p.block != 128 && p.block != 512) p.block = 256;
   if (p.spacing0 < 2) p.spacing0 = 2;
   if (p.spacing_deep < 2) p.spacing_deep = 2;
   return p;

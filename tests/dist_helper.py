@@ -18,8 +18,10 @@ def main() -> None:
     bench.barrier(world)
     t_local = 10.0 * (rank + 1)  # rank 1 is the slower one
     ms, value = bench.whole_job(1000, t_local, 5, world)
-    print(json.dumps({"rank": rank, "world": world, "ms_per_step": ms, "value": value,
-                      "backend": bench.dist_backend()}), flush=True)
+    # one file per rank (the ranks share stdout, where lines can interleave)
+    out = Path(os.environ["KASCADE_DIST_OUT"]) / f"rank{rank}.json"
+    out.write_text(json.dumps({"rank": rank, "world": world, "ms_per_step": ms, "value": value,
+                               "backend": bench.dist_backend()}))
     bench.barrier(world)
     import torch.distributed as dist
 

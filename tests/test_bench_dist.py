@@ -20,8 +20,8 @@ def _free_port() -> int:
         return s.getsockname()[1]
 
 
-def _torchrun(args, timeout=240):
-    env = dict(os.environ, KASCADE_BENCH_BACKEND="gloo", CUDA_VISIBLE_DEVICES="")
+def _torchrun(args, timeout=240, extra_env=None):
+    env = dict(os.environ, KASCADE_BENCH_BACKEND="gloo", CUDA_VISIBLE_DEVICES="", **(extra_env or {}))
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes", "1", "--nproc-per-node", "2",
            "--master-addr", "127.0.0.1", "--master-port", str(_free_port())] + args
     return subprocess.run(cmd, cwd=ROOT, env=env, capture_output=True, text=True, timeout=timeout)
@@ -39,10 +39,10 @@ def _json_lines(text):
     return out
 
 
-def test_whole_job_takes_the_slowest_rank_and_every_ranks_elements():
-    res = _torchrun([str(ROOT / "tests" / "dist_helper.py")])
+def test_whole_job_takes_the_slowest_rank_and_every_ranks_elements(tmp_path):
+    res = _torchrun([str(ROOT / "tests" / "dist_helper.py")], extra_env={"KASCADE_DIST_OUT": str(tmp_path)})
     assert res.returncode == 0, res.stderr[-2000:]
-    lines = _json_lines(res.stdout)
+    lines = [json.loads((tmp_path / f"rank{r}.json").read_text()) for r in (0, 1)]
     assert sorted(d["rank"] for d in lines) == [0, 1]
     for d in lines:
         assert d["world"] == 2 and d["backend"] == "gloo"

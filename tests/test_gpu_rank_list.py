@@ -25,7 +25,10 @@ TUNINGS = {"default": {}, "deep": DEEP, "sparse": SPARSE, "chains1": dict(DEEP, 
            "log_chains1": dict(DEEP, level0_mode=2, chains_per_thread=1),
            "log_chains4": dict(DEEP, level0_mode=2, chains_per_thread=4),
            # a hop cap so small that level 0 always falls back to the stamping chase
-           "log_fallback": dict(DEEP, level0_mode=2, max_chain=2)}
+           "log_fallback": dict(DEEP, level0_mode=2, max_chain=2),
+           # chase block sizes the autotuner may pick
+           "block128": dict(DEEP, block_size=128), "block512_chains4": dict(DEEP, block_size=512, chains_per_thread=4),
+           "log_block512": dict(DEEP, level0_mode=2, block_size=512)}
 
 
 @pytest.mark.parametrize("tuning", list(TUNINGS))
