@@ -265,12 +265,16 @@ KASCADE_API kascade_status kascade_ctx_set_size_classes(kascade_ctx* ctx, const 
 KASCADE_API int kascade_ctx_get_size_classes(kascade_ctx* ctx, uint64_t* max_size, uint32_t* spacing,
                                              int cap);
 /* Per size class (same count and order as the size-class table): chains in
- * flight per chase thread (1, 2 or 4) and chase block size (128, 256 or 512).
- * A call uses the class of its size; a batch the class that holds most of
- * its elements.  kascade_ctx_set_size_classes resets these to 2 and 256. */
+ * flight per chase thread (1, 2 or 4), chase block size (128, 256 or 512) and
+ * the ruler spacing for calls that rank one instance on their own (NULL:
+ * unchanged; the table's spacing applies inside batches).  A call uses the
+ * class of its size; a batch the class that holds most of its elements.
+ * kascade_ctx_set_size_classes resets these to 2, 256 and its own spacing. */
 KASCADE_API kascade_status kascade_ctx_set_class_launch(kascade_ctx* ctx, const uint32_t* chains,
-                                                        const uint32_t* block, uint32_t count);
-KASCADE_API int kascade_ctx_get_class_launch(kascade_ctx* ctx, uint32_t* chains, uint32_t* block, int cap);
+                                                        const uint32_t* block, const uint32_t* single_spacing,
+                                                        uint32_t count);
+KASCADE_API int kascade_ctx_get_class_launch(kascade_ctx* ctx, uint32_t* chains, uint32_t* block,
+                                             uint32_t* single_spacing, int cap);
 /* Size this context's grids for `sms` SMs (0 = all SMs): its persistent and
  * grid-stride kernels then hold that many SMs' worth of block slots, and
  * work on other streams (the server's latency lane) finds the rest free. */

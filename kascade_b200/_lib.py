@@ -142,8 +142,8 @@ _SIGS = {
     ),
     "kascade_ctx_set_size_classes": (_status, [_ctx_p, P(c_u64), P(c_u32), c_u32]),
     "kascade_ctx_get_size_classes": (c_int, [_ctx_p, P(c_u64), P(c_u32), c_int]),
-    "kascade_ctx_set_class_launch": (_status, [_ctx_p, P(c_u32), P(c_u32), c_u32]),
-    "kascade_ctx_get_class_launch": (c_int, [_ctx_p, P(c_u32), P(c_u32), c_int]),
+    "kascade_ctx_set_class_launch": (_status, [_ctx_p, P(c_u32), P(c_u32), P(c_u32), c_u32]),
+    "kascade_ctx_get_class_launch": (c_int, [_ctx_p, P(c_u32), P(c_u32), P(c_u32), c_int]),
     "kascade_ctx_set_sm_budget": (_status, [_ctx_p, c_int]),
     "kascade_server_config_init": (None, [P(ServerConfig)]),
     "kascade_server_create": (_status, [P(ServerConfig), P(c_void_p)]),

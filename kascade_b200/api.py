@@ -482,27 +482,32 @@ def get_size_classes(ctx: Context):
     return [int(ms[i]) for i in range(k)], [int(sp[i]) for i in range(k)]
 
 
-def set_class_launch(ctx: Context, chains, blocks) -> None:
-    """Per size class: chains per chase thread (1, 2, 4) and chase block size
-    (128, 256, 512); one entry per class of the current table."""
+def set_class_launch(ctx: Context, chains, blocks, single_spacing=None) -> None:
+    """Per size class: chains per chase thread (1, 2, 4), chase block size
+    (128, 256, 512) and, optionally, the ruler spacing of calls that rank one
+    instance on their own; one entry per class of the current table."""
     k = len(chains)
     ch = (ctypes.c_uint32 * k)(*[int(x) for x in chains])
     bl = (ctypes.c_uint32 * k)(*[int(x) for x in blocks])
-    check(lib.kascade_ctx_set_class_launch(ctx.handle, ch, bl, k), "kascade_ctx_set_class_launch", ctx.handle)
+    ss = None if single_spacing is None else (ctypes.c_uint32 * k)(*[int(x) for x in single_spacing])
+    check(lib.kascade_ctx_set_class_launch(ctx.handle, ch, bl, ss, k), "kascade_ctx_set_class_launch", ctx.handle)
 
 
 def get_class_launch(ctx: Context):
+    """(chains, blocks, single-call spacings) per size class."""
     ch = (ctypes.c_uint32 * 64)()
     bl = (ctypes.c_uint32 * 64)()
-    k = lib.kascade_ctx_get_class_launch(ctx.handle, ch, bl, 64)
-    return [int(ch[i]) for i in range(k)], [int(bl[i]) for i in range(k)]
+    ss = (ctypes.c_uint32 * 64)()
+    k = lib.kascade_ctx_get_class_launch(ctx.handle, ch, bl, ss, 64)
+    return [int(ch[i]) for i in range(k)], [int(bl[i]) for i in range(k)], [int(ss[i]) for i in range(k)]
 
 
 def load_tuning(ctx: Context, table: dict) -> None:
     """Install an autotuner table (the dict autotune.tune returns)."""
     cls = table["classes"]
     set_size_classes(ctx, [c["max"] for c in cls], [c["spacing"] for c in cls])
-    set_class_launch(ctx, [c["chains"] for c in cls], [c["block"] for c in cls])
+    set_class_launch(ctx, [c["chains"] for c in cls], [c["block"] for c in cls],
+                     [c.get("spacing_single", c["spacing"]) for c in cls])
 
 
 def batch_sizes(count: int, seed: int, lo_log2: int = 6, hi_log2: int = 22, total: Optional[int] = None,

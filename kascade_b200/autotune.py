@@ -6,6 +6,8 @@ recursive forests, the batched workload's mix) and picks
 
   1. the mean ruler spacing (ruler density), then, at that spacing,
   2. the chains in flight per chase thread and the chase block size,
+  3. the ruler spacing for calls that rank one instance on their own (up to
+     32 of the class's instances, one call each),
 
 by measured elements/s.  The table it returns is what `load_tuning` installs
 in a context; `write_header` turns it into the library's built-in defaults
@@ -107,9 +109,29 @@ def tune(device: int = 0, total: int = 1 << 24, reps: int = 3, log=print) -> dic
         torch.cuda.synchronize()
         if not (torch.equal(root, ref_root) and torch.equal(rank, ref_rank)):
             raise RuntimeError(f"class {k}: tuned parameters change the results")
+        # one instance per call: up to 32 of the class's instances, back to back
+        offs = np.concatenate([[0], np.cumsum(sizes)])
+        picks = list(range(min(32, len(sizes))))
+
+        def run_single(t):
+            for i in picks:
+                a, b_ = int(offs[i]), int(offs[i + 1])
+                if kinds[i] == kb.SEG_LIST:
+                    kb.rank_list(inp[a:b_], w[a:b_], tuning=t, root_out=root[a:b_], rank_out=rank[a:b_], ctx=ctx)
+                else:
+                    kb.root_forest(inp[a:b_], tuning=t, root_out=root[a:b_], depth_out=rank[a:b_], ctx=ctx)
+
+        best_single = None
+        for sp in SPACINGS:
+            t = kb.GpuTuning(ruler_spacing=sp, chains_per_thread=chains, block_size=block)
+            ms1 = _time_ms(lambda: run_single(t), reps)
+            if best_single is None or ms1 < best_single[0]:
+                best_single = (ms1, sp)
+        n_single = int(offs[len(picks)])
         entry = {"max": int(min(cmax, (1 << 64) - 1)), "spacing": spacing, "chains": chains, "block": block,
-                 "instances": int(len(sizes)), "elements": n, "ms": round(ms, 4),
-                 "elements_per_s": n / (ms / 1000.0)}
+                 "spacing_single": best_single[1], "instances": int(len(sizes)), "elements": n, "ms": round(ms, 4),
+                 "elements_per_s": n / (ms / 1000.0), "single_calls": len(picks),
+                 "single_elements_per_s": n_single / (best_single[0] / 1000.0)}
         log(json.dumps(entry))
         classes.append(entry)
         del inp, w, root, rank, ref_root, ref_rank
@@ -137,6 +159,7 @@ def write_header(table: dict, path) -> None:
 #define KS_TUNED_COUNT {len(cls)}
 #define KS_TUNED_MAX {arr('max', max_fmt)}
 #define KS_TUNED_SPACING {arr('spacing', lambda v: f'{v}u')}
+#define KS_TUNED_SPACING_SINGLE {arr('spacing_single', lambda v: f'{v}u')}
 #define KS_TUNED_CHAINS {arr('chains', lambda v: f'{v}u')}
 #define KS_TUNED_BLOCK {arr('block', lambda v: f'{v}u')}
 """

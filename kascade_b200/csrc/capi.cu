@@ -473,27 +473,32 @@ KASCADE_API kascade_status kascade_ctx_set_size_classes(kascade_ctx* c, const ui
   c->class_spacing.assign(spacing, spacing + count);
   c->class_chains.assign(count, 2u);
   c->class_block.assign(count, 256u);
+  c->class_spacing_single.assign(spacing, spacing + count);
   return KASCADE_OK;
 }
 
 KASCADE_API kascade_status kascade_ctx_set_class_launch(kascade_ctx* c, const uint32_t* chains, const uint32_t* block,
-                                                        uint32_t count) {
+                                                        const uint32_t* single_spacing, uint32_t count) {
   if (!c || !chains || !block || count != c->class_max.size()) return KASCADE_ERR_INVALID_ARG;
   for (uint32_t i = 0; i < count; ++i) {
     if (chains[i] != 1 && chains[i] != 2 && chains[i] != 4) return KASCADE_ERR_INVALID_ARG;
     if (block[i] != 128 && block[i] != 256 && block[i] != 512) return KASCADE_ERR_INVALID_ARG;
+    if (single_spacing && single_spacing[i] < 2) return KASCADE_ERR_INVALID_ARG;
   }
   c->class_chains.assign(chains, chains + count);
   c->class_block.assign(block, block + count);
+  if (single_spacing) c->class_spacing_single.assign(single_spacing, single_spacing + count);
   return KASCADE_OK;
 }
 
-KASCADE_API int kascade_ctx_get_class_launch(kascade_ctx* c, uint32_t* chains, uint32_t* block, int cap) {
+KASCADE_API int kascade_ctx_get_class_launch(kascade_ctx* c, uint32_t* chains, uint32_t* block,
+                                             uint32_t* single_spacing, int cap) {
   if (!c) return 0;
   const int n = (int)c->class_max.size();
   for (int i = 0; i < n && i < cap; ++i) {
     if (chains) chains[i] = c->class_chains[i];
     if (block) block[i] = c->class_block[i];
+    if (single_spacing) single_spacing[i] = c->class_spacing_single[i];
   }
   return n;
 }

@@ -49,13 +49,16 @@ struct kascade_ctx {
   cudaStream_t last_stream = nullptr;
   bool async_pending = false;
   // size classes: instances of at most class_max[i] elements use a mean ruler
-  // spacing of class_spacing[i]; a call (or a batch, by the class holding
+  // spacing of class_spacing[i] inside a batch; a call (or a batch, by the class holding
   // most of its elements) chases with class_chains[i] chains per thread in
   // blocks of class_block[i] threads.  Defaults: the autotuner's table.
   std::vector<unsigned long long> class_max = KS_TUNED_MAX;
   std::vector<uint32_t> class_spacing = KS_TUNED_SPACING;
   std::vector<uint32_t> class_chains = KS_TUNED_CHAINS;
   std::vector<uint32_t> class_block = KS_TUNED_BLOCK;
+  // spacing for a call that ranks one instance on its own: fewer, larger
+  // levels pay off there, since each level costs launches and a host wait
+  std::vector<uint32_t> class_spacing_single = KS_TUNED_SPACING_SINGLE;
   int class_of(unsigned long long n) const {
     for (size_t i = 0; i < class_max.size(); ++i)
       if (n <= class_max[i]) return (int)i;

@@ -594,9 +594,9 @@ Params make_params(const kascade_ctx& ctx, const kascade_opts* o, uint64_t n) {
   // Spacing trades chase critical path (~ spacing * ln(n/spacing) hops)
   // against ruler-table size; these defaults are the tuned values for
   // random lists on B200 (see the autotune table in the batch path).
-  p.spacing0 = spacing_for(ctx, n);
   {
     const int k = ctx.class_of(n);
+    p.spacing0 = ctx.class_spacing_single[k];
     p.chains = ctx.class_chains[k];
     p.block = ctx.class_block[k];
   }

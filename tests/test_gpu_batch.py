@@ -71,10 +71,10 @@ def test_class_launch_parameters_keep_results(kb, oracle_mod):
     segs = kb.make_segments(sizes, kinds)
     ctx = kb.Context()
     kb.set_size_classes(ctx, [1 << 9, 1 << 12, 1 << 40], [4, 8, 24])
-    assert kb.get_class_launch(ctx) == ([2, 2, 2], [256, 256, 256])
+    assert kb.get_class_launch(ctx) == ([2, 2, 2], [256, 256, 256], [4, 8, 24])
     for chains, block in ((1, 128), (2, 512), (4, 256), (4, 512)):
         kb.set_class_launch(ctx, [chains] * 3, [block] * 3)
-        assert kb.get_class_launch(ctx) == ([chains] * 3, [block] * 3)
+        assert kb.get_class_launch(ctx)[:2] == ([chains] * 3, [block] * 3)
         root, rank = kb.rank_batch(inputs, segs, w, ctx=ctx)
         _check(kb, oracle_mod, inputs, w, sizes, kinds, root, rank)
     with pytest.raises(kb.KascadeError):
@@ -87,12 +87,13 @@ def test_class_launch_parameters_keep_results(kb, oracle_mod):
 def test_autotune_table_loads(kb):
     from kascade_b200 import autotune
 
-    table = {"gpu": "test", "classes": [{"max": 1 << 10, "spacing": 6, "chains": 1, "block": 128},
-                                        {"max": (1 << 64) - 1, "spacing": 40, "chains": 4, "block": 512}]}
+    table = {"gpu": "test", "classes": [{"max": 1 << 10, "spacing": 6, "chains": 1, "block": 128, "spacing_single": 16},
+                                        {"max": (1 << 64) - 1, "spacing": 40, "chains": 4, "block": 512,
+                                         "spacing_single": 48}]}
     ctx = kb.Context()
     kb.load_tuning(ctx, table)
     assert kb.get_size_classes(ctx) == ([1 << 10, (1 << 64) - 1], [6, 40])
-    assert kb.get_class_launch(ctx) == ([1, 4], [128, 512])
+    assert kb.get_class_launch(ctx) == ([1, 4], [128, 512], [16, 48])
     ctx.close()
     sizes, kinds = autotune.class_sizes(2, 1 << 16, 1)
     assert sizes.min() > autotune.CLASS_MAX[1] and sizes.max() <= autotune.CLASS_MAX[2]
