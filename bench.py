@@ -55,6 +55,19 @@ B_ALG = {"list": lambda w: 8 + (4 if w else 0) + 16 + 32, "forest": lambda w: 8 
 # dependent 16 B record read lands in one random 32 B sector, and the 16 B
 # stamp it writes back.
 B_CHASE = 32 + 16
+# Random-access roofline, stated as 32 B sectors touched x 32 B / peak: the
+# sectors the ranking pipeline touches per level-0 list element.  prepare:
+# succ 8 B (1/4 sector) + weight 4 B (1/8) + record write 16 B (1/2); chase:
+# the record's random sector read + its stamp written back (1 + 1);
+# propagate: record read (1/2) + the ruler result's random sector (1) + root
+# and rank writes (1/2).  Deeper levels add ~2% and are left out.
+SECTORS_LIST = {True: 0.25 + 0.125 + 0.5 + 2 + 2, False: 0.25 + 0.5 + 2 + 2}
+# DRAM bytes the level-0 chase moves per record it reads, from ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum of the level-0 k_chase launch
+# on a 2^25-element list: 3.924 GB + 1.036 GB over 2^25 + 2 797 812 record
+# reads, every element once plus each chain's closing ruler record; traffic
+# grows in proportion): profiles/chase_propagate_prepare_list25_ncu.md
+CHASE_DRAM_BYTES_PER_VISIT = (3.924e9 + 1.036e9) / (33_554_432 + 2_797_812)
 
 
 def log(*a):
@@ -522,17 +535,29 @@ def main():
             # levels, divided over the chase launches of one step
             total_units = sum(levels[:-1]) if len(levels) > 1 else units
             per_launch_bytes = B_CHASE * total_units / launches_per_step
+            traffic = CHASE_DRAM_BYTES_PER_VISIT * total_units / launches_per_step
             bytes_note = (f"{B_CHASE} B per element visited (one random 32 B sector for the 16 B record + 16 B "
                           f"stamp) x {total_units} elements over {launches_per_step:.0f} chase launches per step")
         else:
             per_launch_bytes = n * b_alg / (d_cnt / args.steps)
+            traffic = None
             bytes_note = f"{b_alg} B/element x n per step, over this kernel's launches"
         ach = per_launch_bytes / per_launch_s / 1e9
         roofline = {"bound": "hbm", "kernel": dominant, "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
                     "frac": round(ach / hbm, 4), "peak_source": f"{hbm_src} (MEASURED_PEAKS.json hbm_gbs)"
                     if hbm_src == "measured" else "fallback 6.65 TB/s",
-                    "traffic": None, "algorithmic_bytes": bytes_note}
+                    "traffic": round(traffic) if traffic else None,
+                    "traffic_note": ("ncu dram bytes per visited element on a 2^25 list, scaled by the visits per "
+                                     "launch" if traffic else None),
+                    "algorithmic_bytes": bytes_note}
     pipeline = {"b_alg_per_elem": b_alg, "achieved_gbs": round(pipe_gbs, 1), "frac": round(pipe_gbs / hbm, 4)}
+    random_access = None
+    if kind == "list":
+        sectors = SECTORS_LIST[bool(weighted)]
+        floor_ms = n * 32 * sectors / (hbm * 1e9) * 1000.0
+        random_access = {"sectors_per_element": sectors, "bytes_per_element": 32 * sectors,
+                         "floor_ms": round(floor_ms, 3), "frac": round(floor_ms / ms_per_step, 4),
+                         "peak_gbs": hbm}
 
     # end-to-end through the host-buffer API (pinned host memory)
     e2e = None
@@ -620,7 +645,8 @@ def main():
                        "parallelism": f"replicas x{world} (independent instances, no collective)",
                        "l2": "inputs larger than L2 (16 B records x n = %.1f GiB)" % (16 * n / 2**30),
                        "ruler_spacing": args.spacing or "auto", "levels": levels},
-            "roofline": roofline, "pipeline_roofline": pipeline, "cpu_baseline": cpu, "e2e": e2e,
+            "roofline": roofline, "pipeline_roofline": pipeline, "random_access_roofline": random_access,
+            "cpu_baseline": cpu, "e2e": e2e,
             "clocks": clk, "gpu_launches": launches,
             "kernels_ms_per_step": {k: round(v, 4) for k, v in sorted(step_kernel_ms.items())},
             "secondary": secondary or None, "batched": batched, "served": served,
