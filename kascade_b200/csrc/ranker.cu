@@ -19,6 +19,7 @@
 #include <cstdio>
 
 #include "ranker.cuh"
+#include "tma.cuh"
 
 namespace ks {
 
@@ -62,13 +63,14 @@ inline uint32_t salt_for(uint32_t seed, int level) { return mix32(seed + 0x9E377
 // ---------------------------------------------------------------------------
 template <class W>
 __global__ void __launch_bounds__(256, 4) k_prepare_arrays(const uint64_t* __restrict__ succ, W w, uint32_t n,
-                                                        Rec* __restrict__ rec, uint32_t* __restrict__ ruler_elem,
+                                                        uint64_t start, Rec* __restrict__ rec,
+                                                        uint32_t* __restrict__ ruler_elem,
                                                         uint32_t* __restrict__ counter, uint32_t salt,
                                                         uint32_t thresh, DevStatus* st) {
   __shared__ uint32_t sm[33];
   __shared__ uint32_t sbase;
   const uint64_t tile_sz = (uint64_t)blockDim.x * PREP_ITEMS;
-  for (uint64_t tile = (uint64_t)blockIdx.x * tile_sz; tile < n; tile += (uint64_t)gridDim.x * tile_sz) {
+  for (uint64_t tile = start + (uint64_t)blockIdx.x * tile_sz; tile < n; tile += (uint64_t)gridDim.x * tile_sz) {
     uint32_t sv[PREP_ITEMS];
     typename W::T wv[PREP_ITEMS];
     uint32_t rl = 0, cnt = 0;
@@ -117,6 +119,116 @@ __global__ void __launch_bounds__(256, 4) k_prepare_arrays(const uint64_t* __res
         }
         rec[x] = r;
       }
+    }
+    __syncthreads();
+  }
+}
+
+// The same work for 16 B-aligned inputs, with the input tiles moved by bulk
+// (TMA) copies: a persistent block keeps PT_STAGES tiles of succ (and
+// weights) in flight into shared memory while it numbers the rulers of an
+// earlier tile and writes its records, so the loads no longer wait behind the
+// block scan and the ruler-id atomic.  Full tiles only; the caller hands the
+// tail to k_prepare_arrays.
+constexpr int PT_TILE = 2048;
+constexpr int PT_STAGES = 4;
+constexpr int PT_ITEMS = PT_TILE / 256;
+
+template <bool W32>
+__global__ void __launch_bounds__(256) k_prepare_tma(const uint64_t* __restrict__ succ, const uint32_t* __restrict__ w,
+                                                     uint32_t n, uint32_t ntiles, Rec* __restrict__ rec,
+                                                     uint32_t* __restrict__ ruler_elem,
+                                                     uint32_t* __restrict__ counter, uint32_t salt, uint32_t thresh,
+                                                     DevStatus* st) {
+  constexpr uint32_t SB = PT_TILE * 8, WB = W32 ? PT_TILE * 4 : 0, STAGE = SB + WB;
+  extern __shared__ __align__(128) unsigned char dyn[];
+  __shared__ __align__(8) uint64_t bar[PT_STAGES];
+  __shared__ uint32_t sm[33];
+  __shared__ uint32_t sbase;
+  const uint32_t tid = threadIdx.x;
+  if (tid == 0) {
+    for (int i = 0; i < PT_STAGES; ++i) mbar_init(&bar[i], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  // the k-th tile of this block goes to stage k % PT_STAGES
+  auto issue = [&](uint32_t k) {
+    const uint32_t t = blockIdx.x + k * gridDim.x;
+    if (t >= ntiles) return;
+    unsigned char* dst = dyn + (k % PT_STAGES) * STAGE;
+    uint64_t* b = &bar[k % PT_STAGES];
+    mbar_expect_tx(b, STAGE);
+    bulk_g2s(dst, succ + (uint64_t)t * PT_TILE, SB, b);
+    if (W32) bulk_g2s(dst + SB, w + (uint64_t)t * PT_TILE, WB, b);
+  };
+  if (tid == 0)
+    for (uint32_t k = 0; k < PT_STAGES; ++k) issue(k);
+  for (uint32_t k = 0;; ++k) {
+    const uint32_t t = blockIdx.x + k * gridDim.x;
+    if (t >= ntiles) break;
+    const uint32_t sg = k % PT_STAGES;
+    const bool ok = mbar_wait_bounded(&bar[sg], (k / PT_STAGES) & 1u);
+    if (__syncthreads_or(!ok)) {
+      // a copy never completed: report it and let the copies in flight land
+      // before the block's shared memory goes away
+      if (tid == 0) {
+        set_error(st, KASCADE_ERR_TIMEOUT, t);
+        for (uint32_t j = k; j < k + PT_STAGES; ++j)
+          if (blockIdx.x + j * gridDim.x < ntiles) mbar_wait_bounded(&bar[j % PT_STAGES], (j / PT_STAGES) & 1u);
+      }
+      __syncthreads();
+      return;
+    }
+    const uint64_t* ss = reinterpret_cast<const uint64_t*>(dyn + sg * STAGE);
+    const uint32_t* ws = reinterpret_cast<const uint32_t*>(dyn + sg * STAGE + SB);
+    const uint64_t base = (uint64_t)t * PT_TILE;
+    uint32_t sv[PT_ITEMS], wv[PT_ITEMS];
+    uint32_t rl = 0, cnt = 0;
+#pragma unroll
+    for (int i = 0; i < PT_ITEMS; ++i) {
+      const uint32_t j = i * 256 + tid;
+      const uint32_t x = (uint32_t)(base + j);
+      unsigned long long sx = ss[j];
+      if (sx >= n) {
+        set_error(st, KASCADE_ERR_OUT_OF_RANGE, x);
+        sx = x;
+      }
+      sv[i] = (uint32_t)sx;
+      wv[i] = W32 ? ws[j] : 1u;
+      if (sx == x || sampled(x, salt, thresh)) {
+        rl |= 1u << i;
+        cnt++;
+      }
+    }
+    __syncthreads();  // the stage is read: refill it with this block's tile k + PT_STAGES
+    if (tid == 0) {
+      fence_proxy_async();
+      issue(k + PT_STAGES);
+    }
+    uint32_t total;
+    const uint32_t pre = block_exclusive_scan(cnt, sm, &total);
+    if (tid == 0) {
+      const uint32_t b = total ? atomicAdd(counter, total) : 0u;
+      if ((uint64_t)b + total > MAX_RULERS) set_error(st, KASCADE_ERR_TOO_LARGE, b);
+      sbase = b;
+    }
+    __syncthreads();
+    uint32_t id = sbase + pre;
+#pragma unroll
+    for (int i = 0; i < PT_ITEMS; ++i) {
+      const uint32_t x = (uint32_t)(base + i * 256 + tid);
+      Rec r;
+      r.a = wv[i];
+      r.b = sv[i];
+      r.c = TAG_UNREACHED;
+      if (rl & (1u << i)) {
+        if (id < MAX_RULERS) {
+          r.c = TAG_RULER | id;
+          ruler_elem[id] = x;
+        }
+        id++;
+      }
+      st_rec_cs(rec + x, r);
     }
     __syncthreads();
   }
@@ -307,10 +419,11 @@ __global__ void __launch_bounds__(512) k_chase(Rec* __restrict__ rec, uint32_t n
 // ---------------------------------------------------------------------------
 template <class Sink>
 __global__ void __launch_bounds__(256) k_propagate(const Rec* __restrict__ rec, uint32_t n_out, uint32_t n_all,
-                                                   const Out* __restrict__ out_next, Sink sink, DevStatus* st) {
+                                                   uint64_t start, const Out* __restrict__ out_next, Sink sink,
+                                                   DevStatus* st) {
   const uint32_t stride = gridDim.x * blockDim.x;
   const uint64_t pol = l2_keep_policy();
-  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x * PROP_ITEMS + threadIdx.x; base < n_out;
+  for (uint64_t base = start + (uint64_t)blockIdx.x * blockDim.x * PROP_ITEMS + threadIdx.x; base < n_out;
        base += (uint64_t)stride * PROP_ITEMS) {
     Rec rv[PROP_ITEMS];
 #pragma unroll
@@ -557,9 +670,9 @@ kascade_status launch_chase(kascade_ctx& ctx, Rec* rec, uint32_t n, const uint32
 template <class Sink>
 kascade_status launch_propagate(kascade_ctx& ctx, const Rec* rec, uint32_t n_out, uint32_t n_all, const Out* out_next,
                                 const Sink& sink, cudaStream_t s) {
-  unsigned grid = grid_for(ctx, ((uint64_t)n_out + PROP_ITEMS - 1) / PROP_ITEMS, 256, 8);
   ProfScope ps(ctx, "propagate", s);
-  k_propagate<Sink><<<grid, 256, 0, s>>>(rec, n_out, n_all, out_next, sink, ctx.d_status);
+  const unsigned grid = grid_for(ctx, ((uint64_t)n_out + PROP_ITEMS - 1) / PROP_ITEMS, 256, 8);
+  k_propagate<Sink><<<grid, 256, 0, s>>>(rec, n_out, n_all, 0, out_next, sink, ctx.d_status);
   KS_CHECK_LAUNCH();
   return KASCADE_OK;
 }
@@ -627,24 +740,57 @@ kascade_status prepare_arrays(kascade_ctx& ctx, const uint64_t* succ, WKind wk, 
   uint32_t* ctr = alloc<uint32_t>(ctx, 1);
   if (!ctr) return KASCADE_ERR_OOM;
   KS_CUDA(cudaMemsetAsync(ctr, 0, sizeof(uint32_t), s));
-  unsigned grid = grid_for(ctx, ((uint64_t)n + 256 * PREP_ITEMS - 1) / (256 * PREP_ITEMS) * 256, 256, 8);
   uint32_t salt = salt_for(p.seed, 0), th = thresh_for(p.spacing0);
   {
     ProfScope ps(ctx, "prepare", s);
-    switch (wk) {
-      case WKind::Unit:
-        k_prepare_arrays<WUnit><<<grid, 256, 0, s>>>(succ, WUnit{}, n, rec, ruler_elem, ctr, salt, th, ctx.d_status);
-        break;
-      case WKind::U32:
-        k_prepare_arrays<WU32><<<grid, 256, 0, s>>>(succ, WU32{(const uint32_t*)w}, n, rec, ruler_elem, ctr, salt, th,
-                                                    ctx.d_status);
-        break;
-      case WKind::I64:
-        k_prepare_arrays<WI64><<<grid, 256, 0, s>>>(succ, WI64{(const int64_t*)w}, n, rec, ruler_elem, ctr, salt, th,
-                                                    ctx.d_status);
-        break;
+    // full tiles of 16 B-aligned inputs go through the bulk-copy kernel
+    uint64_t start = 0;
+    const bool aligned = (reinterpret_cast<uintptr_t>(succ) % 16 == 0) &&
+                         (wk == WKind::Unit || (wk == WKind::U32 && reinterpret_cast<uintptr_t>(w) % 16 == 0));
+    const uint32_t ntiles = n / PT_TILE;
+    if (aligned && ntiles >= (uint32_t)ctx.usable_sms()) {
+      const unsigned g = (unsigned)std::min<uint64_t>(ntiles, (uint64_t)ctx.usable_sms() * 2);
+      if (wk == WKind::U32) {
+        constexpr int smem = PT_STAGES * PT_TILE * 12;
+        static bool raised = false;
+        if (!raised) {
+          KS_CUDA(cudaFuncSetAttribute(k_prepare_tma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+          raised = true;
+        }
+        k_prepare_tma<true><<<g, 256, smem, s>>>(succ, (const uint32_t*)w, n, ntiles, rec, ruler_elem, ctr, salt, th,
+                                                 ctx.d_status);
+      } else {
+        constexpr int smem = PT_STAGES * PT_TILE * 8;
+        static bool raised = false;
+        if (!raised) {
+          KS_CUDA(cudaFuncSetAttribute(k_prepare_tma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+          raised = true;
+        }
+        k_prepare_tma<false><<<g, 256, smem, s>>>(succ, nullptr, n, ntiles, rec, ruler_elem, ctr, salt, th,
+                                                  ctx.d_status);
+      }
+      KS_CHECK_LAUNCH();
+      start = (uint64_t)ntiles * PT_TILE;
     }
-    KS_CHECK_LAUNCH();
+    if (start < n) {
+      const uint64_t rest = n - start;
+      const unsigned grid = grid_for(ctx, (rest + 256 * PREP_ITEMS - 1) / (256 * PREP_ITEMS) * 256, 256, 8);
+      switch (wk) {
+        case WKind::Unit:
+          k_prepare_arrays<WUnit><<<grid, 256, 0, s>>>(succ, WUnit{}, n, start, rec, ruler_elem, ctr, salt, th,
+                                                       ctx.d_status);
+          break;
+        case WKind::U32:
+          k_prepare_arrays<WU32><<<grid, 256, 0, s>>>(succ, WU32{(const uint32_t*)w}, n, start, rec, ruler_elem, ctr,
+                                                      salt, th, ctx.d_status);
+          break;
+        case WKind::I64:
+          k_prepare_arrays<WI64><<<grid, 256, 0, s>>>(succ, WI64{(const int64_t*)w}, n, start, rec, ruler_elem, ctr,
+                                                      salt, th, ctx.d_status);
+          break;
+      }
+      KS_CHECK_LAUNCH();
+    }
   }
   return read_u32(ctx, ctr, r_out, s);
 }

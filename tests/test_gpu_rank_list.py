@@ -91,6 +91,31 @@ def test_write_free_above_2_22(kb, oracle_mod, layout):
     ctx.close()
 
 
+@pytest.mark.parametrize("offset", [(0, 0), (1, 0), (0, 1), (1, 3)])
+def test_input_alignment(kb, oracle_mod, offset):
+    """Inputs that start 16 B aligned take the bulk-copy prepare for their full
+    tiles and the plain one for the tail; shifted inputs take the plain one."""
+    import torch
+
+    n = 148 * 2048 * 2 + 777
+    succ_h = oracle_mod.gen_list(n, 0xA1, 0)
+    w_h = oracle_mod.gen_weights(n, 0xA2, 16)
+    root_o, rank_o = oracle_mod.rank_list(succ_h, w_h)
+    so, wo = offset
+    sbuf = torch.empty(n + so, dtype=torch.int64, device="cuda")
+    sbuf[so:] = dev64(succ_h)
+    wbuf = torch.empty(n + wo, dtype=torch.int32, device="cuda")
+    wbuf[wo:] = dev32(w_h)
+    for w in (wbuf[wo:], None):
+        root, rank = kb.rank_list(sbuf[so:], w)
+        if w is None:
+            ro, ko = oracle_mod.rank_list(succ_h)
+        else:
+            ro, ko = root_o, rank_o
+        np.testing.assert_array_equal(host_u64(root), ro)
+        np.testing.assert_array_equal(host_u64(rank), ko)
+
+
 @pytest.mark.parametrize("parts", [2, 37, 1000, 20000])
 def test_many_lists(kb, oracle_mod, parts):
     rng = np.random.default_rng(parts)
