@@ -6,7 +6,7 @@
 #define KS_TUNED_GPU "NVIDIA B200"
 #define KS_TUNED_COUNT 7
 #define KS_TUNED_MAX {1024ull, 8192ull, 65536ull, 524288ull, 4194304ull, 33554432ull, ~0ull}
-#define KS_TUNED_SPACING {4u, 6u, 6u, 6u, 8u, 24u, 64u}
-#define KS_TUNED_SPACING_SINGLE {32u, 6u, 12u, 6u, 24u, 12u, 48u}
+#define KS_TUNED_SPACING {4u, 8u, 6u, 6u, 8u, 24u, 64u}
+#define KS_TUNED_SPACING_SINGLE {128u, 6u, 12u, 8u, 24u, 12u, 48u}
 #define KS_TUNED_CHAINS {1u, 1u, 1u, 1u, 1u, 1u, 1u}
-#define KS_TUNED_BLOCK {512u, 128u, 512u, 512u, 256u, 128u, 256u}
+#define KS_TUNED_BLOCK {128u, 512u, 512u, 128u, 128u, 512u, 128u}
