@@ -172,6 +172,51 @@ KASCADE_API kascade_status kascade_is_list(kascade_ctx* ctx, const uint64_t* suc
                                            int* is_list_out, void* stream);
 
 /* ----------------------------------------------------------------------------
+ * Result statistics on the device: the bench's compute_stats
+ * (bench/detail/stats.hpp:9-50, bench/detail/stats.cpp:24-162) over root and
+ * rank arrays (a ranking's or a rooting's output).  Level values are the
+ * reference's StatsLevel.  Basic: trees = elements with root[i] == i, max and
+ * mean rank.  Extensive (both levels): per tree (keyed by root) size, rank sum
+ * and max rank, reduced to the counts and means below; EXTENSIVE also lists
+ * the non-trivial trees (size > 1) into per_tree (device memory, up to
+ * per_tree_cap entries, ordered by root; *per_tree_count = how many exist).
+ * ---------------------------------------------------------------------------*/
+typedef enum {
+  KASCADE_STATS_NONE = 1,
+  KASCADE_STATS_BASIC = 2,
+  KASCADE_STATS_REDUCED_EXTENSIVE = 3,
+  KASCADE_STATS_EXTENSIVE = 4
+} kascade_stats_level;
+
+typedef struct kascade_stats {
+  /* BasicStats */
+  uint64_t num_trees;
+  int64_t max_rank;
+  double avg_rank;
+  /* ExtensiveStats (levels 3 and 4) */
+  uint64_t ext_num_trees; /* distinct roots among root[]                 */
+  uint64_t num_nontrivial_trees;
+  uint64_t nontrivial_size_sum;
+  int64_t nontrivial_rank_sum;
+  uint64_t max_size;
+  double avg_size;
+  double nontrivial_avg_size;
+  double nontrivial_avg_rank;
+} kascade_stats;
+
+typedef struct kascade_tree_stats {
+  uint64_t root;
+  uint64_t size;
+  int64_t max_rank;
+  int64_t rank_sum;
+} kascade_tree_stats;
+
+KASCADE_API kascade_status kascade_compute_stats(kascade_ctx* ctx, const uint64_t* root, const int64_t* rank,
+                                                 uint64_t n, int level, kascade_stats* out,
+                                                 kascade_tree_stats* per_tree, uint64_t per_tree_cap,
+                                                 uint64_t* per_tree_count, void* stream);
+
+/* ----------------------------------------------------------------------------
  * Tree rooting (device pointers).
  *   parent[v] (parent[v] == v marks a root) -> root_out[v], depth_out[v]
  *   (edge count to the root; 0 at roots), via an Euler tour of the forest

@@ -33,7 +33,12 @@ from .api import (  # noqa: F401
     make_segments,
     rank_batch,
     set_size_classes,
+    STATS_BASIC,
+    STATS_EXTENSIVE,
+    STATS_NONE,
+    STATS_REDUCED_EXTENSIVE,
     compute_euler_tour,
+    compute_stats,
     default_context,
     gen_forest,
     gen_list,

@@ -56,6 +56,15 @@ class ServerStats(ctypes.Structure):
                 ("partition_batches", c_u64)]
 
 
+class Stats(ctypes.Structure):
+    """Mirror of ``kascade_stats``."""
+
+    _fields_ = [("num_trees", c_u64), ("max_rank", ctypes.c_int64), ("avg_rank", ctypes.c_double),
+                ("ext_num_trees", c_u64), ("num_nontrivial_trees", c_u64), ("nontrivial_size_sum", c_u64),
+                ("nontrivial_rank_sum", ctypes.c_int64), ("max_size", c_u64), ("avg_size", ctypes.c_double),
+                ("nontrivial_avg_size", ctypes.c_double), ("nontrivial_avg_rank", ctypes.c_double)]
+
+
 class Opts(ctypes.Structure):
     """Mirror of ``kascade_opts``."""
 
@@ -143,6 +152,8 @@ _SIGS = {
     "kascade_ctx_set_size_classes": (_status, [_ctx_p, P(c_u64), P(c_u32), c_u32]),
     "kascade_ctx_get_size_classes": (c_int, [_ctx_p, P(c_u64), P(c_u32), c_int]),
     "kascade_ctx_set_class_launch": (_status, [_ctx_p, P(c_u32), P(c_u32), P(c_u32), c_u32]),
+    "kascade_compute_stats": (_status, [_ctx_p, c_void_p, c_void_p, c_u64, c_int, P(Stats), c_void_p, c_u64,
+                                        P(c_u64), c_void_p]),
     "kascade_ctx_get_class_launch": (c_int, [_ctx_p, P(c_u32), P(c_u32), P(c_u32), c_int]),
     "kascade_ctx_set_sm_budget": (_status, [_ctx_p, c_int]),
     "kascade_server_config_init": (None, [P(ServerConfig)]),

@@ -16,7 +16,7 @@ from typing import Optional
 import numpy as np
 import torch
 
-from ._lib import KascadeError, Opts, Segment, ServerConfig, ServerStats, check, lib
+from ._lib import Stats, KascadeError, Opts, Segment, ServerConfig, ServerStats, check, lib
 
 
 class Algorithm(IntEnum):
@@ -373,6 +373,32 @@ def is_list(succ_array: torch.Tensor, ctx: Optional[Context] = None) -> bool:
     check(lib.kascade_is_list(c.handle, succ_array.data_ptr(), succ_array.numel(), ctypes.byref(out),
                               _stream(succ_array)), "kascade_is_list", c.handle)
     return bool(out.value)
+
+
+STATS_NONE, STATS_BASIC, STATS_REDUCED_EXTENSIVE, STATS_EXTENSIVE = 1, 2, 3, 4
+
+
+def compute_stats(root_array: torch.Tensor, rank_array: torch.Tensor, level: int = STATS_EXTENSIVE,
+                  ctx: Optional[Context] = None):
+    """The bench's compute_stats (bench/detail/stats.hpp:46-50) on the device:
+    (figures dict, non-trivial trees as an (k, 4) int64 array of root, size,
+    max rank, rank sum ordered by root; empty below STATS_EXTENSIVE)."""
+    _dev64(root_array, "root_array")
+    _dev64(rank_array, "rank_array")
+    n = root_array.numel()
+    c = _ctx_for(root_array, ctx)
+    st = Stats()
+    cnt = ctypes.c_uint64(0)
+    per_tree = None
+    if level >= STATS_EXTENSIVE and n:
+        per_tree = torch.empty((n // 2 + 1, 4), dtype=torch.int64, device=root_array.device)
+    check(lib.kascade_compute_stats(c.handle, root_array.data_ptr(), rank_array.data_ptr(), n, level,
+                                    ctypes.byref(st), per_tree.data_ptr() if per_tree is not None else None,
+                                    per_tree.shape[0] if per_tree is not None else 0, ctypes.byref(cnt),
+                                    _stream(root_array)), "kascade_compute_stats", c.handle)
+    figs = {f: getattr(st, f) for f, _ in Stats._fields_}
+    trees = per_tree[:cnt.value].cpu().numpy() if per_tree is not None else np.zeros((0, 4), np.int64)
+    return figs, trees
 
 
 def rank_via_euler_tour(config: EulerTourConfig, succ_array: torch.Tensor, rank_array: torch.Tensor,

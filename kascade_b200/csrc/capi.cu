@@ -354,6 +354,21 @@ KASCADE_API kascade_status kascade_is_list(kascade_ctx* c, const uint64_t* succ,
   return end_call(c, s, st, nullptr);
 }
 
+KASCADE_API kascade_status kascade_compute_stats(kascade_ctx* c, const uint64_t* root, const int64_t* rank, uint64_t n,
+                                                 int level, kascade_stats* out, kascade_tree_stats* per_tree,
+                                                 uint64_t per_tree_cap, uint64_t* per_tree_count, void* stream) {
+  cudaStream_t s = as_stream(stream);
+  if (!out || (n && (!root || !rank)) || level < KASCADE_STATS_NONE || level > KASCADE_STATS_EXTENSIVE)
+    return KASCADE_ERR_INVALID_ARG;
+  std::memset(out, 0, sizeof(*out));
+  if (per_tree_count) *per_tree_count = 0;
+  if (level == KASCADE_STATS_NONE || n == 0) return KASCADE_OK;
+  KS_TRY(begin_call(c, s, nullptr));
+  kascade_status st =
+      compute_stats(*c, root, rank, n, level, out, per_tree, per_tree_cap, per_tree_count, s);
+  return end_call(c, s, st, nullptr);
+}
+
 KASCADE_API kascade_status kascade_root_forest(kascade_ctx* c, const uint64_t* parent, uint64_t n, uint64_t* root_out,
                                                uint64_t* depth_out, const kascade_opts* opts, void* stream) {
   cudaStream_t s = as_stream(stream);

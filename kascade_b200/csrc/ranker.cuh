@@ -165,6 +165,10 @@ kascade_status rank_sublist(kascade_ctx& ctx, Rec* rec, uint32_t n, const uint32
 // Write-free level 0: read-only chase that logs (element, ruler, distance),
 // recursion on the ruler sub-list, then resolve + partition by element window
 // and a windowed scatter into the outputs.
+kascade_status compute_stats(kascade_ctx& ctx, const uint64_t* root, const int64_t* rank, uint64_t n, int level,
+                             kascade_stats* out, kascade_tree_stats* per_tree, uint64_t per_tree_cap,
+                             uint64_t* per_tree_count, cudaStream_t s);
+
 kascade_status rank_level0_log(kascade_ctx& ctx, const Rec* rec, uint32_t n, uint32_t r0,
                                const uint32_t* ruler_elem0, const LogTarget& t, const Params& p,
                                cudaStream_t s);

@@ -12,6 +12,7 @@ ORACLE_SO = HERE / "_build" / "libkascade_oracle.so"
 REF_SO = HERE / "_ref" / "libkascade_ref.so"
 
 __all__ = [
+    "compute_stats",
     "build", "has_ref", "rank_list", "root_forest", "local_pointer_chasing", "pointer_doubling",
     "euler_tour", "rank_via_euler_tour", "is_list", "pack", "unpack", "gen_list", "gen_weights",
     "gen_forest", "ref_gather_rank", "ref_local_pointer_chasing",
@@ -168,3 +169,44 @@ def ref_local_pointer_chasing(succ: np.ndarray, rank: np.ndarray) -> None:
     """In place, the reference's lib/kascade/local_pointer_chasing.cpp."""
     assert succ.dtype == np.uint64 and rank.dtype == np.int64
     _r().ref_local_pointer_chasing(_p(succ), _p(rank), U64(succ.size))
+
+
+def compute_stats(root: np.ndarray, rank: np.ndarray, level: int) -> tuple[dict, list]:
+    """The bench's compute_stats (bench/detail/stats.cpp:110-162 basic, 24-108
+    per tree) on one rank: level 2 basic, 3 reduced extensive, 4 extensive
+    (also the non-trivial trees, here ordered by root).  numpy restatement."""
+    root = np.asarray(root, dtype=np.uint64)
+    rank = np.asarray(rank).view(np.int64) if np.asarray(rank).dtype == np.uint64 else np.asarray(rank, np.int64)
+    n = root.size
+    out = {"num_trees": 0, "max_rank": 0, "avg_rank": 0.0}
+    if level < 2 or n == 0:
+        return out, []
+    idx = np.arange(n, dtype=np.uint64)
+    out["num_trees"] = int(np.count_nonzero(root == idx))  # stats.cpp:117-119 (is_root)
+    out["max_rank"] = int(rank.max())                        # stats.cpp:120-122
+    total = int(np.sum(rank, dtype=np.int64))                # stats.cpp:123-125, int64 wrap
+    out["avg_rank"] = float(total) / float(n)                # stats.cpp:133-134
+    if level < 3:
+        return out, []
+    keys, inv = np.unique(root, return_inverse=True)         # one entry per tree (stats.cpp:32-39)
+    size = np.bincount(inv, minlength=keys.size).astype(np.int64)
+    rsum = np.zeros(keys.size, np.int64)
+    np.add.at(rsum, inv, rank)
+    rmax = np.full(keys.size, np.iinfo(np.int64).min, np.int64)
+    np.maximum.at(rmax, inv, rank)
+    nt = size > 1                                            # stats.cpp:58-64
+    out["ext_num_trees"] = int(keys.size)
+    out["num_nontrivial_trees"] = int(nt.sum())
+    out["nontrivial_size_sum"] = int(size[nt].sum())
+    out["nontrivial_rank_sum"] = int(np.sum(rsum[nt], dtype=np.int64))
+    out["max_size"] = int(size.max())
+    trivial = out["ext_num_trees"] - out["num_nontrivial_trees"]
+    div = lambda a, b: 0.0 if b == 0 else float(a) / float(b)  # noqa: E731  (stats.cpp:19-22)
+    out["avg_size"] = div(out["nontrivial_size_sum"] + trivial, out["ext_num_trees"])
+    out["nontrivial_avg_size"] = div(out["nontrivial_size_sum"], out["num_nontrivial_trees"])
+    out["nontrivial_avg_rank"] = div(out["nontrivial_rank_sum"], out["nontrivial_size_sum"])
+    trees = []
+    if level >= 4:
+        trees = [(int(k), int(a), int(b), int(c)) for k, a, b, c in zip(keys[nt], size[nt], rmax[nt], rsum[nt])]
+    return out, trees
+

@@ -113,3 +113,19 @@ def test_oracle_detects_cycle(oracle_mod):
     succ = np.array([1, 2, 0, 3], np.uint64)  # 0->1->2->0, 3 root
     with pytest.raises(ValueError):
         oracle_mod.rank_list(succ)
+
+
+def test_stats_restatement_small(oracle_mod):
+    """compute_stats restated with numpy against a direct loop on a tiny case."""
+    root = np.array([0, 0, 2, 0, 4, 4, 6], np.uint64)
+    rank = np.array([0, 3, 0, 1, 0, 2, 0], np.int64)
+    figs, trees = oracle_mod.compute_stats(root, rank, 4)
+    assert figs["num_trees"] == 4 and figs["max_rank"] == 3
+    assert figs["avg_rank"] == pytest.approx(6 / 7)
+    assert figs["ext_num_trees"] == 4 and figs["num_nontrivial_trees"] == 2
+    assert figs["nontrivial_size_sum"] == 5 and figs["nontrivial_rank_sum"] == 6
+    assert figs["max_size"] == 3
+    assert figs["avg_size"] == pytest.approx((5 + 2) / 4)
+    assert figs["nontrivial_avg_size"] == pytest.approx(5 / 2)
+    assert figs["nontrivial_avg_rank"] == pytest.approx(6 / 5)
+    assert trees == [(0, 3, 3, 4), (4, 2, 2, 2)]
