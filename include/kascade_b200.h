@@ -334,6 +334,25 @@ KASCADE_API kascade_status kascade_ctx_set_sm_budget(kascade_ctx* ctx, int sms);
  * lanes free up and both lanes' work overlaps on the device.
  * ------------------------------------------------------------------------- */
 typedef struct kascade_server kascade_server;
+/* Batch plans: one batch captured once as a CUDA graph (the whole
+ * device-driven pipeline: record build, forest tours, every ruling-set level,
+ * propagation) and replayed by one graph launch per call.  The segment table
+ * and the input / weight / output pointers are fixed at creation; their
+ * contents may change between launches.  Creation runs the batch once and
+ * returns KASCADE_ERR_UNSUPPORTED if it needs the host-driven recursion (a
+ * level outgrowing its capacity, e.g. very many roots); a launch that meets
+ * that case (new contents with far more roots) returns KASCADE_ERR_TIMEOUT,
+ * and kascade_rank_batch handles such a batch.  A plan owns its scratch;
+ * launches of one plan are ordered on the device.  No counterpart in the
+ * reference (its rounds are MPI exchanges per call). */
+typedef struct kascade_batch_plan kascade_batch_plan;
+KASCADE_API kascade_status kascade_batch_plan_create(int device, const kascade_segment* segs, uint32_t num_segs,
+                                                     const uint64_t* input, const uint32_t* weights, uint64_t total_n,
+                                                     uint64_t* root_out, uint64_t* rank_out,
+                                                     const kascade_opts* opts, kascade_batch_plan** plan);
+KASCADE_API kascade_status kascade_batch_plan_launch(kascade_batch_plan* plan, void* stream);
+KASCADE_API kascade_status kascade_batch_plan_destroy(kascade_batch_plan* plan);
+
 typedef struct kascade_server_config {
   uint32_t struct_size;
   int device;

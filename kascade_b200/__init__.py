@@ -16,6 +16,7 @@ from .api import (  # noqa: F401
     SEG_LIST,
     Algorithm,
     B200Ranking,
+    BatchPlan,
     Context,
     EulerTourConfig,
     GpuTuning,

@@ -152,6 +152,10 @@ _SIGS = {
     "kascade_ctx_set_size_classes": (_status, [_ctx_p, P(c_u64), P(c_u32), c_u32]),
     "kascade_ctx_get_size_classes": (c_int, [_ctx_p, P(c_u64), P(c_u32), c_int]),
     "kascade_ctx_set_class_launch": (_status, [_ctx_p, P(c_u32), P(c_u32), P(c_u32), c_u32]),
+    "kascade_batch_plan_create": (_status, [c_int, c_void_p, c_u32, c_void_p, c_void_p, c_u64, c_void_p, c_void_p,
+                                            c_void_p, P(c_void_p)]),
+    "kascade_batch_plan_launch": (_status, [c_void_p, c_void_p]),
+    "kascade_batch_plan_destroy": (_status, [c_void_p]),
     "kascade_compute_stats": (_status, [_ctx_p, c_void_p, c_void_p, c_u64, c_int, P(Stats), c_void_p, c_u64,
                                         P(c_u64), c_void_p]),
     "kascade_ctx_get_class_launch": (c_int, [_ctx_p, P(c_u32), P(c_u32), P(c_u32), c_int]),

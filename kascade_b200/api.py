@@ -493,6 +493,47 @@ def rank_batch(inputs: torch.Tensor, segments, weights: Optional[torch.Tensor] =
     return root_out, rank_out
 
 
+class BatchPlan:
+    """A batch captured once as a CUDA graph and replayed
+    (kascade_batch_plan_*).  The segment table and the tensors are fixed at
+    creation; their contents may change between launches."""
+
+    def __init__(self, inputs: torch.Tensor, segments, weights: Optional[torch.Tensor] = None, *,
+                 root_out: Optional[torch.Tensor] = None, rank_out: Optional[torch.Tensor] = None,
+                 tuning: Optional[GpuTuning] = None):
+        _dev64(inputs, "inputs")
+        if weights is not None:
+            _dev32(weights, "weights")
+        n = inputs.numel()
+        self.inputs, self.weights, self.segments = inputs, weights, segments
+        self.root = root_out if root_out is not None else torch.empty(n, dtype=torch.int64, device=inputs.device)
+        self.rank = rank_out if rank_out is not None else torch.empty(n, dtype=torch.int64, device=inputs.device)
+        o = (tuning or GpuTuning()).to_opts()
+        h = ctypes.c_void_p()
+        torch.cuda.synchronize(inputs.device)
+        check(lib.kascade_batch_plan_create(inputs.device.index or 0, segments, len(segments), inputs.data_ptr(),
+                                            weights.data_ptr() if weights is not None else None, n,
+                                            self.root.data_ptr(), self.rank.data_ptr(), ctypes.byref(o),
+                                            ctypes.byref(h)), "kascade_batch_plan_create")
+        self.handle = h
+
+    def launch(self):
+        """Replay on the current stream; returns (root, rank)."""
+        check(lib.kascade_batch_plan_launch(self.handle, _stream(self.inputs)), "kascade_batch_plan_launch")
+        return self.root, self.rank
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            lib.kascade_batch_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def set_size_classes(ctx: Context, max_sizes, spacings) -> None:
     """Install a size-class table (max instance size -> mean ruler spacing)."""
     k = len(max_sizes)

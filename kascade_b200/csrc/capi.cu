@@ -25,7 +25,7 @@ kascade_status unpack_impl(kascade_ctx& ctx, const uint64_t* succ_packed, const 
                            cudaStream_t s);
 kascade_status rank_batch_impl(kascade_ctx& ctx, const kascade_segment* segs, uint32_t nseg, const uint64_t* in,
                                const uint32_t* weights, uint64_t total, uint64_t* root_out, uint64_t* rank_out,
-                               const kascade_opts* opts, cudaStream_t s);
+                               const kascade_opts* opts, cudaStream_t s, bool device_levels);
 }  // namespace ks
 
 using namespace ks;
@@ -472,9 +472,46 @@ KASCADE_API kascade_status kascade_rank_batch(kascade_ctx* c, const kascade_segm
                                               void* stream) {
   cudaStream_t s = as_stream(stream);
   if (total_n && (!segs || !num_segs || !input || !root_out || !rank_out)) return KASCADE_ERR_INVALID_ARG;
+  // The device-driven recursion (no host waits) first; a batch it cannot hold
+  // (a level outgrowing its capacity, e.g. very many roots) reports
+  // KASCADE_ERR_TIMEOUT and is ranked again on the host-driven path.  Async
+  // calls take the host-driven path directly (their status is read later).
+  const bool async = opts && opts->async;
   KS_TRY(begin_call(c, s, opts));
-  kascade_status st = rank_batch_impl(*c, segs, num_segs, input, weights, total_n, root_out, rank_out, opts, s);
+  kascade_status st = rank_batch_impl(*c, segs, num_segs, input, weights, total_n, root_out, rank_out, opts, s, !async);
+  st = end_call(c, s, st, opts);
+  if (st != KASCADE_ERR_TIMEOUT || async) return st;
+  KS_TRY(begin_call(c, s, opts));
+  st = rank_batch_impl(*c, segs, num_segs, input, weights, total_n, root_out, rank_out, opts, s, false);
   return end_call(c, s, st, opts);
+}
+
+extern "C++" {
+namespace ks {
+kascade_status rank_batch_device_call(kascade_ctx* c, const kascade_segment* segs, uint32_t nseg, const uint64_t* in,
+                                      const uint32_t* weights, uint64_t total, uint64_t* root_out,
+                                      uint64_t* rank_out, const kascade_opts* opts, cudaStream_t s) {
+  KS_TRY(begin_call(c, s, opts));
+  const kascade_status st = rank_batch_impl(*c, segs, nseg, in, weights, total, root_out, rank_out, opts, s, true);
+  return end_call(c, s, st, opts);
+}
+kascade_status batch_plan_create(int device, const kascade_segment* segs, uint32_t nseg, const uint64_t* in,
+                                 const uint32_t* weights, uint64_t total, uint64_t* root_out, uint64_t* rank_out,
+                                 const kascade_opts* opts, kascade_batch_plan** out);
+kascade_status batch_plan_launch(kascade_batch_plan* plan, cudaStream_t s);
+}  // namespace ks
+}  // extern "C++"
+
+KASCADE_API kascade_status kascade_batch_plan_create(int device, const kascade_segment* segs, uint32_t num_segs,
+                                                     const uint64_t* input, const uint32_t* weights, uint64_t total_n,
+                                                     uint64_t* root_out, uint64_t* rank_out,
+                                                     const kascade_opts* opts, kascade_batch_plan** plan) {
+  if (!plan) return KASCADE_ERR_INVALID_ARG;
+  return batch_plan_create(device, segs, num_segs, input, weights, total_n, root_out, rank_out, opts, plan);
+}
+
+KASCADE_API kascade_status kascade_batch_plan_launch(kascade_batch_plan* plan, void* stream) {
+  return batch_plan_launch(plan, as_stream(stream));
 }
 
 KASCADE_API kascade_status kascade_ctx_set_size_classes(kascade_ctx* c, const uint64_t* max_size,

@@ -236,7 +236,11 @@ __global__ void __launch_bounds__(256) k_prepare_tma(const uint64_t* __restrict_
 
 // Deeper levels: the chase of the level above wrote the records (tag
 // unreached); sample rulers in place and record each ruler's level-0 index.
+// n_dev (device-driven recursion): the level's size is read from device
+// memory, n is then its capacity; rulers beyond cap_next are reported as an
+// overflow (KASCADE_ERR_TIMEOUT, the caller reruns on the host-driven path).
 __global__ void __launch_bounds__(256) k_prepare_level(Rec* __restrict__ rec, uint32_t n,
+                                                       const uint32_t* __restrict__ n_dev, uint32_t cap_next,
                                                        const uint32_t* __restrict__ elem0,
                                                        uint32_t* __restrict__ ruler_elem,
                                                        uint32_t* __restrict__ elem0_next,
@@ -244,6 +248,7 @@ __global__ void __launch_bounds__(256) k_prepare_level(Rec* __restrict__ rec, ui
                                                        uint32_t thresh, DevStatus* st) {
   __shared__ uint32_t sm[33];
   __shared__ uint32_t sbase;
+  if (n_dev) n = min(*n_dev, n);
   const uint64_t tile_sz = (uint64_t)blockDim.x * PREP_ITEMS;
   for (uint64_t tile = (uint64_t)blockIdx.x * tile_sz; tile < n; tile += (uint64_t)gridDim.x * tile_sz) {
     Rec rv[PREP_ITEMS];
@@ -275,9 +280,13 @@ __global__ void __launch_bounds__(256) k_prepare_level(Rec* __restrict__ rec, ui
         Rec r = rv[i];
         r.c = TAG_UNREACHED;
         if (rl & (1u << i)) {
-          r.c = TAG_RULER | id;
-          ruler_elem[id] = (uint32_t)x;
-          elem0_next[id] = elem0 ? elem0[x] : (uint32_t)x;
+          if (id < cap_next) {
+            r.c = TAG_RULER | id;
+            ruler_elem[id] = (uint32_t)x;
+            elem0_next[id] = elem0 ? elem0[x] : (uint32_t)x;
+          } else {
+            set_error(st, KASCADE_ERR_TIMEOUT, id);  // more rulers than the next level holds
+          }
           id++;
         }
         rec[x] = r;
@@ -306,10 +315,13 @@ __device__ __forceinline__ void end_chain_on_error(Rec* rec_next, uint32_t id) {
 // (weight = distance to that ruler, successor = that ruler's id).
 // ---------------------------------------------------------------------------
 template <int C>
-__global__ void __launch_bounds__(512) k_chase(Rec* __restrict__ rec, uint32_t n,
+__global__ void __launch_bounds__(512) k_chase(Rec* __restrict__ rec, uint32_t n, const uint32_t* __restrict__ n_dev,
                                                const uint32_t* __restrict__ ruler_elem, uint32_t r,
-                                               Rec* __restrict__ rec_next, uint32_t* __restrict__ work,
-                                               DevStatus* st) {
+                                               const uint32_t* __restrict__ r_dev, Rec* __restrict__ rec_next,
+                                               uint32_t* __restrict__ work, DevStatus* st) {
+  // device-driven recursion: sizes from device memory, n and r capacities
+  if (n_dev) n = min(*n_dev, n);
+  if (r_dev) r = min(*r_dev, r);
   constexpr uint32_t BATCH = 32u * C;
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t lt = lanemask_lt();
@@ -419,8 +431,13 @@ __global__ void __launch_bounds__(512) k_chase(Rec* __restrict__ rec, uint32_t n
 // ---------------------------------------------------------------------------
 template <class Sink>
 __global__ void __launch_bounds__(256) k_propagate(const Rec* __restrict__ rec, uint32_t n_out, uint32_t n_all,
-                                                   uint64_t start, const Out* __restrict__ out_next, Sink sink,
+                                                   const uint32_t* __restrict__ n_dev, uint64_t start,
+                                                   const Out* __restrict__ out_next, uint32_t out_cap, Sink sink,
                                                    DevStatus* st) {
+  // out_cap: entries of out_next.  Only the device-driven recursion can meet
+  // a larger id (a level that outgrew its capacity, already reported as
+  // KASCADE_ERR_TIMEOUT); such elements are skipped.
+  if (n_dev) n_all = n_out = min(*n_dev, n_out);
   const uint32_t stride = gridDim.x * blockDim.x;
   const uint64_t pol = l2_keep_policy();
   for (uint64_t base = start + (uint64_t)blockIdx.x * blockDim.x * PROP_ITEMS + threadIdx.x; base < n_out;
@@ -438,8 +455,10 @@ __global__ void __launch_bounds__(256) k_propagate(const Rec* __restrict__ rec, 
     for (int i = 0; i < PROP_ITEMS; ++i) {
       uint64_t x = base + (uint64_t)i * blockDim.x;
       ov[i] = Out{0, 0, 0};
-      if (x < n_out && !tag_unreached(rv[i].c))
-        ov[i] = ld_out_keep(out_next + (tag_ruler(rv[i].c) ? tag_id(rv[i].c) : rv[i].c), pol);
+      if (x < n_out && !tag_unreached(rv[i].c)) {
+        const uint32_t id = tag_ruler(rv[i].c) ? tag_id(rv[i].c) : rv[i].c;
+        if (id < out_cap) ov[i] = ld_out_keep(out_next + id, pol);
+      }
     }
 #pragma unroll
     for (int i = 0; i < PROP_ITEMS; ++i) {
@@ -472,9 +491,18 @@ __global__ void __launch_bounds__(256) k_propagate(const Rec* __restrict__ rec, 
           set_error(st, KASCADE_ERR_CYCLE, x);
           continue;
         }
-        o = ld_out(out_next + (tag_ruler(r.c) ? tag_id(r.c) : r.c));
-      } else if (tag_ruler(r.c)) {
-        is_root = (r.b == (uint32_t)x);
+        const uint32_t id = tag_ruler(r.c) ? tag_id(r.c) : r.c;
+        if (id >= out_cap) {
+          set_error(st, KASCADE_ERR_TIMEOUT, id);
+          continue;
+        }
+        o = ld_out(out_next + id);
+      } else {
+        if ((tag_ruler(r.c) ? tag_id(r.c) : r.c) >= out_cap) {
+          set_error(st, KASCADE_ERR_TIMEOUT, x);
+          continue;
+        }
+        if (tag_ruler(r.c)) is_root = (r.b == (uint32_t)x);
       }
       uint64_t rank;
       uint32_t root;
@@ -559,8 +587,10 @@ __global__ void __launch_bounds__(BASE_THREADS) k_base(const Rec* __restrict__ r
 // pointer doubling: double-buffered jump rounds over 16 B records.
 // done bit 0: successor is a root; bit 1: the element is a root.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_pd_init(const Rec* __restrict__ rec, uint32_t n, PdRec* __restrict__ a,
+__global__ void __launch_bounds__(256) k_pd_init(const Rec* __restrict__ rec, uint32_t n,
+                                                 const uint32_t* __restrict__ n_dev, PdRec* __restrict__ a,
                                                  DevStatus* st) {
+  if (n_dev) n = min(*n_dev, n);
   for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; x < n; x += (uint64_t)gridDim.x * blockDim.x) {
     Rec r = rec[x];
     if (r.b >= n) {  // guard: treat as a root and report
@@ -577,7 +607,8 @@ __global__ void __launch_bounds__(256) k_pd_init(const Rec* __restrict__ rec, ui
 }
 
 __global__ void __launch_bounds__(256) k_pd_round(const PdRec* __restrict__ a, PdRec* __restrict__ b, uint32_t n,
-                                                  uint32_t* __restrict__ active) {
+                                                  const uint32_t* __restrict__ n_dev, uint32_t* __restrict__ active) {
+  if (n_dev) n = min(*n_dev, n);
   uint32_t cnt = 0;
   for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; x < n; x += (uint64_t)gridDim.x * blockDim.x) {
     PdRec e = a[x];
@@ -597,13 +628,30 @@ __global__ void __launch_bounds__(256) k_pd_round(const PdRec* __restrict__ a, P
 
 template <class Sink>
 __global__ void __launch_bounds__(256) k_pd_final(const PdRec* __restrict__ a, uint32_t n,
+                                                  const uint32_t* __restrict__ n_dev,
                                                   const uint32_t* __restrict__ elem0, Sink sink) {
+  if (n_dev) n = min(*n_dev, n);
   for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; x < n; x += (uint64_t)gridDim.x * blockDim.x) {
     PdRec e = a[x];
     uint32_t rt = e.succ;
     if (elem0) rt = elem0[rt];
     sink.put((uint32_t)x, e.rank, rt, (e.done & 2u) != 0u);
   }
+}
+
+// After a fixed number of rounds every element must point at a root; one that
+// does not sits on a rootless cycle.
+__global__ void __launch_bounds__(256) k_pd_check(const PdRec* __restrict__ a, uint32_t n,
+                                                  const uint32_t* __restrict__ n_dev, DevStatus* st) {
+  if (n_dev) n = min(*n_dev, n);
+  for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; x < n; x += (uint64_t)gridDim.x * blockDim.x)
+    if (!(a[x].done & 1u)) set_error(st, KASCADE_ERR_CYCLE, x);
+}
+
+// A level's size (device) against its capacity: more means the device-driven
+// recursion cannot hold it; the caller reruns on the host-driven path.
+__global__ void k_check_count(const uint32_t* __restrict__ cnt, uint32_t cap, DevStatus* st) {
+  if (*cnt > cap) set_error(st, KASCADE_ERR_TIMEOUT, *cnt);
 }
 
 // ---------------------------------------------------------------------------
@@ -647,7 +695,7 @@ kascade_status launch_chase_c(kascade_ctx& ctx, Rec* rec, uint32_t n, const uint
   uint64_t need_blocks = (need + warps_per_block - 1) / warps_per_block;
   if (need_blocks < grid) grid = (unsigned)(need_blocks ? need_blocks : 1);
   ProfScope ps(ctx, "chase", s);
-  k_chase<C><<<grid, block, 0, s>>>(rec, n, ruler_elem, r, rec_next, work, ctx.d_status);
+  k_chase<C><<<grid, block, 0, s>>>(rec, n, nullptr, ruler_elem, r, nullptr, rec_next, work, ctx.d_status);
   KS_CHECK_LAUNCH();
   return KASCADE_OK;
 }
@@ -667,12 +715,44 @@ kascade_status launch_chase(kascade_ctx& ctx, Rec* rec, uint32_t n, const uint32
   }
 }
 
+// Chase with sizes in device memory: n and r are the capacities.
+template <int C>
+kascade_status launch_chase_dev_c(kascade_ctx& ctx, Rec* rec, uint32_t n, const uint32_t* n_dev,
+                                  const uint32_t* ruler_elem, uint32_t r, const uint32_t* r_dev, Rec* rec_next,
+                                  uint32_t* work, uint32_t block, cudaStream_t s) {
+  static int occ[3] = {-1, -1, -1};
+  const int bi = block == 128 ? 0 : block == 512 ? 2 : 1;
+  if (occ[bi] < 0) occ[bi] = occupancy(k_chase<C>, (int)block, 0);
+  unsigned grid = (unsigned)(ctx.usable_sms() * occ[bi]);
+  const uint64_t warps_per_block = block / 32;
+  const uint64_t need = ((uint64_t)r + 32ull * C - 1) / (32ull * C);
+  const uint64_t need_blocks = (need + warps_per_block - 1) / warps_per_block;
+  if (need_blocks < grid) grid = (unsigned)(need_blocks ? need_blocks : 1);
+  ProfScope ps(ctx, "chase", s);
+  k_chase<C><<<grid, block, 0, s>>>(rec, n, n_dev, ruler_elem, r, r_dev, rec_next, work, ctx.d_status);
+  KS_CHECK_LAUNCH();
+  return KASCADE_OK;
+}
+
+kascade_status launch_chase_dev(kascade_ctx& ctx, Rec* rec, uint32_t n, const uint32_t* n_dev,
+                                const uint32_t* ruler_elem, uint32_t r, const uint32_t* r_dev, Rec* rec_next,
+                                uint32_t* work, const Params& p, cudaStream_t s) {
+  switch (p.chains) {
+    case 1:
+      return launch_chase_dev_c<1>(ctx, rec, n, n_dev, ruler_elem, r, r_dev, rec_next, work, p.block, s);
+    case 4:
+      return launch_chase_dev_c<4>(ctx, rec, n, n_dev, ruler_elem, r, r_dev, rec_next, work, p.block, s);
+    default:
+      return launch_chase_dev_c<2>(ctx, rec, n, n_dev, ruler_elem, r, r_dev, rec_next, work, p.block, s);
+  }
+}
+
 template <class Sink>
 kascade_status launch_propagate(kascade_ctx& ctx, const Rec* rec, uint32_t n_out, uint32_t n_all, const Out* out_next,
-                                const Sink& sink, cudaStream_t s) {
+                                uint32_t out_cap, const Sink& sink, cudaStream_t s) {
   ProfScope ps(ctx, "propagate", s);
   const unsigned grid = grid_for(ctx, ((uint64_t)n_out + PROP_ITEMS - 1) / PROP_ITEMS, 256, 8);
-  k_propagate<Sink><<<grid, 256, 0, s>>>(rec, n_out, n_all, 0, out_next, sink, ctx.d_status);
+  k_propagate<Sink><<<grid, 256, 0, s>>>(rec, n_out, n_all, nullptr, 0, out_next, out_cap, sink, ctx.d_status);
   KS_CHECK_LAUNCH();
   return KASCADE_OK;
 }
@@ -806,7 +886,7 @@ kascade_status pointer_double_records(kascade_ctx& ctx, const Rec* rec, uint32_t
   unsigned grid = grid_for(ctx, n, 256, 8);
   {
     ProfScope ps(ctx, "pd_init", s);
-    k_pd_init<<<grid, 256, 0, s>>>(rec, n, a, ctx.d_status);
+    k_pd_init<<<grid, 256, 0, s>>>(rec, n, nullptr, a, ctx.d_status);
     KS_CHECK_LAUNCH();
   }
   int rounds = 0;
@@ -814,7 +894,7 @@ kascade_status pointer_double_records(kascade_ctx& ctx, const Rec* rec, uint32_t
     KS_CUDA(cudaMemsetAsync(active, 0, sizeof(uint32_t), s));
     {
       ProfScope ps(ctx, "pd_round", s);
-      k_pd_round<<<grid, 256, 0, s>>>(a, b, n, active);
+      k_pd_round<<<grid, 256, 0, s>>>(a, b, n, nullptr, active);
       KS_CHECK_LAUNCH();
     }
     PdRec* t = a;
@@ -830,7 +910,7 @@ kascade_status pointer_double_records(kascade_ctx& ctx, const Rec* rec, uint32_t
   }
   {
     ProfScope ps(ctx, "pd_final", s);
-    k_pd_final<Sink><<<grid, 256, 0, s>>>(a, n, elem0, sink);
+    k_pd_final<Sink><<<grid, 256, 0, s>>>(a, n, nullptr, elem0, sink);
     KS_CHECK_LAUNCH();
   }
   return KASCADE_OK;
@@ -850,8 +930,8 @@ kascade_status rank_deep(kascade_ctx& ctx, Rec* rec, uint32_t n, const uint32_t*
   unsigned grid = grid_for(ctx, ((uint64_t)n + 256 * PREP_ITEMS - 1) / (256 * PREP_ITEMS) * 256, 256, 8);
   {
     ProfScope ps(ctx, "prepare_level", s);
-    k_prepare_level<<<grid, 256, 0, s>>>(rec, n, elem0, ruler_elem, elem0_next, ctr, salt_for(p.seed, level),
-                                         thresh_for(p.spacing_deep), ctx.d_status);
+    k_prepare_level<<<grid, 256, 0, s>>>(rec, n, nullptr, n, elem0, ruler_elem, elem0_next, ctr,
+                                         salt_for(p.seed, level), thresh_for(p.spacing_deep), ctx.d_status);
     KS_CHECK_LAUNCH();
   }
   uint32_t r = 0;
@@ -863,7 +943,7 @@ kascade_status rank_deep(kascade_ctx& ctx, Rec* rec, uint32_t n, const uint32_t*
   if (!rec_next || !out_next) return KASCADE_ERR_OOM;
   KS_TRY(launch_chase(ctx, rec, n, ruler_elem, r, rec_next, p, s));
   KS_TRY(rank_deep(ctx, rec_next, r, elem0_next, SinkOut{out_next}, level + 1, p, s));
-  return launch_propagate(ctx, rec, n, n, out_next, sink, s);
+  return launch_propagate(ctx, rec, n, n, out_next, r, sink, s);
 }
 
 }  // namespace
@@ -890,8 +970,134 @@ kascade_status rank_records(kascade_ctx& ctx, Rec* rec, uint32_t n, uint32_t r0,
   KS_TRY(launch_chase(ctx, rec, n, ruler_elem0, r0, rec1, p, s));
   // level-1 elements are level-0 rulers: their level-0 index is ruler_elem0
   KS_TRY(rank_deep(ctx, rec1, r0, ruler_elem0, SinkOut{out1}, 1, p, s));
-  return launch_propagate(ctx, rec, sink.limit(n), n, out1, sink, s);
+  return launch_propagate(ctx, rec, sink.limit(n), n, out1, r0, sink, s);
 }
+
+// ---------------------------------------------------------------------------
+// Recursion without host waits.  Level sizes stay in device memory; every
+// kernel is sized for its level's capacity and reads the size at run time.
+// Capacities shrink by the deep-level ruler density (1.5x margin plus room for
+// roots); the last level (at most DEV_FINAL elements, or the first that stops
+// shrinking) runs pointer doubling for a fixed number of rounds.  A level that
+// outgrows its capacity reports KASCADE_ERR_TIMEOUT and the caller reruns on
+// the host-driven path.  The sequence of launches depends only on n and the
+// capacities, so it can be captured in a CUDA graph.
+// ---------------------------------------------------------------------------
+constexpr int MAX_DEV_LEVELS = 8;
+constexpr uint32_t DEV_FINAL = 1u << 17;
+constexpr uint32_t DEV_ROOT_MARGIN = 1u << 16;
+
+uint32_t dev_cap_next(uint32_t cap, uint32_t spacing) {
+  const uint64_t nx = (uint64_t)cap * 3 / (2ull * (spacing < 2 ? 2 : spacing)) + DEV_ROOT_MARGIN;
+  return nx < cap ? (uint32_t)nx : cap;
+}
+
+template <class Sink>
+kascade_status rank_records_dev(kascade_ctx& ctx, Rec* rec, uint32_t n, const uint32_t* r0_dev, uint32_t cap1,
+                                uint32_t* ruler_elem0, const Sink& sink, const Params& p, cudaStream_t s) {
+  ctx.last_levels.clear();
+  ctx.last_levels.push_back(n);
+  if (n == 0) return KASCADE_OK;
+  uint32_t caps[MAX_DEV_LEVELS + 1];
+  caps[0] = n;
+  caps[1] = cap1 < n ? cap1 : n;
+  int L = 1;
+  while (caps[L] > DEV_FINAL && L < MAX_DEV_LEVELS) {
+    const uint32_t nx = dev_cap_next(caps[L], p.spacing_deep);
+    if ((uint64_t)nx * 10 >= (uint64_t)caps[L] * 9) break;  // no longer shrinking: final level here
+    caps[L + 1] = nx;
+    ++L;
+  }
+  for (int k = 1; k <= L; ++k) ctx.last_levels.push_back(caps[k]);  // capacities, not sizes
+  uint32_t* cnt = alloc<uint32_t>(ctx, MAX_DEV_LEVELS + 2);
+  if (!cnt) return KASCADE_ERR_OOM;
+  KS_CUDA(cudaMemsetAsync(cnt, 0, sizeof(uint32_t) * (MAX_DEV_LEVELS + 2), s));
+  Rec* recs[MAX_DEV_LEVELS + 1];
+  Out* outs[MAX_DEV_LEVELS + 1];
+  uint32_t* rulers[MAX_DEV_LEVELS + 1];
+  const uint32_t* elem0s[MAX_DEV_LEVELS + 1];
+  const uint32_t* sizes[MAX_DEV_LEVELS + 1];
+  recs[0] = rec;
+  rulers[0] = ruler_elem0;
+  elem0s[1] = ruler_elem0;  // level-1 elements are level-0 rulers
+  sizes[1] = r0_dev;
+  for (int k = 1; k <= L; ++k) {
+    recs[k] = alloc<Rec>(ctx, caps[k]);
+    outs[k] = alloc<Out>(ctx, caps[k]);
+    if (!recs[k] || !outs[k]) return KASCADE_ERR_OOM;
+    if (k < L) {
+      rulers[k] = alloc<uint32_t>(ctx, caps[k + 1]);
+      uint32_t* e0 = alloc<uint32_t>(ctx, caps[k + 1]);
+      if (!rulers[k] || !e0) return KASCADE_ERR_OOM;
+      elem0s[k + 1] = e0;
+      sizes[k + 1] = cnt + k + 1;
+    }
+  }
+  k_check_count<<<1, 1, 0, s>>>(r0_dev, caps[1], ctx.d_status);
+  KS_CHECK_LAUNCH();
+  // level 0 chase: capacities as bounds, the ruler count from device memory
+  {
+    uint32_t* work = alloc<uint32_t>(ctx, 1);
+    if (!work) return KASCADE_ERR_OOM;
+    KS_CUDA(cudaMemsetAsync(work, 0, sizeof(uint32_t), s));
+    KS_TRY(launch_chase_dev(ctx, recs[0], n, nullptr, rulers[0], caps[1], r0_dev, recs[1], work, p, s));
+  }
+  for (int k = 1; k < L; ++k) {
+    {
+      ProfScope ps(ctx, "prepare_level", s);
+      const unsigned grid =
+          grid_for(ctx, ((uint64_t)caps[k] + 256 * PREP_ITEMS - 1) / (256 * PREP_ITEMS) * 256, 256, 8);
+      k_prepare_level<<<grid, 256, 0, s>>>(recs[k], caps[k], sizes[k], caps[k + 1], elem0s[k], rulers[k],
+                                           const_cast<uint32_t*>(elem0s[k + 1]), cnt + k + 1,
+                                           salt_for(p.seed, k), thresh_for(p.spacing_deep), ctx.d_status);
+      KS_CHECK_LAUNCH();
+    }
+    uint32_t* work = alloc<uint32_t>(ctx, 1);
+    if (!work) return KASCADE_ERR_OOM;
+    KS_CUDA(cudaMemsetAsync(work, 0, sizeof(uint32_t), s));
+    KS_TRY(launch_chase_dev(ctx, recs[k], caps[k], sizes[k], rulers[k], caps[k + 1], sizes[k + 1], recs[k + 1], work,
+                            p, s));
+  }
+  // final level: pointer doubling, enough rounds for any list it can hold
+  {
+    const uint32_t m = caps[L];
+    PdRec* a = alloc<PdRec>(ctx, m);
+    PdRec* b = alloc<PdRec>(ctx, m);
+    uint32_t* active = alloc<uint32_t>(ctx, 1);
+    if (!a || !b || !active) return KASCADE_ERR_OOM;
+    const unsigned grid = grid_for(ctx, m, 256, 8);
+    ProfScope ps(ctx, "pd_final_level", s);
+    k_pd_init<<<grid, 256, 0, s>>>(recs[L], m, sizes[L], a, ctx.d_status);
+    KS_CHECK_LAUNCH();
+    int rounds = 2;
+    while ((1ull << (rounds - 2)) < m) ++rounds;
+    for (int i = 0; i < rounds; ++i) {
+      k_pd_round<<<grid, 256, 0, s>>>(a, b, m, sizes[L], active);
+      KS_CHECK_LAUNCH();
+      PdRec* t = a;
+      a = b;
+      b = t;
+    }
+    k_pd_check<<<grid, 256, 0, s>>>(a, m, sizes[L], ctx.d_status);
+    KS_CHECK_LAUNCH();
+    k_pd_final<SinkOut><<<grid, 256, 0, s>>>(a, m, sizes[L], elem0s[L], SinkOut{outs[L]});
+    KS_CHECK_LAUNCH();
+  }
+  // propagate back up
+  for (int k = L - 1; k >= 1; --k) {
+    ProfScope ps(ctx, "propagate", s);
+    const unsigned grid = grid_for(ctx, ((uint64_t)caps[k] + PROP_ITEMS - 1) / PROP_ITEMS, 256, 8);
+    k_propagate<SinkOut><<<grid, 256, 0, s>>>(recs[k], caps[k], caps[k], sizes[k], 0, outs[k + 1], caps[k + 1],
+                                              SinkOut{outs[k]}, ctx.d_status);
+    KS_CHECK_LAUNCH();
+  }
+  return launch_propagate(ctx, rec, sink.limit(n), n, outs[1], caps[1], sink, s);
+}
+
+template kascade_status rank_records_dev<SinkBatch>(kascade_ctx&, Rec*, uint32_t, const uint32_t*, uint32_t,
+                                                    uint32_t*, const SinkBatch&, const Params&, cudaStream_t);
+template kascade_status rank_records_dev<SinkPlain>(kascade_ctx&, Rec*, uint32_t, const uint32_t*, uint32_t,
+                                                    uint32_t*, const SinkPlain&, const Params&, cudaStream_t);
 
 kascade_status rank_sublist(kascade_ctx& ctx, Rec* rec, uint32_t n, const uint32_t* elem0, Out* out, int level,
                             const Params& p, cudaStream_t s) {

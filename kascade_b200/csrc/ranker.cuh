@@ -165,6 +165,15 @@ kascade_status rank_sublist(kascade_ctx& ctx, Rec* rec, uint32_t n, const uint32
 // Write-free level 0: read-only chase that logs (element, ruler, distance),
 // recursion on the ruler sub-list, then resolve + partition by element window
 // and a windowed scatter into the outputs.
+// The recursion without host waits (see ranker.cu): r0_dev holds the level-0
+// ruler count, cap1 bounds it.  Errors, including a level that outgrows its
+// capacity (KASCADE_ERR_TIMEOUT: rerun on the host-driven path), land in the
+// device status word.
+template <class Sink>
+kascade_status rank_records_dev(kascade_ctx& ctx, Rec* rec, uint32_t n, const uint32_t* r0_dev, uint32_t cap1,
+                                uint32_t* ruler_elem0, const Sink& sink, const Params& p, cudaStream_t s);
+uint32_t dev_cap_next(uint32_t cap, uint32_t spacing);
+
 kascade_status compute_stats(kascade_ctx& ctx, const uint64_t* root, const int64_t* rank, uint64_t n, int level,
                              kascade_stats* out, kascade_tree_stats* per_tree, uint64_t per_tree_cap,
                              uint64_t* per_tree_count, cudaStream_t s);

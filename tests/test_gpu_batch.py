@@ -54,6 +54,55 @@ def test_batch_large_instances(kb, oracle_mod):
     _check(kb, oracle_mod, inputs, w, sizes, kinds, root, rank)
 
 
+def test_batch_device_levels_and_fallback(kb, oracle_mod):
+    """The batch recursion keeps level sizes on the device; a batch whose
+    levels outgrow their capacities (every element a root) is ranked again on
+    the host-driven path, with the same exact results."""
+    # normal: a batch big enough for several device-driven levels
+    sizes, kinds = kb.batch_sizes(64, seed=21, lo_log2=12, hi_log2=19)
+    inputs, w = kb.gen_batch(sizes, kinds, seed=23)
+    ctx = kb.Context()
+    root, rank = kb.rank_batch(inputs, kb.make_segments(sizes, kinds), w, ctx=ctx)
+    _check(kb, oracle_mod, inputs, w, sizes, kinds, root, rank)
+    # all roots: level 1 is as large as level 0
+    sizes = np.full(40, 50_000, np.int64)
+    kinds = np.zeros(40, np.int64)
+    inputs = torch.cat([torch.arange(50_000, dtype=torch.int64, device="cuda") for _ in range(40)])
+    root, rank = kb.rank_batch(inputs, kb.make_segments(sizes, kinds), None, ctx=ctx)
+    _check(kb, oracle_mod, inputs, None, sizes, kinds, root, rank)
+    ctx.close()
+
+
+def test_batch_plan_graph_replay(kb, oracle_mod):
+    """A batch captured as a CUDA graph: replays give the plain call's exact
+    results, also after the inputs' contents change in place."""
+    sizes, kinds = kb.batch_sizes(200, seed=31, lo_log2=6, hi_log2=16)
+    inputs, w = kb.gen_batch(sizes, kinds, seed=33)
+    segs = kb.make_segments(sizes, kinds)
+    plan = kb.BatchPlan(inputs, segs, w)
+    for _ in range(2):
+        root, rank = plan.launch()
+        torch.cuda.synchronize()
+        _check(kb, oracle_mod, inputs, w, sizes, kinds, root, rank)
+    # new contents, same shape
+    inputs2, w2 = kb.gen_batch(sizes, kinds, seed=35)
+    inputs.copy_(inputs2)
+    w.copy_(w2)
+    root, rank = plan.launch()
+    torch.cuda.synchronize()
+    _check(kb, oracle_mod, inputs, w, sizes, kinds, root, rank)
+    r_p, k_p = kb.rank_batch(inputs, segs, w)
+    assert torch.equal(root, r_p) and torch.equal(rank, k_p)
+    plan.close()
+    # a batch that needs the host-driven recursion cannot be planned
+    sizes = np.full(40, 50_000, np.int64)
+    kinds = np.zeros(40, np.int64)
+    roots = torch.cat([torch.arange(50_000, dtype=torch.int64, device="cuda") for _ in range(40)])
+    with pytest.raises(kb.KascadeError) as e:
+        kb.BatchPlan(roots, kb.make_segments(sizes, kinds))
+    assert e.value.name == "UNSUPPORTED"
+
+
 def test_batch_only_lists_and_only_forests(kb, oracle_mod):
     for kind in (0, 1):
         sizes = np.array([5000, 1, 7, 20000, 333], np.int64)
