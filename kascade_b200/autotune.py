@@ -26,7 +26,7 @@ from pathlib import Path
 import numpy as np
 
 # class upper bounds (elements; ranking records for forests are 2 per vertex)
-CLASS_MAX = (1 << 10, 1 << 13, 1 << 16, 1 << 19, 1 << 22, 1 << 25, (1 << 64) - 1)
+CLASS_MAX = (1 << 10, 1 << 13, 1 << 16, 1 << 19, 1 << 22, 1 << 25, 1 << 27, (1 << 64) - 1)
 SPACINGS = (4, 6, 8, 12, 16, 24, 32, 48, 64, 96, 128)
 CHAINS = (1, 2, 4)
 BLOCKS = (128, 256, 512)
@@ -76,8 +76,8 @@ def tune(device: int = 0, total: int = 1 << 24, reps: int = 3, log=print) -> dic
     ctx = kb.Context(device)
     classes = []
     for k, cmax in enumerate(CLASS_MAX):
-        # the two largest classes: a few instances of up to 2^25 / 2^28 elements
-        scale = 1 if k + 2 < len(CLASS_MAX) else (4 if k + 2 == len(CLASS_MAX) else 16)
+        # the three largest classes: a few instances each (up to 2^25, 2^27, 2^28 elements)
+        scale = {len(CLASS_MAX) - 3: 4, len(CLASS_MAX) - 2: 8, len(CLASS_MAX) - 1: 24}.get(k, 1)
         sizes, kinds = class_sizes(k, scale * total, 0xA7 + k)
         kinds = np.where(kinds == 0, kb.SEG_LIST, kb.SEG_FOREST)
         inp, w = kb.gen_batch(sizes, kinds, seed=0x7E + k, device=dev)

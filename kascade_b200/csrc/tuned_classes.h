@@ -4,9 +4,9 @@
 // library starts every context with it.
 #pragma once
 #define KS_TUNED_GPU "NVIDIA B200"
-#define KS_TUNED_COUNT 7
-#define KS_TUNED_MAX {1024ull, 8192ull, 65536ull, 524288ull, 4194304ull, 33554432ull, ~0ull}
-#define KS_TUNED_SPACING {4u, 8u, 6u, 6u, 8u, 24u, 64u}
-#define KS_TUNED_SPACING_SINGLE {128u, 6u, 12u, 8u, 24u, 12u, 48u}
-#define KS_TUNED_CHAINS {1u, 1u, 1u, 1u, 1u, 1u, 1u}
-#define KS_TUNED_BLOCK {128u, 512u, 512u, 128u, 128u, 512u, 128u}
+#define KS_TUNED_COUNT 8
+#define KS_TUNED_MAX {1024ull, 8192ull, 65536ull, 524288ull, 4194304ull, 33554432ull, 134217728ull, ~0ull}
+#define KS_TUNED_SPACING {4u, 6u, 6u, 4u, 6u, 12u, 24u, 96u}
+#define KS_TUNED_SPACING_SINGLE {48u, 6u, 12u, 12u, 24u, 32u, 24u, 96u}
+#define KS_TUNED_CHAINS {1u, 1u, 1u, 1u, 1u, 1u, 4u, 4u}
+#define KS_TUNED_BLOCK {256u, 128u, 128u, 512u, 512u, 512u, 512u, 512u}
