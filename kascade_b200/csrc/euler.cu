@@ -82,7 +82,8 @@ struct SlotsBatch {
 // written slots and numbers them (one atomic per tile, as in prepare).
 template <class Slots>
 __global__ void __launch_bounds__(256) k_tour_build(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
-                                                    uint32_t n, const uint2* __restrict__ seg, Rec* __restrict__ rec,
+                                                    uint32_t n, const uint2* __restrict__ seg,
+                                                    const uint32_t* __restrict__ root_bits, Rec* __restrict__ rec,
                                                     uint32_t* __restrict__ ruler_elem, uint32_t* __restrict__ counter,
                                                     uint32_t salt, Slots slots, DevStatus* st) {
   __shared__ uint32_t sm[33];
@@ -131,22 +132,9 @@ __global__ void __launch_bounds__(256) k_tour_build(const uint32_t* __restrict__
         bool head = false;
         bool first = true;
         if (q > 0 && keys[q - 1] == p) first = (vals[q - 1] == p) && (q < 2 || keys[q - 2] != p);
-        if (first) {
-          if (q > 0 && keys[q - 1] == p) {
-            head = true;  // preceded by p's own entry: p is a root
-          } else {
-            const uint2 sp = seg[p];  // p is a root iff its own entry (p, p) is in its segment
-            uint32_t lo = sp.x, hi = sp.y;
-            while (lo < hi) {
-              const uint32_t mid = (lo + hi) >> 1;
-              if (vals[mid] < p)
-                lo = mid + 1;
-              else
-                hi = mid;
-            }
-            head = (lo < sp.y && vals[lo] == p);
-          }
-        }
+        // p is a root: its bit came from the sort's first pass (an L2-resident
+        // bitmap instead of a search of p's children)
+        if (first) head = (__ldg(root_bits + (p >> 5)) >> (p & 31)) & 1u;
         if (sampled(slot_up, salt, th)) {
           rl |= 1u << (2 * i);
           cnt++;
@@ -258,9 +246,14 @@ __global__ void __launch_bounds__(256) k_ref_tour(const uint64_t* __restrict__ p
 }
 
 kascade_status sort_children(kascade_ctx& ctx, const uint64_t* parent, uint32_t n, uint32_t** keys, uint32_t** vals,
-                             uint2** seg, cudaStream_t s) {
+                             uint2** seg, uint32_t** root_bits, cudaStream_t s) {
   SortSource src;
   src.parent = parent;
+  if (root_bits) {
+    *root_bits = alloc<uint32_t>(ctx, ((uint64_t)n + 31) / 32 + 1);
+    if (!*root_bits) return KASCADE_ERR_OOM;
+    src.root_bits = *root_bits;
+  }
   KS_TRY(radix_sort_pairs(ctx, src, n, bits_for(n), keys, vals, s));
   *seg = alloc<uint2>(ctx, n);
   if (!*seg) return KASCADE_ERR_OOM;
@@ -278,7 +271,8 @@ kascade_status root_forest_impl(kascade_ctx& ctx, const uint64_t* parent, uint32
   if (n == 0) return KASCADE_OK;
   uint32_t *keys, *vals;
   uint2* seg;
-  KS_TRY(sort_children(ctx, parent, n, &keys, &vals, &seg, s));
+  uint32_t* root_bits = nullptr;
+  KS_TRY(sort_children(ctx, parent, n, &keys, &vals, &seg, &root_bits, s));
   const uint32_t m = 2 * n;
   Rec* rec = alloc<Rec>(ctx, m);
   uint32_t* ruler_elem = alloc<uint32_t>(ctx, m);
@@ -289,7 +283,7 @@ kascade_status root_forest_impl(kascade_ctx& ctx, const uint64_t* parent, uint32
     ProfScope ps(ctx, "tour_build", s);
     const unsigned grid = grid_for(ctx, ((uint64_t)n + 256 * TB_ITEMS - 1) / (256 * TB_ITEMS) * 256, 256, 8);
     SlotsSingle slots{n, (uint32_t)(4294967296.0 / (double)(p.spacing0 < 2 ? 2 : p.spacing0))};
-    k_tour_build<SlotsSingle><<<grid, 256, 0, s>>>(keys, vals, n, seg, rec, ruler_elem, ctr,
+    k_tour_build<SlotsSingle><<<grid, 256, 0, s>>>(keys, vals, n, seg, root_bits, rec, ruler_elem, ctr,
                                                    mix32(p.seed ^ 0x70757254u), slots, ctx.d_status);
     KS_CHECK_LAUNCH();
   }
@@ -308,11 +302,12 @@ kascade_status batch_tours(kascade_ctx& ctx, const uint64_t* fpar, uint32_t F, c
   if (F == 0) return KASCADE_OK;
   uint32_t *keys, *vals;
   uint2* seg;
-  KS_TRY(sort_children(ctx, fpar, F, &keys, &vals, &seg, s));
+  uint32_t* root_bits = nullptr;
+  KS_TRY(sort_children(ctx, fpar, F, &keys, &vals, &seg, &root_bits, s));
   SlotsBatch slots{fd, foff, fthresh, nf, down_base};
   ProfScope ps(ctx, "tour_build", s);
   const unsigned grid = grid_for(ctx, ((uint64_t)F + 256 * TB_ITEMS - 1) / (256 * TB_ITEMS) * 256, 256, 8);
-  k_tour_build<SlotsBatch><<<grid, 256, 0, s>>>(keys, vals, F, seg, rec, ruler_elem, counter, salt, slots,
+  k_tour_build<SlotsBatch><<<grid, 256, 0, s>>>(keys, vals, F, seg, root_bits, rec, ruler_elem, counter, salt, slots,
                                                 ctx.d_status);
   KS_CHECK_LAUNCH();
   return KASCADE_OK;
@@ -324,7 +319,7 @@ kascade_status compute_euler_tour_impl(kascade_ctx& ctx, const uint64_t* parent,
   if (n == 0) return KASCADE_OK;
   uint32_t *keys, *vals;
   uint2* seg;
-  KS_TRY(sort_children(ctx, parent, n, &keys, &vals, &seg, s));
+  KS_TRY(sort_children(ctx, parent, n, &keys, &vals, &seg, nullptr, s));
   uint32_t* deg = alloc<uint32_t>(ctx, n);
   uint32_t* droot = alloc<uint32_t>(ctx, n);
   uint32_t* xadj = alloc<uint32_t>(ctx, n);

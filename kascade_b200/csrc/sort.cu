@@ -108,19 +108,29 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_hist(SortSource src, cons
     cnt[threadIdx.x] = 0;
     __syncthreads();
     uint64_t base = (uint64_t)tile * SORT_TILE;
-#pragma unroll 4
-    for (int i = 0; i < SORT_ITEMS; ++i) {
+    uint32_t kv[SORT_ITEMS];
+#pragma unroll
+    for (int i = 0; i < SORT_ITEMS; ++i) {  // loads first, all in flight together
       uint64_t x = base + (uint64_t)i * SORT_THREADS + threadIdx.x;
+      kv[i] = 0xFFFFFFFFu;
       if (x < n) {
-        uint32_t k;
         if (FROM_PARENT) {
           unsigned long long p = __ldg(reinterpret_cast<const unsigned long long*>(src.parent) + x);
-          k = (p >= n) ? (uint32_t)x : (uint32_t)p;
+          kv[i] = (p >= n) ? (uint32_t)x : (uint32_t)p;
         } else {
-          k = keys[x];
+          kv[i] = keys[x];
         }
-        atomicAdd(&cnt[(k >> shift) & (RADIX - 1)], 1u);
       }
+      if (FROM_PARENT && src.root_bits) {
+        // a warp's 32 consecutive elements make one word of root bits
+        const uint32_t bits = __ballot_sync(0xffffffffu, x < n && kv[i] == (uint32_t)x);
+        if ((threadIdx.x & 31) == 0 && x < n) src.root_bits[x >> 5] = bits;
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < SORT_ITEMS; ++i) {
+      uint64_t x = base + (uint64_t)i * SORT_THREADS + threadIdx.x;
+      if (x < n) atomicAdd(&cnt[(kv[i] >> shift) & (RADIX - 1)], 1u);
     }
     __syncthreads();
     hist[(uint64_t)threadIdx.x * num_tiles + tile] = cnt[threadIdx.x];
@@ -147,12 +157,20 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_scatter(SortSource src, c
     __syncthreads();
     const uint64_t base = (uint64_t)tile * SORT_TILE + (uint64_t)warp * WARP_ITEMS;
     uint32_t kk[SORT_ITEMS], vv[SORT_ITEMS], rk[SORT_ITEMS];
+    // all of the tile's loads first (independent, in flight together), then
+    // the ranking, which waits on each key in turn
+#pragma unroll
+    for (int j = 0; j < SORT_ITEMS; ++j) {
+      const uint64_t x = base + (uint64_t)j * 32 + lane;
+      kk[j] = 0xFFFFFFFFu;
+      vv[j] = 0;
+      if (x < n) load_pair<FROM_PARENT>(src, keys, vals, n, (uint32_t)x, kk[j], vv[j], st);
+    }
 #pragma unroll
     for (int j = 0; j < SORT_ITEMS; ++j) {
       const uint64_t x = base + (uint64_t)j * 32 + lane;
       const bool valid = x < n;
-      uint32_t k = 0xFFFFFFFFu, v = 0;
-      if (valid) load_pair<FROM_PARENT>(src, keys, vals, n, (uint32_t)x, k, v, st);
+      const uint32_t k = kk[j], v = vv[j];
       const uint32_t d = valid ? ((k >> shift) & (RADIX - 1)) : 0xFFFFu;
       const uint32_t peers = __match_any_sync(FULL, d);
       const uint32_t before = __popc(peers & lt);
