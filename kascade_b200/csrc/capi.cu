@@ -48,6 +48,7 @@ kascade_status begin_call(kascade_ctx* ctx, cudaStream_t s, const kascade_opts* 
   KS_TRY(status_reset(*ctx, s));
   ctx->profile = o && o->profile;
   ctx->async_pending = false;
+  ctx->pending_levels = 0;
   return KASCADE_OK;
 }
 
@@ -68,14 +69,26 @@ kascade_status end_call(kascade_ctx* ctx, cudaStream_t s, kascade_status st, con
   return status_finish(*ctx, s);
 }
 
+// device_levels: the ruling-set recursion keeps its level sizes on the device
+// (no host wait inside the call); a list it cannot hold reports
+// KASCADE_ERR_TIMEOUT and the caller reruns without it.  Only for calls whose
+// outputs are not their inputs (the rerun needs the inputs intact).
 kascade_status rank_list_generic(kascade_ctx& ctx, const uint64_t* succ, WKind wk, const void* w, uint64_t n,
                                  uint64_t* root_out, uint64_t* rank_out, int keep_roots, const Params& p,
-                                 cudaStream_t s) {
+                                 cudaStream_t s, bool device_levels = false) {
   if (n == 0) return KASCADE_OK;
   if (n > MAX_LIST) return KASCADE_ERR_TOO_LARGE;
   Rec* rec = alloc<Rec>(ctx, n);
   uint32_t* ruler_elem = alloc<uint32_t>(ctx, n);
   if (!rec || !ruler_elem) return KASCADE_ERR_OOM;
+  if (device_levels && p.algorithm == KASCADE_ALGO_SPARSE_RULING_SET && n > p.base_max && n < p.level0_log_min &&
+      p.max_levels > 0) {
+    uint32_t* r_dev = nullptr;
+    KS_TRY(prepare_arrays(ctx, succ, wk, w, (uint32_t)n, rec, ruler_elem, nullptr, p, s, &r_dev));
+    SinkPlain sink{root_out, rank_out, keep_roots};
+    return rank_records_dev(ctx, rec, (uint32_t)n, r_dev, dev_cap_next((uint32_t)n, p.spacing0), ruler_elem, sink,
+                            p, s);
+  }
   uint32_t r0 = 0;
   KS_TRY(prepare_arrays(ctx, succ, wk, w, (uint32_t)n, rec, ruler_elem, &r0, p, s));
   SinkPlain sink{root_out, rank_out, keep_roots};
@@ -254,11 +267,18 @@ KASCADE_API kascade_status kascade_rank_list(kascade_ctx* c, const uint64_t* suc
                                              void* stream) {
   cudaStream_t s = as_stream(stream);
   if (n && (!succ || !root_out || !rank_out)) return KASCADE_ERR_INVALID_ARG;
+  const bool dev = !(opts && opts->async);  // an async call's status is read later: no rerun
   KS_TRY(begin_call(c, s, opts));
   Params p = make_params(*c, opts, n);
   kascade_status st = validate_list(*c, succ, n, opts, p, s);
   if (st == KASCADE_OK)
-    st = rank_list_generic(*c, succ, weights ? WKind::U32 : WKind::Unit, weights, n, root_out, rank_out, 0, p, s);
+    st = rank_list_generic(*c, succ, weights ? WKind::U32 : WKind::Unit, weights, n, root_out, rank_out, 0, p, s,
+                           dev);
+  st = end_call(c, s, st, opts);
+  if (st != KASCADE_ERR_TIMEOUT || !dev) return st;
+  // a level outgrew the device-driven recursion: rank again on the host-driven path
+  KS_TRY(begin_call(c, s, opts));
+  st = rank_list_generic(*c, succ, weights ? WKind::U32 : WKind::Unit, weights, n, root_out, rank_out, 0, p, s);
   return end_call(c, s, st, opts);
 }
 

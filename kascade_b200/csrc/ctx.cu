@@ -105,6 +105,12 @@ kascade_status status_finish(kascade_ctx& ctx, cudaStream_t s) {
     return ctx.last_status;
   }
   collect_times(ctx);
+  if (ctx.pending_levels) {
+    const uint32_t* lv = reinterpret_cast<const uint32_t*>(ctx.h_pinned + KS_PINNED_LEVELS);
+    ctx.last_levels.assign(1, ctx.pending_n);
+    for (int k = 1; k <= ctx.pending_levels; ++k) ctx.last_levels.push_back(lv[k]);
+    ctx.pending_levels = 0;
+  }
   const DevStatus* st = reinterpret_cast<const DevStatus*>(ctx.h_pinned);
   ctx.error_info = st->info;
   ctx.last_status = (kascade_status)st->code;

@@ -40,6 +40,10 @@ struct kascade_ctx {
   std::map<std::string, std::pair<double, unsigned long long>> times;
   std::vector<std::string> time_names;  // stable storage for returned names
   std::vector<unsigned long long> last_levels;
+  // level sizes of a device-driven recursion, copied to the pinned buffer by
+  // the call and read into last_levels when its status is read
+  int pending_levels = 0;
+  unsigned long long pending_n = 0;
   unsigned long long error_info = 0;
   kascade_status last_status = KASCADE_OK;
   // ordering between calls issued on different streams: the next call's
@@ -78,6 +82,7 @@ struct kascade_ctx {
 namespace ks {
 
 constexpr int KS_PINNED_WORDS = 64;
+constexpr int KS_PINNED_LEVELS = 40;  // first word of the device-driven level sizes
 
 // Arena -------------------------------------------------------------------
 kascade_status arena_begin_call(kascade_ctx& ctx, cudaStream_t s);

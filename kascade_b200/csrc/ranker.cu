@@ -650,8 +650,11 @@ __global__ void __launch_bounds__(256) k_pd_check(const PdRec* __restrict__ a, u
 
 // A level's size (device) against its capacity: more means the device-driven
 // recursion cannot hold it; the caller reruns on the host-driven path.
-__global__ void k_check_count(const uint32_t* __restrict__ cnt, uint32_t cap, DevStatus* st) {
-  if (*cnt > cap) set_error(st, KASCADE_ERR_TIMEOUT, *cnt);
+__global__ void k_check_count(const uint32_t* __restrict__ cnt, uint32_t cap, uint32_t* __restrict__ copy,
+                              DevStatus* st) {
+  const uint32_t c = *cnt;
+  if (copy) *copy = c;
+  if (c > cap) set_error(st, KASCADE_ERR_TIMEOUT, c);
 }
 
 // ---------------------------------------------------------------------------
@@ -816,9 +819,11 @@ Params make_params(const kascade_ctx& ctx, const kascade_opts* o, uint64_t n) {
 }
 
 kascade_status prepare_arrays(kascade_ctx& ctx, const uint64_t* succ, WKind wk, const void* w, uint32_t n, Rec* rec,
-                              uint32_t* ruler_elem, uint32_t* r_out, const Params& p, cudaStream_t s) {
+                              uint32_t* ruler_elem, uint32_t* r_out, const Params& p, cudaStream_t s,
+                              uint32_t** r_dev) {
   uint32_t* ctr = alloc<uint32_t>(ctx, 1);
   if (!ctr) return KASCADE_ERR_OOM;
+  if (r_dev) *r_dev = ctr;
   KS_CUDA(cudaMemsetAsync(ctr, 0, sizeof(uint32_t), s));
   uint32_t salt = salt_for(p.seed, 0), th = thresh_for(p.spacing0);
   {
@@ -872,7 +877,8 @@ kascade_status prepare_arrays(kascade_ctx& ctx, const uint64_t* succ, WKind wk, 
       KS_CHECK_LAUNCH();
     }
   }
-  return read_u32(ctx, ctr, r_out, s);
+  // r_out == nullptr: the count stays on the device (*r_dev)
+  return r_out ? read_u32(ctx, ctr, r_out, s) : KASCADE_OK;
 }
 
 template <class Sink>
@@ -1008,7 +1014,6 @@ kascade_status rank_records_dev(kascade_ctx& ctx, Rec* rec, uint32_t n, const ui
     caps[L + 1] = nx;
     ++L;
   }
-  for (int k = 1; k <= L; ++k) ctx.last_levels.push_back(caps[k]);  // capacities, not sizes
   uint32_t* cnt = alloc<uint32_t>(ctx, MAX_DEV_LEVELS + 2);
   if (!cnt) return KASCADE_ERR_OOM;
   KS_CUDA(cudaMemsetAsync(cnt, 0, sizeof(uint32_t) * (MAX_DEV_LEVELS + 2), s));
@@ -1033,7 +1038,7 @@ kascade_status rank_records_dev(kascade_ctx& ctx, Rec* rec, uint32_t n, const ui
       sizes[k + 1] = cnt + k + 1;
     }
   }
-  k_check_count<<<1, 1, 0, s>>>(r0_dev, caps[1], ctx.d_status);
+  k_check_count<<<1, 1, 0, s>>>(r0_dev, caps[1], cnt + 1, ctx.d_status);
   KS_CHECK_LAUNCH();
   // level 0 chase: capacities as bounds, the ruler count from device memory
   {
@@ -1091,7 +1096,13 @@ kascade_status rank_records_dev(kascade_ctx& ctx, Rec* rec, uint32_t n, const ui
                                               SinkOut{outs[k]}, ctx.d_status);
     KS_CHECK_LAUNCH();
   }
-  return launch_propagate(ctx, rec, sink.limit(n), n, outs[1], caps[1], sink, s);
+  KS_TRY(launch_propagate(ctx, rec, sink.limit(n), n, outs[1], caps[1], sink, s));
+  // the level sizes travel back with the call's status
+  KS_CUDA(cudaMemcpyAsync(reinterpret_cast<uint32_t*>(ctx.h_pinned + KS_PINNED_LEVELS), cnt,
+                          sizeof(uint32_t) * (L + 1), cudaMemcpyDeviceToHost, s));
+  ctx.pending_levels = L;
+  ctx.pending_n = n;
+  return KASCADE_OK;
 }
 
 template kascade_status rank_records_dev<SinkBatch>(kascade_ctx&, Rec*, uint32_t, const uint32_t*, uint32_t,

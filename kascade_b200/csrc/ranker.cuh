@@ -147,7 +147,7 @@ enum class WKind { Unit, U32, I64 };
 // ruler_elem must hold n entries; *r_out receives the ruler count.
 kascade_status prepare_arrays(kascade_ctx& ctx, const uint64_t* succ, WKind wk, const void* w,
                               uint32_t n, Rec* rec, uint32_t* ruler_elem, uint32_t* r_out,
-                              const Params& p, cudaStream_t s);
+                              const Params& p, cudaStream_t s, uint32_t** r_dev = nullptr);
 
 // Rank level-0 records that carry ruler tags (r0 rulers, listed in
 // ruler_elem0) and deliver the results to the sink.

@@ -116,6 +116,19 @@ def test_input_alignment(kb, oracle_mod, offset):
         np.testing.assert_array_equal(host_u64(rank), ko)
 
 
+def test_device_levels_overflow_rerun(kb, oracle_mod):
+    """Every element a root: the first level is as large as the list, more
+    than the device-driven recursion holds; the call reranks on the
+    host-driven path and the result is exact."""
+    n = 300_000
+    succ_h = np.arange(n, dtype=np.uint64)
+    succ_h[1::2] = np.arange(0, n, 2, dtype=np.uint64)  # pairs: odd -> even, evens are roots
+    root, rank = kb.rank_list(dev64(succ_h))
+    r_o, k_o = oracle_mod.rank_list(succ_h)
+    np.testing.assert_array_equal(host_u64(root), r_o)
+    np.testing.assert_array_equal(host_u64(rank), k_o)
+
+
 @pytest.mark.parametrize("parts", [2, 37, 1000, 20000])
 def test_many_lists(kb, oracle_mod, parts):
     rng = np.random.default_rng(parts)
