@@ -8,7 +8,7 @@
 
 namespace ks {
 kascade_status root_forest_impl(kascade_ctx& ctx, const uint64_t* parent, uint32_t n, uint64_t* root_out,
-                                uint64_t* depth_out, int keep_roots, const Params& p, cudaStream_t s);
+                                uint64_t* depth_out, int keep_roots, const Params& p, cudaStream_t s, bool device_levels = false);
 kascade_status compute_euler_tour_impl(kascade_ctx& ctx, const uint64_t* parent, uint32_t n, uint64_t* tour,
                                        uint64_t* m_out, cudaStream_t s);
 kascade_status gen_list(uint64_t n, uint64_t seed, uint32_t layout, uint64_t* succ, cudaStream_t s);
@@ -394,10 +394,16 @@ KASCADE_API kascade_status kascade_root_forest(kascade_ctx* c, const uint64_t* p
   cudaStream_t s = as_stream(stream);
   if (n && (!parent || !root_out || !depth_out)) return KASCADE_ERR_INVALID_ARG;
   if (n > MAX_FOREST) return KASCADE_ERR_TOO_LARGE;
+  const bool dev = !(opts && opts->async);
   KS_TRY(begin_call(c, s, opts));
   Params p = make_params(*c, opts, 2 * n);
   p.algorithm = KASCADE_ALGO_SPARSE_RULING_SET;
-  kascade_status st = root_forest_impl(*c, parent, (uint32_t)n, root_out, depth_out, 0, p, s);
+  kascade_status st = root_forest_impl(*c, parent, (uint32_t)n, root_out, depth_out, 0, p, s, dev);
+  st = end_call(c, s, st, opts);
+  if (st != KASCADE_ERR_TIMEOUT || !dev) return st;
+  // a tour level outgrew the device-driven recursion: again on the host-driven path
+  KS_TRY(begin_call(c, s, opts));
+  st = root_forest_impl(*c, parent, (uint32_t)n, root_out, depth_out, 0, p, s);
   return end_call(c, s, st, opts);
 }
 

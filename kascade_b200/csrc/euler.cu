@@ -267,7 +267,8 @@ kascade_status sort_children(kascade_ctx& ctx, const uint64_t* parent, uint32_t 
 }  // namespace
 
 kascade_status root_forest_impl(kascade_ctx& ctx, const uint64_t* parent, uint32_t n, uint64_t* root_out,
-                                uint64_t* depth_out, int keep_roots, const Params& p, cudaStream_t s) {
+                                uint64_t* depth_out, int keep_roots, const Params& p, cudaStream_t s,
+                                bool device_levels) {
   if (n == 0) return KASCADE_OK;
   uint32_t *keys, *vals;
   uint2* seg;
@@ -287,9 +288,11 @@ kascade_status root_forest_impl(kascade_ctx& ctx, const uint64_t* parent, uint32
                                                    mix32(p.seed ^ 0x70757254u), slots, ctx.d_status);
     KS_CHECK_LAUNCH();
   }
+  SinkTour sink{root_out, depth_out, n, keep_roots};
+  if (device_levels && m > p.base_max && m < p.level0_log_min && p.max_levels > 0)
+    return rank_records_dev(ctx, rec, m, ctr, dev_cap_next(m, p.spacing0), ruler_elem, sink, p, s);
   uint32_t r = 0;
   KS_TRY(read_u32(ctx, ctr, &r, s));
-  SinkTour sink{root_out, depth_out, n, keep_roots};
   return rank_records(ctx, rec, m, r, ruler_elem, sink, p, s);
 }
 

@@ -1107,6 +1107,8 @@ kascade_status rank_records_dev(kascade_ctx& ctx, Rec* rec, uint32_t n, const ui
 
 template kascade_status rank_records_dev<SinkBatch>(kascade_ctx&, Rec*, uint32_t, const uint32_t*, uint32_t,
                                                     uint32_t*, const SinkBatch&, const Params&, cudaStream_t);
+template kascade_status rank_records_dev<SinkTour>(kascade_ctx&, Rec*, uint32_t, const uint32_t*, uint32_t,
+                                                   uint32_t*, const SinkTour&, const Params&, cudaStream_t);
 template kascade_status rank_records_dev<SinkPlain>(kascade_ctx&, Rec*, uint32_t, const uint32_t*, uint32_t,
                                                     uint32_t*, const SinkPlain&, const Params&, cudaStream_t);
 
