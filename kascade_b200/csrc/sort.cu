@@ -1,6 +1,6 @@
 // Exclusive scan (reduce-then-scan) and LSD radix sort with 8-bit digits.
 //
-// Radix sort, per pass over 4096-key tiles:
+// Radix sort, per pass over 2048-key tiles:
 //   hist    : per-tile digit counts, stored digit-major (count[d][tile])
 //   scan    : one exclusive scan over all counts gives every (digit, tile)
 //             its global output offset
@@ -25,8 +25,8 @@ constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
 
 constexpr int RADIX = 256;
 constexpr int SORT_THREADS = 256;
-constexpr int SORT_ITEMS = 16;
-constexpr int SORT_TILE = SORT_THREADS * SORT_ITEMS;  // 4096
+constexpr int SORT_ITEMS = 8;
+constexpr int SORT_TILE = SORT_THREADS * SORT_ITEMS;  // 2048
 constexpr int SORT_WARPS = SORT_THREADS / 32;
 constexpr int WARP_ITEMS = SORT_TILE / SORT_WARPS;  // 512 consecutive keys per warp
 
