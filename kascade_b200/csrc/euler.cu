@@ -40,6 +40,19 @@ __global__ void __launch_bounds__(256) k_seg_bounds(const uint32_t* __restrict__
   }
 }
 
+// A single forest: the position of each parent's first child goes into the
+// tag word of that parent's up record (slot p), which the tour build then
+// reads and overwrites in one go (one sector, read then written back)
+// instead of reading a separate segment table.
+constexpr uint32_t NO_CHILD = 0xFFFFFFFFu;
+__global__ void __launch_bounds__(256) k_first_child(const uint32_t* __restrict__ keys, uint32_t n,
+                                                     Rec* __restrict__ rec) {
+  for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t k = keys[q];
+    if (q == 0 || keys[q - 1] != k) rec[k].c = (uint32_t)q;
+  }
+}
+
 // Where the records of a forest's tour live.  A single forest of n vertices:
 // up edge of v at slot v, down edge of sorted entry q at slot n + q.  A batch
 // of forests (compacted into one vertex space with per-forest bases fd[j]):
@@ -80,7 +93,7 @@ struct SlotsBatch {
 
 // Writes both tour records of every sorted entry q, samples rulers among the
 // written slots and numbers them (one atomic per tile, as in prepare).
-template <class Slots>
+template <class Slots, bool FIRST_IN_REC>
 __global__ void __launch_bounds__(256) k_tour_build(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
                                                     uint32_t n, const uint2* __restrict__ seg,
                                                     const uint32_t* __restrict__ root_bits, Rec* __restrict__ rec,
@@ -123,9 +136,15 @@ __global__ void __launch_bounds__(256) k_tour_build(const uint32_t* __restrict__
         ru[i].b = succ_up;
         su[i] = slot_up;
         // down edge p -> c: descend to c's first child, else come back up
-        const uint2 sg = seg[c];
+        uint32_t first_child = NO_CHILD;
+        if (FIRST_IN_REC) {
+          first_child = __ldcg(&rec[slot_up].c);  // c's own up slot, rewritten below
+        } else {
+          const uint2 sg = seg[c];
+          if (sg.x < sg.y) first_child = sg.x;
+        }
         rd[i].a = ~0ull;  // -1
-        rd[i].b = (sg.x < sg.y) ? slots.down(sg.x) : slot_up;
+        rd[i].b = (first_child != NO_CHILD) ? slots.down(first_child) : slot_up;
         sd[i] = slot_down;
         // the down edge to a root's first child is the head of that tree's
         // tour: make it a ruler so that no tour element is left unreached
@@ -247,6 +266,7 @@ __global__ void __launch_bounds__(256) k_ref_tour(const uint64_t* __restrict__ p
 
 kascade_status sort_children(kascade_ctx& ctx, const uint64_t* parent, uint32_t n, uint32_t** keys, uint32_t** vals,
                              uint2** seg, uint32_t** root_bits, cudaStream_t s) {
+  // seg == nullptr: no segment table (a single forest keeps first children in its records)
   SortSource src;
   src.parent = parent;
   if (root_bits) {
@@ -255,6 +275,7 @@ kascade_status sort_children(kascade_ctx& ctx, const uint64_t* parent, uint32_t 
     src.root_bits = *root_bits;
   }
   KS_TRY(radix_sort_pairs(ctx, src, n, bits_for(n), keys, vals, s));
+  if (!seg) return KASCADE_OK;
   *seg = alloc<uint2>(ctx, n);
   if (!*seg) return KASCADE_ERR_OOM;
   KS_CUDA(cudaMemsetAsync(*seg, 0, sizeof(uint2) * (size_t)n, s));
@@ -271,9 +292,8 @@ kascade_status root_forest_impl(kascade_ctx& ctx, const uint64_t* parent, uint32
                                 bool device_levels) {
   if (n == 0) return KASCADE_OK;
   uint32_t *keys, *vals;
-  uint2* seg;
   uint32_t* root_bits = nullptr;
-  KS_TRY(sort_children(ctx, parent, n, &keys, &vals, &seg, &root_bits, s));
+  KS_TRY(sort_children(ctx, parent, n, &keys, &vals, nullptr, &root_bits, s));
   const uint32_t m = 2 * n;
   Rec* rec = alloc<Rec>(ctx, m);
   uint32_t* ruler_elem = alloc<uint32_t>(ctx, m);
@@ -281,10 +301,17 @@ kascade_status root_forest_impl(kascade_ctx& ctx, const uint64_t* parent, uint32
   if (!rec || !ruler_elem || !ctr) return KASCADE_ERR_OOM;
   KS_CUDA(cudaMemsetAsync(ctr, 0, sizeof(uint32_t), s));
   {
+    // up slots start with "no child"; every parent then records its first child
+    ProfScope ps(ctx, "seg_bounds", s);
+    KS_CUDA(cudaMemsetAsync(rec, 0xFF, sizeof(Rec) * (size_t)n, s));
+    k_first_child<<<grid_for(ctx, n, 256, 8), 256, 0, s>>>(keys, n, rec);
+    KS_CHECK_LAUNCH();
+  }
+  {
     ProfScope ps(ctx, "tour_build", s);
     const unsigned grid = grid_for(ctx, ((uint64_t)n + 256 * TB_ITEMS - 1) / (256 * TB_ITEMS) * 256, 256, 8);
     SlotsSingle slots{n, (uint32_t)(4294967296.0 / (double)(p.spacing0 < 2 ? 2 : p.spacing0))};
-    k_tour_build<SlotsSingle><<<grid, 256, 0, s>>>(keys, vals, n, seg, root_bits, rec, ruler_elem, ctr,
+    k_tour_build<SlotsSingle, true><<<grid, 256, 0, s>>>(keys, vals, n, nullptr, root_bits, rec, ruler_elem, ctr,
                                                    mix32(p.seed ^ 0x70757254u), slots, ctx.d_status);
     KS_CHECK_LAUNCH();
   }
@@ -310,8 +337,8 @@ kascade_status batch_tours(kascade_ctx& ctx, const uint64_t* fpar, uint32_t F, c
   SlotsBatch slots{fd, foff, fthresh, nf, down_base};
   ProfScope ps(ctx, "tour_build", s);
   const unsigned grid = grid_for(ctx, ((uint64_t)F + 256 * TB_ITEMS - 1) / (256 * TB_ITEMS) * 256, 256, 8);
-  k_tour_build<SlotsBatch><<<grid, 256, 0, s>>>(keys, vals, F, seg, root_bits, rec, ruler_elem, counter, salt, slots,
-                                                ctx.d_status);
+  k_tour_build<SlotsBatch, false><<<grid, 256, 0, s>>>(keys, vals, F, seg, root_bits, rec, ruler_elem, counter, salt,
+                                                        slots, ctx.d_status);
   KS_CHECK_LAUNCH();
   return KASCADE_OK;
 }
