@@ -229,14 +229,17 @@ def calibrate(local: int) -> None:
 
     ctx = kb.Context(local)
     out = {}
-    names = ["independent_read", "independent_read_write", "dependent_read", "dependent_read_write"]
+    names = ["independent_read", "independent_read_write", "dependent_read", "dependent_read_write",
+             "dependent_32B_full_write", "dependent_64B_full_write", "dependent_64B_16B_write", "dependent_32B_read"]
     for mode, nm in enumerate(names):
         for bps in (8, 16):
             v = ctypes.c_double(0)
             kb._lib.check(kb.lib.kascade_calibrate_random_access(ctx.handle, 1 << 28, mode, bps, ctypes.byref(v)),
                           "calibrate", ctx.handle)
             out[f"{nm}@{bps}blk"] = round(v.value, 2)
-    print(json.dumps({"calibration": "G random 16 B record accesses/s, 2^28 records (4 GiB)", **out}), flush=True)
+    print(json.dumps({"calibration": "G random record accesses/s, 2^28 records of 16 B (modes 0-3), 32 B or "
+                                     "64 B (modes 4-7; 16 B of each read, the whole record or 16 B written back)",
+                      **out}), flush=True)
     ctx.close()
 
 

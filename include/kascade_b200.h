@@ -449,7 +449,10 @@ KASCADE_API kascade_status kascade_rank_list_noalloc(const uint64_t* succ, const
  * Measurement.  Random-access calibration: G random 16 B record accesses per
  * second in an array of n_records (far larger than L2).  mode 0: independent
  * reads, 1: independent read + write back, 2: dependent chains (reads),
- * 3: dependent chains with write back.  Diagnostic with no counterpart in the
+ * 3: dependent chains with write back; dependent chains over wider records
+ * (16 B of each read): 4: 32 B records rewritten whole, 5: 64 B records
+ * rewritten whole, 6: 64 B records with 16 B written back, 7: 32 B records,
+ * reads only.  Diagnostic with no counterpart in the
  * reference; it measures the ceiling the ruler chase runs against.
  * ------------------------------------------------------------------------- */
 KASCADE_API kascade_status kascade_calibrate_random_access(kascade_ctx* ctx, uint64_t n_records,
