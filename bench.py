@@ -62,12 +62,21 @@ B_CHASE = 32 + 16
 # propagate: record read (1/2) + the ruler result's random sector (1) + root
 # and rank writes (1/2).  Deeper levels add ~2% and are left out.
 SECTORS_LIST = {True: 0.25 + 0.125 + 0.5 + 2 + 2, False: 0.25 + 0.5 + 2 + 2}
+# The same count for the write-free level 0 (the default from 2^25 elements):
+# prepare as above; chase: the record's random sector read + the 16 B log
+# entry (1 + 1/2); resolve: log read + resolved entry written (1/2 + 1/2; its
+# ruler lookups hit L1 for the most part and are left out); partition: read +
+# write (1/2 + 1/2); place: read (1/2) + root and rank writes (1/2).
+SECTORS_LIST_LOG = {True: 0.25 + 0.125 + 0.5 + 1.5 + 1 + 1 + 1, False: 0.25 + 0.5 + 1.5 + 1 + 1 + 1}
 # DRAM bytes the level-0 chase moves per record it reads, from ncu
 # (dram__bytes_read.sum + dram__bytes_write.sum of the level-0 k_chase launch
 # on a 2^25-element list: 3.924 GB + 1.036 GB over 2^25 + 2 797 812 record
 # reads, every element once plus each chain's closing ruler record; traffic
 # grows in proportion): profiles/chase_propagate_prepare_list25_ncu.md
 CHASE_DRAM_BYTES_PER_VISIT = (3.924e9 + 1.036e9) / (33_554_432 + 2_797_812)
+# The same for the write-free chase (k_chase_log), which reads each record
+# and appends a 16 B log entry: profiles/chase_log_list25_ncu.md
+CHASE_LOG_DRAM_BYTES_PER_VISIT = None
 
 
 def log(*a):
@@ -539,6 +548,7 @@ def main():
     step_kernel_ms = {k: v[0] / args.steps for k, v in ktimes.items()}
     dominant = max(ktimes, key=lambda k: ktimes[k][0]) if ktimes else None
     levels = ctx.levels()
+    write_free = "place" in ktimes  # level 0 ran the write-free chase
 
     hbm, hbm_src = peaks()
     b_alg = B_ALG[kind](weighted)
@@ -557,9 +567,11 @@ def main():
             # levels, divided over the chase launches of one step
             total_units = sum(levels[:-1]) if len(levels) > 1 else units
             per_launch_bytes = B_CHASE * total_units / launches_per_step
-            traffic = CHASE_DRAM_BYTES_PER_VISIT * total_units / launches_per_step
-            bytes_note = (f"{B_CHASE} B per element visited (one random 32 B sector for the 16 B record + 16 B "
-                          f"stamp) x {total_units} elements over {launches_per_step:.0f} chase launches per step")
+            per_visit = CHASE_LOG_DRAM_BYTES_PER_VISIT if write_free else CHASE_DRAM_BYTES_PER_VISIT
+            traffic = per_visit * total_units / launches_per_step if per_visit else None
+            second = "16 B log entry" if write_free else "16 B stamp"
+            bytes_note = (f"{B_CHASE} B per element visited (one random 32 B sector for the 16 B record + {second}) "
+                          f"x {total_units} elements over {launches_per_step:.0f} chase launches per step")
         else:
             per_launch_bytes = n * b_alg / (d_cnt / args.steps)
             traffic = None
@@ -575,10 +587,15 @@ def main():
     pipeline = {"b_alg_per_elem": b_alg, "achieved_gbs": round(pipe_gbs, 1), "frac": round(pipe_gbs / hbm, 4)}
     random_access = None
     if kind == "list":
-        sectors = SECTORS_LIST[bool(weighted)]
+        sectors = (SECTORS_LIST_LOG if write_free else SECTORS_LIST)[bool(weighted)]
         floor_ms = n * 32 * sectors / (hbm * 1e9) * 1000.0
-        random_access = {"sectors_per_element": sectors, "bytes_per_element": 32 * sectors,
+        # the fewer-sector design (stamping level 0) as a conservative floor
+        sectors_min = min(SECTORS_LIST[bool(weighted)], SECTORS_LIST_LOG[bool(weighted)])
+        floor_min_ms = n * 32 * sectors_min / (hbm * 1e9) * 1000.0
+        random_access = {"level0": "write-free" if write_free else "stamping",
+                         "sectors_per_element": sectors, "bytes_per_element": 32 * sectors,
                          "floor_ms": round(floor_ms, 3), "frac": round(floor_ms / ms_per_step, 4),
+                         "sectors_min_design": sectors_min, "frac_min_design": round(floor_min_ms / ms_per_step, 4),
                          "peak_gbs": hbm}
 
     # end-to-end through the host-buffer API (pinned host memory)

@@ -85,8 +85,11 @@ typedef struct kascade_opts {
   uint32_t async;             /* 1: return after enqueueing; see kascade_ctx_sync   */
   uint32_t profile;           /* 1: time each kernel with CUDA events               */
   uint32_t seed;              /* ruler-sampling seed                                */
-  uint32_t level0_mode;       /* 0 auto, 1 stamping chase, 2 write-free chase
-                                 (log + windowed scatter) for the first level      */
+  uint32_t level0_mode;       /* first level: 0 auto (write-free from 2^25
+                                 elements on, where it is faster), 1 stamping
+                                 chase, 2 write-free chase (read-only chase, log,
+                                 radix partition by element, dense placement);
+                                 in-place calls always stamp                      */
   uint32_t max_chain;         /* hop cap of the write-free chase before it hands
                                  level 0 to the stamping chase (0 = 64 x spacing)  */
 } kascade_opts;
@@ -368,7 +371,10 @@ typedef struct kascade_server_config {
                                     batches then run in an SM partition (a green
                                     context) of the other SMs, rounded down to a
                                     multiple of 8; 0 = no partition             */
-  uint32_t reserved2;
+  uint32_t small_reserve_pct;    /* share of the budget (percent, at most 90) that
+                                    only latency-lane requests may fill (default
+                                    10; 0 = none): an overloaded throughput lane
+                                    cannot hold back small requests' admission  */
   uint64_t result_heap_bytes;    /* device memory set aside at creation for
                                     results (default hbm_budget_bytes / 2); a
                                     batch that finds no room there allocates   */

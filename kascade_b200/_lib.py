@@ -41,7 +41,7 @@ class ServerConfig(ctypes.Structure):
     _fields_ = [("struct_size", c_u32), ("device", c_int), ("hbm_budget_bytes", c_u64),
                 ("max_batch_requests", c_u32), ("reserved", c_u32), ("max_batch_elements", c_u64),
                 ("small_max", c_u64), ("small_batch_elements", c_u64), ("latency_sms", c_u32),
-                ("reserved2", c_u32), ("result_heap_bytes", c_u64)]
+                ("small_reserve_pct", c_u32), ("result_heap_bytes", c_u64)]
 
 
 class ServerStats(ctypes.Structure):

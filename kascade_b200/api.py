@@ -628,7 +628,7 @@ class Server:
 
     def __init__(self, device: int = 0, hbm_budget: int = 40 << 30, small_max: int = 1 << 20,
                  small_batch_elements: int = 1 << 23, max_batch_elements: int = 1 << 26,
-                 max_batch_requests: int = 4096, latency_sms: int = 80):
+                 max_batch_requests: int = 4096, latency_sms: int = 80, small_reserve_pct: int = 10):
         cfg = ServerConfig()
         lib.kascade_server_config_init(ctypes.byref(cfg))
         cfg.device = device
@@ -638,6 +638,7 @@ class Server:
         cfg.max_batch_elements = max_batch_elements
         cfg.max_batch_requests = max_batch_requests
         cfg.latency_sms = latency_sms
+        cfg.small_reserve_pct = small_reserve_pct
         h = ctypes.c_void_p()
         check(lib.kascade_server_create(ctypes.byref(cfg), ctypes.byref(h)), "kascade_server_create")
         self.handle = h

@@ -11,20 +11,30 @@
 //             so the log is written with coalesced 16 B stores
 //   recurse   the ruler sub-list (written by the chase in dense id space) is
 //             ranked by the deeper levels
-//   resolve   one pass over the log: rank = rank(ruler) - distance,
-//             root = root(ruler), then partition by element into windows of
-//             2^21 elements (one global atomic per window and log chunk)
-//   scatter   windows are processed in order, so the outputs of about one
-//             window (32 MB) are live in L2 at a time and reach DRAM as full
-//             sectors; a byte flag marks every written element
+//   resolve   first radix pass over the log by element window (2^19
+//             elements), resolving each entry on the way: rank = rank(ruler)
+//             - distance, root = root(ruler).  Tiles of 4 K entries are
+//             sorted by window in shared memory and written as one run per
+//             window; the ruler lookups mostly hit L1 (a log chunk holds the
+//             entries of a few hundred chains)
+//   partition second radix pass: each window into 64 sub-windows of 2^13
+//   place     one sub-window at a time: outputs assembled in shared memory
+//             and written densely, so no output store is random
 //   heads     elements ahead of their list's first ruler were never visited:
-//             they are found by their clear flag and walk forward to the first
-//             flagged element (tours make their heads rulers and skip this)
+//             the place step finds them (no entry in their slot), presets
+//             their root output to a NOT_REACHED sentinel and lists them;
+//             each walks forward to the first element with outputs (tours
+//             make their heads rulers and report an unreached element as a
+//             ruler-free cycle)
+//
+// Calls that must leave roots' outputs untouched (the in-place contract) use
+// the stamping level 0 instead: the sentinel presets would overwrite them.
 //
 // Reference counterparts: the chase of sparse_ruling_set.cpp:147-273 (whose
 // per-element writes are the reference's messages), ruler_propagation.hpp:
 // 148-256 (pull) and post_invert.hpp:195-264 (unreached fix-up).
 #include <algorithm>
+#include <atomic>
 
 #include "ranker.cuh"
 
@@ -33,24 +43,27 @@ namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
 constexpr uint32_t LOG_CHUNK = 1024;  // entries per warp-owned log chunk
-constexpr uint32_t WIN_SHIFT = 19;    // 2^19 elements per output window (8.5 MB of outputs)
+constexpr uint32_t WIN_SHIFT = 19;    // 2^19 elements per window (first partition pass)
 constexpr uint32_t WIN = 1u << WIN_SHIFT;
+constexpr uint32_t SUB_SHIFT = 13;  // 2^13 elements per sub-window (second pass; resolved in shared memory)
+constexpr uint32_t SUB = 1u << SUB_SHIFT;
+constexpr uint32_t SUBS = WIN / SUB;    // sub-windows per window
 constexpr uint32_t MAX_BUCKETS = 8192;  // windows for 2^32 elements
-constexpr uint32_t CURSOR_STRIDE = 8;   // one 32 B sector per window cursor (spreads the atomics)
-constexpr uint32_t FLAG_ONLY = 0xFFFFFFFFu;
-constexpr uint32_t SCATTER_ITEM = 1024;
+constexpr uint32_t CURSOR_STRIDE = 8;   // one 32 B sector per cursor (spreads the atomics)
+constexpr uint32_t PT_THREADS = 256;    // partition: threads per block
+constexpr uint32_t PT_ITEMS = 16;       // partition: entries per thread and tile
+constexpr uint32_t PT_TILE = PT_THREADS * PT_ITEMS;
+constexpr uint32_t PT_TILE_CHUNKS = PT_TILE / LOG_CHUNK;
+constexpr uint32_t FIN_THREADS = 256;  // resolve: threads per block (one sub-window per iteration)
+constexpr uint32_t FIN_GROUP = 8;      // resolve: entries a thread has in flight
+constexpr uint32_t NO_ROOT = 0xFFFFFFFFu;          // shared-memory root slot not written
+constexpr unsigned long long NOT_REACHED = ~0ull;  // root output of an element no chain reached
 
 struct __align__(16) LogEnt {
   uint32_t x;
   uint32_t id;
   uint64_t off;
 };
-struct __align__(16) OutEnt {
-  uint32_t x;
-  uint32_t root;  // FLAG_ONLY: mark reached, leave the outputs untouched
-  uint64_t rank;
-};
-
 __device__ __forceinline__ void st_log(LogEnt* p, uint32_t x, uint32_t id, uint64_t off) {
   __stcs(reinterpret_cast<uint4*>(p), make_uint4(x, id, (uint32_t)off, (uint32_t)(off >> 32)));
 }
@@ -205,160 +218,260 @@ __global__ void __launch_bounds__(512) k_chase_log(const Rec* __restrict__ rec, 
   if (lane == 0 && lend != 0 && lpos != lend) chunk_fill[(lend - 1) / LOG_CHUNK] = LOG_CHUNK - (lend - lpos);
 }
 
-// resolve + partition: one log chunk per block iteration.
-__global__ void __launch_bounds__(256) k_resolve_partition(const LogEnt* __restrict__ log,
-                                                           const uint32_t* __restrict__ chunk_fill, uint32_t nchunks,
-                                                           const Out* __restrict__ out1, uint32_t limit,
-                                                           int keep_roots, uint32_t nb, OutEnt* __restrict__ part,
-                                                           uint32_t* __restrict__ bcursor,
-                                                           unsigned long long* __restrict__ logged, DevStatus* st) {
-  constexpr int PER = LOG_CHUNK / 256;
-  extern __shared__ uint32_t dyn[];
-  uint32_t* bcnt = dyn;        // nb entries
-  uint32_t* bbase = dyn + nb;  // nb entries
-  unsigned long long block_logged = 0;
-  for (uint32_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
-    const uint32_t fill = chunk_fill[ch];
-    if (fill == 0) continue;  // uniform over the block
-    block_logged += fill;
-    for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) bcnt[b] = 0;
-    __syncthreads();
-    OutEnt e[PER];
-    uint32_t bk[PER], loc[PER];
-    bool v[PER];
-    LogEnt le[PER];
+// Exclusive prefix sum of v[0, m) in place (shared memory, m <= MAX_BUCKETS);
+// returns the total to every thread.  Called by all threads of the block.
+__device__ uint32_t block_exclusive_scan(uint32_t* v, uint32_t m) {
+  __shared__ uint32_t warp_sum[PT_THREADS / 32];
+  const uint32_t per = (m + PT_THREADS - 1) / PT_THREADS;
+  const uint32_t lo = min(threadIdx.x * per, m), hi = min(lo + per, m);
+  uint32_t sum = 0;
+  for (uint32_t i = lo; i < hi; ++i) sum += v[i];
+  const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+  uint32_t inc = sum;
 #pragma unroll
-    for (int i = 0; i < PER; ++i) {
-      const uint32_t j = threadIdx.x + i * 256;
-      v[i] = j < fill;
-      if (v[i]) {
-        uint4 raw = __ldcs(reinterpret_cast<const uint4*>(log + (uint64_t)ch * LOG_CHUNK + j));
-        le[i].x = raw.x;
-        le[i].id = raw.y;
-        le[i].off = (uint64_t)raw.z | ((uint64_t)raw.w << 32);
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t t = __shfl_up_sync(FULL, inc, d);
+    if (lane >= (uint32_t)d) inc += t;
+  }
+  if (lane == 31) warp_sum[wid] = inc;
+  __syncthreads();
+  uint32_t before = 0, total = 0;
+  for (uint32_t k = 0; k < PT_THREADS / 32; ++k) {
+    if (k < wid) before += warp_sum[k];
+    total += warp_sum[k];
+  }
+  uint32_t run = before + inc - sum;
+  for (uint32_t i = lo; i < hi; ++i) {
+    const uint32_t c = v[i];
+    v[i] = run;
+    run += c;
+  }
+  __syncthreads();
+  return total;
+}
+
+// Radix partition of 16 B entries by element index.  A block loads a
+// tile of PT_TILE entries into registers, counts them per bucket in shared
+// memory, takes one global cursor step per bucket the tile touches, sorts
+// the tile by bucket in shared memory and writes each bucket's run with
+// consecutive threads: every global store is part of a contiguous run, so
+// L2 sees whole lines instead of one 16 B piece per store.
+//   FROM_LOG (first pass): tiles of PT_TILE_CHUNKS log chunks, buckets are
+//     windows of WIN elements.  Each log entry (element, ruler id, distance)
+//     is resolved on the way: rank = rank(ruler) - distance, root =
+//     root(ruler), from the rulers' results of the recursion.  A log chunk
+//     holds the entries of a few hundred chains, so most of these lookups
+//     hit L1.  Entries of elements at or above `limit` (tour down edges: no
+//     output) are only counted, in `beyond`
+//   otherwise (second pass): tiles inside one window's region, buckets are
+//     its SUBS sub-windows
+// More entries than a bucket holds means some element was logged twice.
+template <bool FROM_LOG>
+__global__ void __launch_bounds__(PT_THREADS, 2) k_partition(const LogEnt* __restrict__ src,
+                                                             const uint32_t* __restrict__ src_info, uint32_t nchunks,
+                                                             const Out* __restrict__ out1, uint32_t limit,
+                                                             uint32_t nb, LogEnt* __restrict__ dst,
+                                                             uint32_t* __restrict__ dcursor,
+                                                             uint32_t* __restrict__ beyond, DevStatus* st) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  uint4* stage = reinterpret_cast<uint4*>(smraw);
+  const uint32_t nbk = FROM_LOG ? nb : SUBS;
+  uint32_t* cnt = reinterpret_cast<uint32_t*>(stage + PT_TILE);  // counts, then the tile's offsets
+  uint32_t* gbase = cnt + nbk;                                   // the tile's start in each bucket
+  __shared__ uint32_t fills[PT_TILE_CHUNKS];
+  __shared__ uint32_t nbeyond;
+  const uint32_t ntiles =
+      FROM_LOG ? (nchunks + PT_TILE_CHUNKS - 1) / PT_TILE_CHUNKS : nb * (WIN / PT_TILE);
+  for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    uint32_t w = 0, valid_end = 0;  // second pass: window and its entry count
+    uint64_t src0;                  // index of the tile's first entry
+    if (FROM_LOG) {
+      src0 = (uint64_t)t * PT_TILE;
+    } else {
+      w = t / (WIN / PT_TILE);
+      const uint32_t k0 = (t % (WIN / PT_TILE)) * PT_TILE;
+      const uint32_t c = min(__ldcg(src_info + (uint64_t)w * CURSOR_STRIDE), WIN);
+      if (k0 >= c) continue;  // block-uniform
+      valid_end = c - k0;
+      src0 = (uint64_t)w * WIN + k0;
+    }
+    for (uint32_t b = threadIdx.x; b < nbk; b += PT_THREADS) cnt[b] = 0;
+    if (FROM_LOG && threadIdx.x < PT_TILE_CHUNKS) {
+      const uint32_t c = t * PT_TILE_CHUNKS + threadIdx.x;
+      fills[threadIdx.x] = c < nchunks ? __ldcg(src_info + c) : 0u;
+    }
+    if (threadIdx.x == 0) nbeyond = 0;
+    __syncthreads();
+    uint4 v[PT_ITEMS];
+    uint32_t pos[PT_ITEMS];
+    uint32_t mine_beyond = 0;
+#pragma unroll
+    for (uint32_t k = 0; k < PT_ITEMS; ++k) {
+      const uint32_t e = k * PT_THREADS + threadIdx.x;
+      const bool valid = FROM_LOG ? (e % LOG_CHUNK) < fills[e / LOG_CHUNK] : e < valid_end;
+      v[k] = valid ? __ldcs(reinterpret_cast<const uint4*>(src + src0 + e)) : make_uint4(NO_ROOT, 0, 0, 0);
+    }
+    if (FROM_LOG) {
+      const uint64_t pol = l2_keep_policy();
+#pragma unroll
+      for (uint32_t k = 0; k < PT_ITEMS; ++k) {
+        if (v[k].x >= limit) continue;
+        const Out o = ld_out_nc_keep(out1 + v[k].y, pol);
+        const uint64_t rank = o.rank - ((uint64_t)v[k].z | ((uint64_t)v[k].w << 32));
+        v[k] = make_uint4(v[k].x, o.root, (uint32_t)rank, (uint32_t)(rank >> 32));
       }
     }
 #pragma unroll
-    for (int i = 0; i < PER; ++i) {
-      if (v[i] && le[i].x >= limit) v[i] = false;  // e.g. tour down edges: no output
-      if (!v[i]) continue;
-      const Out o = ld_out(out1 + le[i].id);
-      e[i].x = le[i].x;
-      e[i].rank = o.rank - le[i].off;
-      e[i].root = (keep_roots && o.root == le[i].x) ? FLAG_ONLY : o.root;
-      bk[i] = le[i].x >> WIN_SHIFT;
-      loc[i] = atomicAdd(&bcnt[bk[i]], 1u);
+    for (uint32_t k = 0; k < PT_ITEMS; ++k) {
+      pos[k] = NO_ROOT;
+      const uint32_t x = v[k].x;
+      if (x < limit) {
+        const uint32_t b = FROM_LOG ? x >> WIN_SHIFT : (x >> SUB_SHIFT) & (SUBS - 1);
+        pos[k] = atomicAdd(&cnt[b], 1u);
+      } else if (FROM_LOG && x != NO_ROOT) {
+        ++mine_beyond;
+      }
+    }
+    if (FROM_LOG && mine_beyond) atomicAdd(&nbeyond, mine_beyond);
+    __syncthreads();
+    for (uint32_t b = threadIdx.x; b < nbk; b += PT_THREADS) {
+      const uint32_t c = cnt[b];
+      const uint64_t ci = FROM_LOG ? (uint64_t)b * CURSOR_STRIDE : ((uint64_t)w * SUBS + b) * CURSOR_STRIDE;
+      gbase[b] = c ? atomicAdd(dcursor + ci, c) : 0u;
+    }
+    if (FROM_LOG && threadIdx.x == 0 && nbeyond) atomicAdd(beyond, nbeyond);
+    const uint32_t total = block_exclusive_scan(cnt, nbk);  // cnt now holds the tile's offsets
+#pragma unroll
+    for (uint32_t k = 0; k < PT_ITEMS; ++k) {
+      if (pos[k] == NO_ROOT) continue;
+      const uint32_t x = v[k].x;
+      const uint32_t b = FROM_LOG ? x >> WIN_SHIFT : (x >> SUB_SHIFT) & (SUBS - 1);
+      stage[cnt[b] + pos[k]] = v[k];
     }
     __syncthreads();
-    for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x)
-      if (bcnt[b]) bbase[b] = atomicAdd(bcursor + (uint64_t)b * CURSOR_STRIDE, bcnt[b]);
-    __syncthreads();
-#pragma unroll
-    for (int i = 0; i < PER; ++i) {
-      if (!v[i]) continue;
-      const uint32_t pos = bbase[bk[i]] + loc[i];
-      if (pos >= WIN) {
-        set_error(st, KASCADE_ERR_NOT_A_LIST, e[i].x);  // an element logged twice
+    for (uint32_t i = threadIdx.x; i < total; i += PT_THREADS) {
+      const uint4 e = stage[i];
+      const uint32_t b = FROM_LOG ? e.x >> WIN_SHIFT : (e.x >> SUB_SHIFT) & (SUBS - 1);
+      const uint32_t p = gbase[b] + (i - cnt[b]);
+      const uint32_t cap = FROM_LOG ? WIN : SUB;
+      if (p >= cap) {
+        set_error(st, KASCADE_ERR_NOT_A_LIST, e.x);  // an element logged twice
         continue;
       }
-      OutEnt* dst = part + (uint64_t)bk[i] * WIN + pos;
-      *reinterpret_cast<uint4*>(dst) = make_uint4(e[i].x, e[i].root, (uint32_t)e[i].rank, (uint32_t)(e[i].rank >> 32));
+      const uint64_t d = FROM_LOG ? (uint64_t)b * WIN + p : (uint64_t)w * WIN + (uint64_t)b * SUB + p;
+      __stcg(reinterpret_cast<uint4*>(dst + d), e);
     }
     __syncthreads();
   }
-  if (threadIdx.x == 0 && block_logged) atomicAdd(logged, block_logged);
 }
 
-// Windowed scatter: work items are handed out in window order.
-__global__ void __launch_bounds__(256) k_scatter(const OutEnt* __restrict__ part, const uint32_t* __restrict__ bcursor,
-                                                 uint32_t nb, uint32_t* __restrict__ work, uint64_t* __restrict__ root_out,
-                                                 uint64_t* __restrict__ rank_out, uint8_t* __restrict__ flags) {
-  __shared__ uint32_t item;
-  constexpr uint32_t IPB = WIN / SCATTER_ITEM;
-  const uint32_t total = nb * IPB;
-  while (true) {
-    if (threadIdx.x == 0) item = atomicAdd(work, 1u);
-    __syncthreads();
-    const uint32_t it = item;
-    __syncthreads();
-    if (it >= total) break;
-    const uint32_t b = it / IPB, k = it % IPB;
-    const uint32_t cnt = min(bcursor[(uint64_t)b * CURSOR_STRIDE], WIN);  // beyond WIN only on invalid input
-    const uint32_t beg = k * SCATTER_ITEM;
-    if (beg >= cnt) continue;
-    const uint32_t stop = min(beg + SCATTER_ITEM, cnt);
-    const OutEnt* src = part + (uint64_t)b * WIN;
-    for (uint32_t j = beg + threadIdx.x; j < stop; j += 256) {
-      const uint4 raw = __ldcs(reinterpret_cast<const uint4*>(src + j));
-      const uint32_t x = raw.x;
-      if (raw.y != FLAG_ONLY) {
-        root_out[x] = raw.y;
-        rank_out[x] = (uint64_t)raw.z | ((uint64_t)raw.w << 32);
-      }
-      if (flags) flags[x] = 1;
-    }
-  }
-}
-
-// Elements never visited (ahead of their list's first ruler).
-__global__ void __launch_bounds__(256) k_find_unreached(const uint8_t* __restrict__ flags, uint32_t n,
-                                                        uint32_t* __restrict__ ulist, uint32_t* __restrict__ ucount,
-                                                        uint32_t ucap, DevStatus* st) {
+// Place: one sub-window (SUB elements) per block iteration.  Its entries
+// (element, root, rank) are read in order and placed in shared memory by
+// element, then the sub-window's outputs are written densely.  Elements without an entry were reached by no chain: their root
+// output becomes NOT_REACHED and they join the unreached list (or, when
+// every list head is a ruler, they lie on a ruler-free cycle).
+__global__ void __launch_bounds__(FIN_THREADS, 2) k_place(const LogEnt* __restrict__ part2,
+                                                            const uint32_t* __restrict__ cursor2, uint32_t nb,
+                                                            uint32_t limit, uint32_t n,
+                                                            const uint32_t* __restrict__ beyond, int heads_are_rulers,
+                                                            uint64_t* __restrict__ root_out,
+                                                            uint64_t* __restrict__ rank_out, uint32_t* __restrict__ ulist,
+                                                            uint32_t* __restrict__ ucount, uint32_t ucap,
+                                                            DevStatus* st) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  unsigned long long* rank_s = reinterpret_cast<unsigned long long*>(smraw);  // SUB entries
+  uint32_t* root_s = reinterpret_cast<uint32_t*>(rank_s + SUB);               // SUB entries
   const uint32_t lane = threadIdx.x & 31u;
-  const uint64_t groups = ((uint64_t)n + 15) / 16;
-  for (uint64_t g0 = (uint64_t)blockIdx.x * blockDim.x; g0 < groups; g0 += (uint64_t)gridDim.x * blockDim.x) {
-    const uint64_t g = g0 + threadIdx.x;
-    uint32_t zero_mask = 0;
-    if (g < groups) {
-      uint4 v = __ldcs(reinterpret_cast<const uint4*>(flags) + g);
-      const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+  if (blockIdx.x == 0 && threadIdx.x == 0 && heads_are_rulers) {
+    const uint32_t want = n - limit;
+    if (*beyond > want) set_error(st, KASCADE_ERR_NOT_A_LIST, *beyond);
+    if (*beyond < want) set_error(st, KASCADE_ERR_CYCLE, *beyond);
+  }
+  const uint32_t items = nb * SUBS;
+  for (uint32_t it = blockIdx.x; it < items; it += gridDim.x) {
+    const uint32_t lo = it * SUB;  // == window * WIN + sub-window * SUB
+    if (lo >= limit) continue;     // block-uniform
+    const uint32_t len = min(SUB, limit - lo);
+    const uint32_t cnt = min(__ldcg(cursor2 + (uint64_t)it * CURSOR_STRIDE), SUB);
+    for (uint32_t i = threadIdx.x; i < SUB; i += FIN_THREADS) root_s[i] = NO_ROOT;
+    __syncthreads();
+    const LogEnt* src = part2 + (uint64_t)it * SUB;
+    for (uint32_t g = 0; g < SUB / FIN_THREADS; g += FIN_GROUP) {
+      uint4 e[FIN_GROUP];
 #pragma unroll
-      for (int k = 0; k < 16; ++k) {
-        const uint32_t byte = (w[k >> 2] >> (8 * (k & 3))) & 0xFFu;
-        if (byte == 0 && g * 16 + k < n) zero_mask |= 1u << k;
+      for (uint32_t j = 0; j < FIN_GROUP; ++j) {
+        const uint32_t i = (g + j) * FIN_THREADS + threadIdx.x;
+        e[j] = i < cnt ? __ldcs(reinterpret_cast<const uint4*>(src + i)) : make_uint4(NO_ROOT, 0, 0, 0);
+      }
+#pragma unroll
+      for (uint32_t j = 0; j < FIN_GROUP; ++j) {
+        if (e[j].x == NO_ROOT) continue;
+        const uint32_t xl = e[j].x - lo;
+        if (xl >= len) {  // not this sub-window's: the partition passes wrote nothing like it
+          set_error(st, KASCADE_ERR_NOT_A_LIST, e[j].x);
+          continue;
+        }
+        if (atomicExch(&root_s[xl], e[j].y) != NO_ROOT) set_error(st, KASCADE_ERR_NOT_A_LIST, e[j].x);
+        rank_s[xl] = (uint64_t)e[j].z | ((uint64_t)e[j].w << 32);
       }
     }
-    uint32_t cnt = __popc(zero_mask);
-    // warp-level exclusive scan of counts, one atomic per warp
-    uint32_t incl = cnt;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      uint32_t y = __shfl_up_sync(FULL, incl, o);
-      if (lane >= (uint32_t)o) incl += y;
+    __syncthreads();
+    for (uint32_t i0 = 0; i0 < len; i0 += FIN_THREADS) {
+      const uint32_t i = i0 + threadIdx.x;
+      bool un = false;
+      if (i < len) {
+        const uint32_t r = root_s[i];
+        un = r == NO_ROOT;
+        __stcs(reinterpret_cast<unsigned long long*>(root_out) + lo + i, un ? NOT_REACHED : (unsigned long long)r);
+        __stcs(reinterpret_cast<unsigned long long*>(rank_out) + lo + i, un ? 0ull : rank_s[i]);
+      }
+      const uint32_t m = __ballot_sync(FULL, un);
+      if (m == 0u) continue;
+      if (heads_are_rulers) {
+        if (un) set_error(st, KASCADE_ERR_CYCLE, lo + i);
+        continue;
+      }
+      uint32_t base = 0;
+      if (lane == 0) base = atomicAdd(ucount, (uint32_t)__popc(m));
+      base = __shfl_sync(FULL, base, 0);
+      if (un) {
+        const uint32_t p = base + __popc(m & lanemask_lt());
+        if (p < ucap)
+          ulist[p] = lo + i;
+        else
+          set_error(st, KASCADE_ERR_TOO_LARGE, p);
+      }
     }
-    const uint32_t wtotal = __shfl_sync(FULL, incl, 31);
-    uint32_t base = 0;
-    if (lane == 31 && wtotal) base = atomicAdd(ucount, wtotal);
-    base = __shfl_sync(FULL, base, 31);
-    uint32_t pos = base + incl - cnt;
-    while (zero_mask) {
-      const int k = __ffs(zero_mask) - 1;
-      zero_mask &= zero_mask - 1;
-      if (pos < ucap)
-        ulist[pos] = (uint32_t)(g * 16 + k);
-      else
-        set_error(st, KASCADE_ERR_TOO_LARGE, pos);
-      pos++;
-    }
+    __syncthreads();
   }
 }
 
-__global__ void __launch_bounds__(256) k_walk_unreached(const Rec* __restrict__ rec, const uint8_t* __restrict__ flags,
-                                                        const uint32_t* __restrict__ ulist,
+// Each unreached element walks forward to the first element with outputs:
+// one the resolve wrote (root output not NOT_REACHED) or one another walker
+// finished.  Walkers write the rank, fence, then the root, and readers load
+// the root, fence, then the rank, so a root seen set comes with its rank.
+// Plain lists only (every element has outputs).
+__global__ void __launch_bounds__(256) k_walk_unreached(const Rec* __restrict__ rec, const uint32_t* __restrict__ ulist,
                                                         const uint32_t* __restrict__ ucount, uint32_t ucap, uint32_t n,
-                                                        uint64_t* __restrict__ root_out, uint64_t* __restrict__ rank_out,
-                                                        DevStatus* st) {
+                                                        uint64_t* root_out, uint64_t* rank_out, DevStatus* st) {
   const uint32_t cnt = min(*ucount, ucap);
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
     const uint32_t u = ulist[i];
     uint64_t acc = 0;
     uint32_t y = u, mark = u, power = 1, lam = 0, hops = 0;
+    unsigned long long base_root = NOT_REACHED;
     bool ok = true;
     while (true) {
       const Rec r = ld_rec_cg(rec + y);
       acc += r.a;
       y = r.b;
-      if (flags[y]) break;
+      if (y >= n) {  // not reachable for a validated input; keeps every load in range
+        set_error(st, KASCADE_ERR_OUT_OF_RANGE, u);
+        ok = false;
+        break;
+      }
+      base_root = __ldcg(reinterpret_cast<const unsigned long long*>(root_out) + y);
+      if (base_root != NOT_REACHED) break;
       if (y == mark || ++hops > n) {
         set_error(st, KASCADE_ERR_CYCLE, u);
         ok = false;
@@ -371,18 +484,11 @@ __global__ void __launch_bounds__(256) k_walk_unreached(const Rec* __restrict__ 
       }
     }
     if (!ok) continue;
-    const Rec ry = ld_rec_cg(rec + y);
-    uint64_t base_rank;
-    uint64_t base_root;
-    if (ry.b == y) {  // a root: rank 0 whatever its output slot holds
-      base_rank = 0;
-      base_root = y;
-    } else {
-      base_rank = rank_out[y];
-      base_root = root_out[y];
-    }
-    root_out[u] = base_root;
+    __threadfence();
+    const unsigned long long base_rank = __ldcg(reinterpret_cast<const unsigned long long*>(rank_out) + y);
     rank_out[u] = acc + base_rank;
+    __threadfence();
+    root_out[u] = base_root;
   }
 }
 
@@ -432,18 +538,16 @@ kascade_status rank_level0_log(kascade_ctx& ctx, const Rec* rec, uint32_t n, uin
   const uint32_t nchunks = (uint32_t)(((uint64_t)n + LOG_CHUNK - 1) / LOG_CHUNK + warps + 1);
   LogEnt* log = alloc<LogEnt>(ctx, (uint64_t)nchunks * LOG_CHUNK);
   uint32_t* chunk_fill = alloc<uint32_t>(ctx, nchunks);
-  uint32_t* counters = alloc<uint32_t>(ctx, 8);  // chunk cursor, chase work, scatter work, unreached count
-  unsigned long long* logged = alloc<unsigned long long>(ctx, 1);
+  uint32_t* counters = alloc<uint32_t>(ctx, 8);  // chunk cursor, chase work, unreached count, beyond
   Rec* rec1 = alloc<Rec>(ctx, r0);
   Out* out1 = alloc<Out>(ctx, r0);
-  if (!log || !chunk_fill || !counters || !logged || !rec1 || !out1) return KASCADE_ERR_OOM;
+  if (!log || !chunk_fill || !counters || !rec1 || !out1) return KASCADE_ERR_OOM;
   KS_CUDA(cudaMemsetAsync(chunk_fill, 0, sizeof(uint32_t) * nchunks, s));
   KS_CUDA(cudaMemsetAsync(counters, 0, sizeof(uint32_t) * 8, s));
-  KS_CUDA(cudaMemsetAsync(logged, 0, sizeof(unsigned long long), s));
   uint32_t* chunk_cursor = counters + 0;
   uint32_t* chase_work = counters + 1;
-  uint32_t* scatter_work = counters + 2;
-  uint32_t* ucount = counters + 3;
+  uint32_t* ucount = counters + 2;
+  uint32_t* beyond = counters + 3;
   const uint64_t cap = p.max_chain ? p.max_chain : 64ull * p.spacing0 + 1024;
   const uint32_t max_hops = cap < n ? (uint32_t)cap : n;
   switch (C) {
@@ -470,53 +574,64 @@ kascade_status rank_level0_log(kascade_ctx& ctx, const Rec* rec, uint32_t n, uin
 
   const uint32_t limit = t.limit < n ? t.limit : n;
   const uint32_t nb = (uint32_t)(((uint64_t)limit + WIN - 1) / WIN);
-  OutEnt* part = alloc<OutEnt>(ctx, (uint64_t)(nb ? nb : 1) * WIN);
-  uint32_t* bcursor = alloc<uint32_t>(ctx, (uint64_t)(nb ? nb : 1) * CURSOR_STRIDE);
-  if (!part || !bcursor) return KASCADE_ERR_OOM;
-  KS_CUDA(cudaMemsetAsync(bcursor, 0, sizeof(uint32_t) * (nb ? nb : 1) * CURSOR_STRIDE, s));
+  const uint32_t nb1 = nb ? nb : 1;
+  // first pass: log -> windows (part); second pass: windows -> sub-windows,
+  // into the log's memory when it is large enough (the log is dead by then)
+  const uint64_t part2_need = (((uint64_t)limit + SUB - 1) / SUB) * SUB;
+  LogEnt* part = alloc<LogEnt>(ctx, (uint64_t)nb1 * WIN);
+  LogEnt* part2 = (uint64_t)nchunks * LOG_CHUNK >= part2_need ? log : alloc<LogEnt>(ctx, part2_need ? part2_need : 1);
+  uint32_t* cursor = alloc<uint32_t>(ctx, (uint64_t)nb1 * (SUBS + 1) * CURSOR_STRIDE);
+  if (!part || !part2 || !cursor) return KASCADE_ERR_OOM;
+  uint32_t* cursor1 = cursor;
+  uint32_t* cursor2 = cursor + (uint64_t)nb1 * CURSOR_STRIDE;
+  KS_CUDA(cudaMemsetAsync(cursor, 0, sizeof(uint32_t) * nb1 * (SUBS + 1) * CURSOR_STRIDE, s));
+  const size_t smem1 = PT_TILE * sizeof(LogEnt) + 2 * sizeof(uint32_t) * nb1;
+  const size_t smem2 = PT_TILE * sizeof(LogEnt) + 2 * sizeof(uint32_t) * SUBS;
+  {
+    // kernel attributes are per device: raise the shared-memory limits once on each
+    static std::atomic<uint64_t> raised{0};
+    int dev = 0;
+    KS_CUDA(cudaGetDevice(&dev));
+    const uint64_t bit = 1ull << (dev & 63);
+    if (!(raised.load() & bit)) {
+      KS_CUDA(cudaFuncSetAttribute(k_partition<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)(PT_TILE * sizeof(LogEnt) + 2 * sizeof(uint32_t) * MAX_BUCKETS)));
+      KS_CUDA(cudaFuncSetAttribute(k_partition<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
+      KS_CUDA(cudaFuncSetAttribute(k_place, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)(SUB * (sizeof(unsigned long long) + sizeof(uint32_t)))));
+      raised.fetch_or(bit);
+    }
+  }
+  const uint64_t resident = (uint64_t)ctx.usable_sms() * 2;
   {
     ProfScope ps(ctx, "resolve", s);
-    const unsigned g = (unsigned)std::min<uint64_t>(nchunks, (uint64_t)ctx.usable_sms() * 8);
-    const size_t smem = 2 * sizeof(uint32_t) * (nb ? nb : 1);
-    if (smem > 48 * 1024) {
-      static bool raised = false;
-      if (!raised) {
-        KS_CUDA(cudaFuncSetAttribute(k_resolve_partition, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)(2 * sizeof(uint32_t) * MAX_BUCKETS)));
-        raised = true;
-      }
-    }
-    k_resolve_partition<<<g, 256, smem, s>>>(log, chunk_fill, nchunks, out1, limit, t.keep_roots, nb, part, bcursor,
-                                             logged, ctx.d_status);
+    const uint32_t tiles1 = (nchunks + PT_TILE_CHUNKS - 1) / PT_TILE_CHUNKS;
+    k_partition<true><<<(unsigned)std::min<uint64_t>(tiles1, resident), PT_THREADS, smem1, s>>>(
+        log, chunk_fill, nchunks, out1, limit, nb, part, cursor1, beyond, ctx.d_status);
     KS_CHECK_LAUNCH();
   }
-  uint32_t lg[2] = {0, 0};
-  KS_TRY(read_u32(ctx, reinterpret_cast<const uint32_t*>(logged), &lg[0], s));
-  KS_TRY(read_u32(ctx, reinterpret_cast<const uint32_t*>(logged) + 1, &lg[1], s));
-  const uint64_t total_logged = (uint64_t)lg[0] | ((uint64_t)lg[1] << 32);
-  if (total_logged > n) return KASCADE_ERR_NOT_A_LIST;
-  const bool need_heads = total_logged < n;
-  if (need_heads && t.heads_are_rulers) return KASCADE_ERR_CYCLE;  // a tour element no ruler reaches
-  uint8_t* flags = nullptr;
-  if (need_heads) {
-    flags = alloc<uint8_t>(ctx, (uint64_t)n + 16);
-    if (!flags) return KASCADE_ERR_OOM;
-    KS_CUDA(cudaMemsetAsync(flags, 0, (size_t)n + 16, s));
+  const uint32_t tiles2 = nb * (WIN / PT_TILE);
+  if (tiles2) {
+    ProfScope ps(ctx, "partition", s);
+    k_partition<false><<<(unsigned)std::min<uint64_t>(tiles2, resident), PT_THREADS, smem2, s>>>(
+        part, cursor1, 0, nullptr, limit, nb, part2, cursor2, beyond, ctx.d_status);
+    KS_CHECK_LAUNCH();
   }
+  // the first pass's output is dead after the second: it holds the unreached list
+  uint32_t* ulist = reinterpret_cast<uint32_t*>(part);
+  const uint32_t ucap = limit;
   {
-    ProfScope ps(ctx, "scatter", s);
-    k_scatter<<<ctx.usable_sms() * 8, 256, 0, s>>>(part, bcursor, nb, scatter_work, t.root, t.rank, flags);
+    ProfScope ps(ctx, "place", s);
+    const uint32_t items = nb * SUBS;
+    const size_t smem = SUB * (sizeof(unsigned long long) + sizeof(uint32_t));
+    k_place<<<(unsigned)std::max<uint64_t>(1, std::min<uint64_t>(items, (uint64_t)ctx.usable_sms() * 2)),
+                FIN_THREADS, smem, s>>>(part2, cursor2, nb, limit, n, beyond, t.heads_are_rulers, t.root, t.rank,
+                                        ulist, ucount, ucap, ctx.d_status);
     KS_CHECK_LAUNCH();
   }
-  if (need_heads) {
-    // the log is dead after resolve: reuse it for the list of unreached elements
-    uint32_t* ulist = reinterpret_cast<uint32_t*>(log);
-    const uint32_t ucap = n;
+  if (!t.heads_are_rulers) {
     ProfScope ps(ctx, "heads", s);
-    const uint64_t groups = ((uint64_t)n + 15) / 16;
-    k_find_unreached<<<grid_for(ctx, groups, 256, 8), 256, 0, s>>>(flags, n, ulist, ucount, ucap, ctx.d_status);
-    KS_CHECK_LAUNCH();
-    k_walk_unreached<<<ctx.usable_sms() * 4, 256, 0, s>>>(rec, flags, ulist, ucount, ucap, n, t.root, t.rank,
+    k_walk_unreached<<<ctx.usable_sms() * 4, 256, 0, s>>>(rec, ulist, ucount, ucap, n, t.root, t.rank,
                                                       ctx.d_status);
     KS_CHECK_LAUNCH();
   }

@@ -127,6 +127,19 @@ __device__ __forceinline__ uint64_t l2_keep_policy() {
   asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
   return pol;
 }
+// Through the read-only (L1) path with the same L2 hint: for lookups whose
+// neighbours in a warp's stream tend to repeat (log entries of one chain).
+__device__ __forceinline__ Out ld_out_nc_keep(const Out* p, uint64_t pol) {
+  uint32_t a, b, c, d;
+  asm volatile("ld.global.nc.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
+               : "=r"(a), "=r"(b), "=r"(c), "=r"(d)
+               : "l"(p), "l"(pol));
+  Out o;
+  o.rank = (uint64_t)a | ((uint64_t)b << 32);
+  o.root = c;
+  o.pad = d;
+  return o;
+}
 __device__ __forceinline__ Out ld_out_keep(const Out* p, uint64_t pol) {
   uint32_t a, b, c, d;
   asm volatile("ld.global.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"

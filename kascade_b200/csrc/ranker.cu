@@ -963,7 +963,7 @@ kascade_status rank_records(kascade_ctx& ctx, Rec* rec, uint32_t n, uint32_t r0,
   if (n <= p.base_max) return launch_base(ctx, rec, n, nullptr, sink, s);
   if (p.algorithm != KASCADE_ALGO_SPARSE_RULING_SET || p.max_levels == 0 || (uint64_t)r0 * 10 > (uint64_t)n * 7)
     return pointer_double_records(ctx, rec, n, nullptr, sink, s);
-  if (Sink::kWriteFree && n >= p.level0_log_min) {
+  if (Sink::kWriteFree && n >= p.level0_log_min && !sink.log_target(n).keep_roots) {
     const kascade_status st = rank_level0_log(ctx, rec, n, r0, ruler_elem0, sink.log_target(n), p, s);
     if (st != KASCADE_ERR_TIMEOUT) return st;
     // a chain exceeded the write-free path's hop cap (invalid input, or an

@@ -28,7 +28,7 @@ struct Params {
   uint32_t block = 256;
   uint32_t seed = 0x6b617363u;
   uint32_t algorithm = KASCADE_ALGO_SPARSE_RULING_SET;
-  uint32_t level0_log_min = 0xFFFFFFFFu;  // level 0 uses the write-free path from this size on (opt-in)
+  uint32_t level0_log_min = 1u << 25;  // level 0 uses the write-free path from this size on
   uint32_t max_chain = 0;              // write-free chase hop cap (0: 64 x spacing0 + 1024)
 };
 

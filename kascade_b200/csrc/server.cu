@@ -44,6 +44,14 @@
 
 #include "ctx.cuh"
 
+namespace ks {
+// capi.cu: a batch call on the host-driven recursion
+kascade_status rank_batch_host_levels_call(kascade_ctx* c, const kascade_segment* segs, uint32_t nseg,
+                                           const uint64_t* in, const uint32_t* weights, uint64_t total,
+                                           uint64_t* root_out, uint64_t* rank_out, const kascade_opts* opts,
+                                           cudaStream_t s);
+}  // namespace ks
+
 namespace {
 
 using Clock = std::chrono::steady_clock;
@@ -354,6 +362,8 @@ kascade_status kascade_server::warm_lane(kascade_ctx* ctx, cudaStream_t stream, 
 // yet.  Admission is accounting only; the lane copies the input when it runs.
 void kascade_server::admit_locked() {
   bool blocked_large = false;
+  // large requests stop short of the share kept for the latency lane
+  const uint64_t reserve = cfg.hbm_budget_bytes / 100 * std::min<uint32_t>(cfg.small_reserve_pct, 90);
   for (auto it = waiting.begin(); it != waiting.end();) {
     Request* r = *it;
     const bool small = r->n <= cfg.small_max;
@@ -361,7 +371,8 @@ void kascade_server::admit_locked() {
       ++it;
       continue;
     }
-    if (bytes_in_use + r->footprint > cfg.hbm_budget_bytes && bytes_in_use > 0) {
+    const uint64_t limit = small ? cfg.hbm_budget_bytes : cfg.hbm_budget_bytes - reserve;
+    if (bytes_in_use + r->footprint > limit && bytes_in_use > 0) {
       if (!small) blocked_large = true;
       ++it;
       continue;
@@ -525,8 +536,18 @@ void kascade_server::lane_loop(int lane) {
       kascade_opts o;
       kascade_opts_init(&o);
       o.profile = tracing ? 1 : 0;
-      st = kascade_rank_batch(C, segs.data(), (uint32_t)segs.size(), d_in, any_w ? d_w : nullptr, elems,
-                              b->d_root, b->d_rank, &o, S);
+      // The latency lane enqueues its whole recursion at once (one host wait).
+      // The throughput lane takes the host-driven recursion: its persistent
+      // kernels hold their SMs until they end, and a batch enqueued whole at
+      // full width would keep them from the latency lane for the batch's
+      // whole duration; level by level, each launch takes the SM budget in
+      // force when it is made.
+      if (lane == 0)
+        st = kascade_rank_batch(C, segs.data(), (uint32_t)segs.size(), d_in, any_w ? d_w : nullptr, elems,
+                                b->d_root, b->d_rank, &o, S);
+      else
+        st = ks::rank_batch_host_levels_call(C, segs.data(), (uint32_t)segs.size(), d_in, any_w ? d_w : nullptr,
+                                             elems, b->d_root, b->d_rank, &o, S);
     }
     // the staged input is free for the next batch once the stream is done;
     // host submissions drop their copies then too
@@ -604,6 +625,7 @@ KASCADE_API void kascade_server_config_init(kascade_server_config* c) {
   c->small_max = 1ull << 20;
   c->small_batch_elements = 1ull << 23;
   c->latency_sms = 80;
+  c->small_reserve_pct = 10;
   c->result_heap_bytes = 0;
 }
 

@@ -87,8 +87,28 @@ def test_write_free_above_2_22(kb, oracle_mod, layout):
     np.testing.assert_array_equal(host_u64(root), root_o)
     np.testing.assert_array_equal(host_u64(rank), rank_o)
     times = ctx.kernel_times()
-    assert "resolve" in times and "scatter" in times
+    assert "resolve" in times and "partition" in times and "place" in times
     ctx.close()
+
+
+def test_write_free_many_lists_several_windows(kb, oracle_mod):
+    """The write-free level 0 on 30 000 lists over several 2^19-element
+    windows: thousands of list heads ahead of their first ruler, spread over
+    many sub-windows, walk to their first reached element."""
+    rng = np.random.default_rng(0xE1)
+    n = 3 * (1 << 19) + 777
+    order = rng.permutation(n).astype(np.uint64)
+    cuts = np.sort(rng.choice(np.arange(1, n), size=30_000 - 1, replace=False))
+    succ_h = np.empty(n, np.uint64)
+    for seg in np.split(order, cuts):
+        succ_h[seg[:-1]] = seg[1:]
+        succ_h[seg[-1]] = seg[-1]
+    w_h = rng.integers(0, 1 << 16, n).astype(np.uint32)
+    root_o, rank_o = oracle_mod.rank_list(succ_h, w_h)
+    for tuning in (dict(level0_mode=2), dict(level0_mode=2, ruler_spacing=200)):
+        root, rank = kb.rank_list(dev64(succ_h), dev32(w_h), tuning=kb.GpuTuning(**tuning))
+        np.testing.assert_array_equal(host_u64(root), root_o)
+        np.testing.assert_array_equal(host_u64(rank), rank_o)
 
 
 @pytest.mark.parametrize("offset", [(0, 0), (1, 0), (0, 1), (1, 3)])
