@@ -468,6 +468,7 @@ def main():
     ap.add_argument("--no-secondary", action="store_true")
     ap.add_argument("--spacing", type=int, default=0)
     ap.add_argument("--chains", type=int, default=0)
+    ap.add_argument("--block", type=int, default=0, help="chase block size override (128, 256 or 512)")
     ap.add_argument("--n", type=int, default=0, help="override the workload size (profiling runs)")
     ap.add_argument("--level0-mode", type=int, default=0, help="0 auto, 1 stamping chase, 2 write-free chase")
     ap.add_argument("--calibrate", action="store_true",
@@ -501,6 +502,7 @@ def main():
     stream = torch.cuda.current_stream(dev)
     seed = 0xC1 + 1000 * rank
     tuning = kb.GpuTuning(profile=True, ruler_spacing=args.spacing, chains_per_thread=args.chains,
+                          block_size=args.block,
                           level0_mode=args.level0_mode)
     if kind == "list":
         inp = kb.gen_list(n, seed, arg, device=dev)
@@ -609,7 +611,7 @@ def main():
             pin_w.copy_(w.cpu())
         pin_root = torch.empty(n, dtype=torch.int64, pin_memory=True)
         pin_rank = torch.empty(n, dtype=torch.int64, pin_memory=True)
-        o = kb.GpuTuning(ruler_spacing=args.spacing, chains_per_thread=args.chains,
+        o = kb.GpuTuning(ruler_spacing=args.spacing, chains_per_thread=args.chains, block_size=args.block,
                          level0_mode=args.level0_mode).to_opts()
         import ctypes
 
@@ -624,7 +626,10 @@ def main():
                                                      pin_rank.data_ptr(), ctypes.byref(o), stream.cuda_stream)
             kb._lib.check(st, "host-buffer call", ctx.handle)
 
-        e2e_step()
+        # two warm-up calls: the first grows the context's arena by the device
+        # copies of the host buffers, the second folds it into one block
+        for _ in range(2):
+            e2e_step()
         barrier(world)
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
@@ -645,7 +650,8 @@ def main():
     if not args.no_secondary and kind == "list" and args.workload == "list" and world == 1:
         # the locality-biased layout of the same configuration
         inp2 = kb.gen_list(n, seed, 1, device=dev)
-        tun2 = kb.GpuTuning(ruler_spacing=args.spacing, chains_per_thread=args.chains, level0_mode=args.level0_mode)
+        tun2 = kb.GpuTuning(ruler_spacing=args.spacing, chains_per_thread=args.chains, block_size=args.block,
+                            level0_mode=args.level0_mode)
         for _ in range(2):
             kb.rank_list(inp2, w, tuning=tun2, root_out=root, rank_out=rk, ctx=ctx)
         torch.cuda.synchronize()

@@ -11,13 +11,13 @@
 //             so the log is written with coalesced 16 B stores
 //   recurse   the ruler sub-list (written by the chase in dense id space) is
 //             ranked by the deeper levels
-//   resolve   first radix pass over the log by element window (2^19
+//   resolve   first radix pass over the log by element window (2^20
 //             elements), resolving each entry on the way: rank = rank(ruler)
-//             - distance, root = root(ruler).  Tiles of 4 K entries are
+//             - distance, root = root(ruler).  Tiles of 2 K entries are
 //             sorted by window in shared memory and written as one run per
 //             window; the ruler lookups mostly hit L1 (a log chunk holds the
 //             entries of a few hundred chains)
-//   partition second radix pass: each window into 64 sub-windows of 2^13
+//   partition second radix pass: each window into 128 sub-windows of 2^13
 //   place     one sub-window at a time: outputs assembled in shared memory
 //             and written densely, so no output store is random
 //   heads     elements ahead of their list's first ruler were never visited:
@@ -43,17 +43,19 @@ namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
 constexpr uint32_t LOG_CHUNK = 1024;  // entries per warp-owned log chunk
-constexpr uint32_t WIN_SHIFT = 19;    // 2^19 elements per window (first partition pass)
+constexpr uint32_t WIN_SHIFT = 20;    // 2^20 elements per window (first partition pass)
 constexpr uint32_t WIN = 1u << WIN_SHIFT;
 constexpr uint32_t SUB_SHIFT = 13;  // 2^13 elements per sub-window (second pass; resolved in shared memory)
 constexpr uint32_t SUB = 1u << SUB_SHIFT;
 constexpr uint32_t SUBS = WIN / SUB;    // sub-windows per window
-constexpr uint32_t MAX_BUCKETS = 8192;  // windows for 2^32 elements
+constexpr uint32_t MAX_BUCKETS = 4096;  // windows for 2^32 elements
 constexpr uint32_t CURSOR_STRIDE = 8;   // one 32 B sector per cursor (spreads the atomics)
 constexpr uint32_t PT_THREADS = 256;    // partition: threads per block
-constexpr uint32_t PT_ITEMS = 16;       // partition: entries per thread and tile
-constexpr uint32_t PT_TILE = PT_THREADS * PT_ITEMS;
-constexpr uint32_t PT_TILE_CHUNKS = PT_TILE / LOG_CHUNK;
+// entries per thread (a tile is PT_THREADS x ITEMS entries) and resident
+// blocks per SM of the two partition passes: 2048-entry tiles, 4 blocks per
+// SM (more tiles in flight per SM than 4096-entry tiles at 2 blocks)
+constexpr uint32_t P1_ITEMS = 8, P1_BLOCKS = 4;
+constexpr uint32_t P2_ITEMS = 8, P2_BLOCKS = 4;
 constexpr uint32_t FIN_THREADS = 256;  // resolve: threads per block (one sub-window per iteration)
 constexpr uint32_t FIN_GROUP = 8;      // resolve: entries a thread has in flight
 constexpr uint32_t NO_ROOT = 0xFFFFFFFFu;          // shared-memory root slot not written
@@ -266,13 +268,16 @@ __device__ uint32_t block_exclusive_scan(uint32_t* v, uint32_t m) {
 //   otherwise (second pass): tiles inside one window's region, buckets are
 //     its SUBS sub-windows
 // More entries than a bucket holds means some element was logged twice.
-template <bool FROM_LOG>
-__global__ void __launch_bounds__(PT_THREADS, 2) k_partition(const LogEnt* __restrict__ src,
+template <bool FROM_LOG, uint32_t ITEMS, uint32_t BLOCKS>
+__global__ void __launch_bounds__(PT_THREADS, BLOCKS) k_partition(const LogEnt* __restrict__ src,
                                                              const uint32_t* __restrict__ src_info, uint32_t nchunks,
                                                              const Out* __restrict__ out1, uint32_t limit,
                                                              uint32_t nb, LogEnt* __restrict__ dst,
                                                              uint32_t* __restrict__ dcursor,
                                                              uint32_t* __restrict__ beyond, DevStatus* st) {
+  constexpr uint32_t PT_TILE = PT_THREADS * ITEMS;
+  constexpr uint32_t PT_TILE_CHUNKS = PT_TILE / LOG_CHUNK;
+  static_assert(PT_TILE % LOG_CHUNK == 0 && WIN % PT_TILE == 0, "tiles hold whole log chunks");
   extern __shared__ __align__(16) unsigned char smraw[];
   uint4* stage = reinterpret_cast<uint4*>(smraw);
   const uint32_t nbk = FROM_LOG ? nb : SUBS;
@@ -302,11 +307,11 @@ __global__ void __launch_bounds__(PT_THREADS, 2) k_partition(const LogEnt* __res
     }
     if (threadIdx.x == 0) nbeyond = 0;
     __syncthreads();
-    uint4 v[PT_ITEMS];
-    uint32_t pos[PT_ITEMS];
+    uint4 v[ITEMS];
+    uint32_t pos[ITEMS];
     uint32_t mine_beyond = 0;
 #pragma unroll
-    for (uint32_t k = 0; k < PT_ITEMS; ++k) {
+    for (uint32_t k = 0; k < ITEMS; ++k) {
       const uint32_t e = k * PT_THREADS + threadIdx.x;
       const bool valid = FROM_LOG ? (e % LOG_CHUNK) < fills[e / LOG_CHUNK] : e < valid_end;
       v[k] = valid ? __ldcs(reinterpret_cast<const uint4*>(src + src0 + e)) : make_uint4(NO_ROOT, 0, 0, 0);
@@ -314,7 +319,7 @@ __global__ void __launch_bounds__(PT_THREADS, 2) k_partition(const LogEnt* __res
     if (FROM_LOG) {
       const uint64_t pol = l2_keep_policy();
 #pragma unroll
-      for (uint32_t k = 0; k < PT_ITEMS; ++k) {
+      for (uint32_t k = 0; k < ITEMS; ++k) {
         if (v[k].x >= limit) continue;
         const Out o = ld_out_nc_keep(out1 + v[k].y, pol);
         const uint64_t rank = o.rank - ((uint64_t)v[k].z | ((uint64_t)v[k].w << 32));
@@ -322,7 +327,7 @@ __global__ void __launch_bounds__(PT_THREADS, 2) k_partition(const LogEnt* __res
       }
     }
 #pragma unroll
-    for (uint32_t k = 0; k < PT_ITEMS; ++k) {
+    for (uint32_t k = 0; k < ITEMS; ++k) {
       pos[k] = NO_ROOT;
       const uint32_t x = v[k].x;
       if (x < limit) {
@@ -342,7 +347,7 @@ __global__ void __launch_bounds__(PT_THREADS, 2) k_partition(const LogEnt* __res
     if (FROM_LOG && threadIdx.x == 0 && nbeyond) atomicAdd(beyond, nbeyond);
     const uint32_t total = block_exclusive_scan(cnt, nbk);  // cnt now holds the tile's offsets
 #pragma unroll
-    for (uint32_t k = 0; k < PT_ITEMS; ++k) {
+    for (uint32_t k = 0; k < ITEMS; ++k) {
       if (pos[k] == NO_ROOT) continue;
       const uint32_t x = v[k].x;
       const uint32_t b = FROM_LOG ? x >> WIN_SHIFT : (x >> SUB_SHIFT) & (SUBS - 1);
@@ -585,8 +590,11 @@ kascade_status rank_level0_log(kascade_ctx& ctx, const Rec* rec, uint32_t n, uin
   uint32_t* cursor1 = cursor;
   uint32_t* cursor2 = cursor + (uint64_t)nb1 * CURSOR_STRIDE;
   KS_CUDA(cudaMemsetAsync(cursor, 0, sizeof(uint32_t) * nb1 * (SUBS + 1) * CURSOR_STRIDE, s));
-  const size_t smem1 = PT_TILE * sizeof(LogEnt) + 2 * sizeof(uint32_t) * nb1;
-  const size_t smem2 = PT_TILE * sizeof(LogEnt) + 2 * sizeof(uint32_t) * SUBS;
+  constexpr uint32_t TILE1 = PT_THREADS * P1_ITEMS, TILE2 = PT_THREADS * P2_ITEMS;
+  const size_t smem1 = TILE1 * sizeof(LogEnt) + 2 * sizeof(uint32_t) * nb1;
+  const size_t smem2 = TILE2 * sizeof(LogEnt) + 2 * sizeof(uint32_t) * SUBS;
+  auto k1 = k_partition<true, P1_ITEMS, P1_BLOCKS>;
+  auto k2 = k_partition<false, P2_ITEMS, P2_BLOCKS>;
   {
     // kernel attributes are per device: raise the shared-memory limits once on each
     static std::atomic<uint64_t> raised{0};
@@ -594,26 +602,25 @@ kascade_status rank_level0_log(kascade_ctx& ctx, const Rec* rec, uint32_t n, uin
     KS_CUDA(cudaGetDevice(&dev));
     const uint64_t bit = 1ull << (dev & 63);
     if (!(raised.load() & bit)) {
-      KS_CUDA(cudaFuncSetAttribute(k_partition<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)(PT_TILE * sizeof(LogEnt) + 2 * sizeof(uint32_t) * MAX_BUCKETS)));
-      KS_CUDA(cudaFuncSetAttribute(k_partition<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
+      KS_CUDA(cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)(TILE1 * sizeof(LogEnt) + 2 * sizeof(uint32_t) * MAX_BUCKETS)));
+      KS_CUDA(cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
       KS_CUDA(cudaFuncSetAttribute(k_place, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)(SUB * (sizeof(unsigned long long) + sizeof(uint32_t)))));
       raised.fetch_or(bit);
     }
   }
-  const uint64_t resident = (uint64_t)ctx.usable_sms() * 2;
   {
     ProfScope ps(ctx, "resolve", s);
-    const uint32_t tiles1 = (nchunks + PT_TILE_CHUNKS - 1) / PT_TILE_CHUNKS;
-    k_partition<true><<<(unsigned)std::min<uint64_t>(tiles1, resident), PT_THREADS, smem1, s>>>(
+    const uint32_t tiles1 = (nchunks + TILE1 / LOG_CHUNK - 1) / (TILE1 / LOG_CHUNK);
+    k1<<<(unsigned)std::min<uint64_t>(tiles1, (uint64_t)ctx.usable_sms() * P1_BLOCKS), PT_THREADS, smem1, s>>>(
         log, chunk_fill, nchunks, out1, limit, nb, part, cursor1, beyond, ctx.d_status);
     KS_CHECK_LAUNCH();
   }
-  const uint32_t tiles2 = nb * (WIN / PT_TILE);
+  const uint32_t tiles2 = nb * (WIN / TILE2);
   if (tiles2) {
     ProfScope ps(ctx, "partition", s);
-    k_partition<false><<<(unsigned)std::min<uint64_t>(tiles2, resident), PT_THREADS, smem2, s>>>(
+    k2<<<(unsigned)std::min<uint64_t>(tiles2, (uint64_t)ctx.usable_sms() * P2_BLOCKS), PT_THREADS, smem2, s>>>(
         part, cursor1, 0, nullptr, limit, nb, part2, cursor2, beyond, ctx.d_status);
     KS_CHECK_LAUNCH();
   }
