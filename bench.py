@@ -75,8 +75,9 @@ SECTORS_LIST_LOG = {True: 0.25 + 0.125 + 0.5 + 1.5 + 1 + 1 + 1, False: 0.25 + 0.
 # grows in proportion): profiles/chase_propagate_prepare_list25_ncu.md
 CHASE_DRAM_BYTES_PER_VISIT = (3.924e9 + 1.036e9) / (33_554_432 + 2_797_812)
 # The same for the write-free chase (k_chase_log), which reads each record
-# and appends a 16 B log entry: profiles/chase_log_list25_ncu.md
-CHASE_LOG_DRAM_BYTES_PER_VISIT = None
+# and appends a 16 B log entry: 3.901 GB read + 0.560 GB written over 2^25 +
+# 1 048 211 record reads (profiles/write_free_level0_list25_ncu.md)
+CHASE_LOG_DRAM_BYTES_PER_VISIT = (3.900669e9 + 0.560097e9) / (33_554_432 + 1_048_211)
 
 
 def log(*a):

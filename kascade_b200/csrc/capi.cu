@@ -214,9 +214,10 @@ KASCADE_API kascade_status kascade_ctx_reserve(kascade_ctx* c, uint64_t bytes) {
 }
 
 KASCADE_API uint64_t kascade_scratch_bytes_rank_list(uint64_t n) {
-  // level-0 records (16n) + ruler list (4n) + write-free path: log (16n),
-  // partitioned results (16n), reached flags (n) + level-1 records/results
-  // and deeper levels + per-warp log chunks
+  // level-0 records (16n) + ruler list (4n) + write-free path: log (16n,
+  // reused by the second partition pass), window partition (16n rounded up
+  // to whole 2^20-element windows), a margin of n, level-1 records/results
+  // and deeper levels + per-warp log chunks, cursors and window rounding
   return 16 * n + 4 * n + 16 * n + 16 * n + n + (40 * n) / 16 + (192ull << 20);
 }
 
