@@ -81,13 +81,20 @@ kascade_status rank_list_generic(kascade_ctx& ctx, const uint64_t* succ, WKind w
   Rec* rec = alloc<Rec>(ctx, n);
   uint32_t* ruler_elem = alloc<uint32_t>(ctx, n);
   if (!rec || !ruler_elem) return KASCADE_ERR_OOM;
-  if (device_levels && p.algorithm == KASCADE_ALGO_SPARSE_RULING_SET && n > p.base_max && n < p.level0_log_min &&
-      p.max_levels > 0) {
+  if (device_levels && p.algorithm == KASCADE_ALGO_SPARSE_RULING_SET && n > p.base_max && p.max_levels > 0) {
     uint32_t* r_dev = nullptr;
-    KS_TRY(prepare_arrays(ctx, succ, wk, w, (uint32_t)n, rec, ruler_elem, nullptr, p, s, &r_dev));
     SinkPlain sink{root_out, rank_out, keep_roots};
-    return rank_records_dev(ctx, rec, (uint32_t)n, r_dev, dev_cap_next((uint32_t)n, p.spacing0), ruler_elem, sink,
-                            p, s);
+    if (n < p.level0_log_min) {
+      KS_TRY(prepare_arrays(ctx, succ, wk, w, (uint32_t)n, rec, ruler_elem, nullptr, p, s, &r_dev));
+      return rank_records_dev(ctx, rec, (uint32_t)n, r_dev, dev_cap_next((uint32_t)n, p.spacing0), ruler_elem,
+                              sink, p, s);
+    }
+    if (!keep_roots) {
+      // the write-free level 0 with the ruler count and the deeper levels on the device
+      KS_TRY(prepare_arrays(ctx, succ, wk, w, (uint32_t)n, rec, ruler_elem, nullptr, p, s, &r_dev));
+      return rank_level0_log(ctx, rec, (uint32_t)n, dev_cap_next((uint32_t)n, p.spacing0), ruler_elem,
+                             sink.log_target((uint32_t)n), p, s, r_dev);
+    }
   }
   uint32_t r0 = 0;
   KS_TRY(prepare_arrays(ctx, succ, wk, w, (uint32_t)n, rec, ruler_elem, &r0, p, s));

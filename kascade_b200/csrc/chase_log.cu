@@ -105,11 +105,13 @@ __device__ __forceinline__ void log_append(bool emit, uint32_t x, uint32_t id, u
 template <int C>
 __global__ void __launch_bounds__(512) k_chase_log(const Rec* __restrict__ rec, uint32_t n,
                                                    const uint32_t* __restrict__ ruler_elem, uint32_t r,
+                                                   const uint32_t* __restrict__ r_dev,
                                                    Rec* __restrict__ rec_next, uint32_t* __restrict__ work,
                                                    LogEnt* __restrict__ log, uint32_t* __restrict__ chunk_fill,
                                                    uint32_t* __restrict__ chunk_cursor, uint32_t nchunks,
                                                    uint32_t max_hops, DevStatus* st) {
   constexpr uint32_t BATCH = 32u * C;
+  if (r_dev) r = min(r, *r_dev);  // the ruler count on the device, r its capacity
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t lt = lanemask_lt();
   uint32_t cid[C], cx[C], hops[C];
@@ -497,16 +499,22 @@ __global__ void __launch_bounds__(256) k_walk_unreached(const Rec* __restrict__ 
   }
 }
 
+// A chain that hit the hop cap, as a status: the device-driven call then
+// reruns on the host-driven path, whose level 0 tells the cases apart.
+__global__ void k_hop_cap_status(DevStatus* st) {
+  if (st->counter[0]) set_error(st, KASCADE_ERR_TIMEOUT, st->counter[0]);
+}
+
 int g_chase_occ[5][3] = {{-1, -1, -1}, {-1, -1, -1}, {-1, -1, -1}, {-1, -1, -1}, {-1, -1, -1}};
 
 template <int C>
 kascade_status launch_chase_log_c(kascade_ctx& ctx, const Rec* rec, uint32_t n, const uint32_t* ruler_elem, uint32_t r,
-                                  Rec* rec_next, uint32_t* work, LogEnt* log, uint32_t* chunk_fill,
-                                  uint32_t* chunk_cursor, uint32_t nchunks, uint32_t max_hops, unsigned grid,
-                                  uint32_t block, cudaStream_t s) {
+                                  const uint32_t* r_dev, Rec* rec_next, uint32_t* work, LogEnt* log,
+                                  uint32_t* chunk_fill, uint32_t* chunk_cursor, uint32_t nchunks, uint32_t max_hops,
+                                  unsigned grid, uint32_t block, cudaStream_t s) {
   ProfScope ps(ctx, "chase", s);
-  k_chase_log<C><<<grid, block, 0, s>>>(rec, n, ruler_elem, r, rec_next, work, log, chunk_fill, chunk_cursor, nchunks,
-                                      max_hops, ctx.d_status);
+  k_chase_log<C><<<grid, block, 0, s>>>(rec, n, ruler_elem, r, r_dev, rec_next, work, log, chunk_fill, chunk_cursor,
+                                      nchunks, max_hops, ctx.d_status);
   KS_CHECK_LAUNCH();
   return KASCADE_OK;
 }
@@ -533,7 +541,8 @@ unsigned chase_grid(const kascade_ctx& ctx, uint32_t r, uint32_t block) {
 }  // namespace
 
 kascade_status rank_level0_log(kascade_ctx& ctx, const Rec* rec, uint32_t n, uint32_t r0, const uint32_t* ruler_elem0,
-                               const LogTarget& t, const Params& p, cudaStream_t s) {
+                               const LogTarget& t, const Params& p, cudaStream_t s, const uint32_t* r0_dev) {
+  if (r0_dev) ctx.last_levels.assign(1, n);  // the deeper sizes come back with the status
   const int C = (p.chains == 1 || p.chains == 4) ? (int)p.chains : 2;
   const uint32_t block = p.block;
   const unsigned grid = C == 1   ? chase_grid<1>(ctx, r0, block)
@@ -546,9 +555,15 @@ kascade_status rank_level0_log(kascade_ctx& ctx, const Rec* rec, uint32_t n, uin
   uint32_t* counters = alloc<uint32_t>(ctx, 8);  // chunk cursor, chase work, unreached count, beyond
   Rec* rec1 = alloc<Rec>(ctx, r0);
   Out* out1 = alloc<Out>(ctx, r0);
-  if (!log || !chunk_fill || !counters || !rec1 || !out1) return KASCADE_ERR_OOM;
+  uint32_t* lv = r0_dev ? alloc<uint32_t>(ctx, MAX_DEV_LEVELS + 2) : nullptr;  // level sizes (device)
+  if (!log || !chunk_fill || !counters || !rec1 || !out1 || (r0_dev && !lv)) return KASCADE_ERR_OOM;
   KS_CUDA(cudaMemsetAsync(chunk_fill, 0, sizeof(uint32_t) * nchunks, s));
   KS_CUDA(cudaMemsetAsync(counters, 0, sizeof(uint32_t) * 8, s));
+  if (r0_dev) {
+    KS_CUDA(cudaMemsetAsync(lv, 0, sizeof(uint32_t) * (MAX_DEV_LEVELS + 2), s));
+    KS_TRY(launch_check_count(ctx, r0_dev, r0, lv + 1, s));
+  }
+  const uint32_t* r_dev = r0_dev ? lv + 1 : nullptr;
   uint32_t* chunk_cursor = counters + 0;
   uint32_t* chase_work = counters + 1;
   uint32_t* ucount = counters + 2;
@@ -557,25 +572,30 @@ kascade_status rank_level0_log(kascade_ctx& ctx, const Rec* rec, uint32_t n, uin
   const uint32_t max_hops = cap < n ? (uint32_t)cap : n;
   switch (C) {
     case 1:
-      KS_TRY(launch_chase_log_c<1>(ctx, rec, n, ruler_elem0, r0, rec1, chase_work, log, chunk_fill, chunk_cursor,
-                                   nchunks, max_hops, grid, block, s));
+      KS_TRY(launch_chase_log_c<1>(ctx, rec, n, ruler_elem0, r0, r_dev, rec1, chase_work, log, chunk_fill,
+                                   chunk_cursor, nchunks, max_hops, grid, block, s));
       break;
     case 4:
-      KS_TRY(launch_chase_log_c<4>(ctx, rec, n, ruler_elem0, r0, rec1, chase_work, log, chunk_fill, chunk_cursor,
-                                   nchunks, max_hops, grid, block, s));
+      KS_TRY(launch_chase_log_c<4>(ctx, rec, n, ruler_elem0, r0, r_dev, rec1, chase_work, log, chunk_fill,
+                                   chunk_cursor, nchunks, max_hops, grid, block, s));
       break;
     default:
-      KS_TRY(launch_chase_log_c<2>(ctx, rec, n, ruler_elem0, r0, rec1, chase_work, log, chunk_fill, chunk_cursor,
-                                   nchunks, max_hops, grid, block, s));
+      KS_TRY(launch_chase_log_c<2>(ctx, rec, n, ruler_elem0, r0, r_dev, rec1, chase_work, log, chunk_fill,
+                                   chunk_cursor, nchunks, max_hops, grid, block, s));
   }
-  {
+  // level-1 elements are level-0 rulers: their level-0 index is ruler_elem0
+  int levels = 0;
+  if (r0_dev) {
+    k_hop_cap_status<<<1, 1, 0, s>>>(ctx.d_status);
+    KS_CHECK_LAUNCH();
+    KS_TRY(rank_deep_dev(ctx, rec1, out1, r0, lv, ruler_elem0, p, s, &levels));
+  } else {
     // a chain hit the hop cap: let the caller rerun level 0 on the stamping path
     uint32_t over = 0;
     KS_TRY(read_u32(ctx, reinterpret_cast<const uint32_t*>(&ctx.d_status->counter[0]), &over, s));
     if (over) return KASCADE_ERR_TIMEOUT;
+    KS_TRY(rank_sublist(ctx, rec1, r0, ruler_elem0, out1, 1, p, s));
   }
-  // level-1 elements are level-0 rulers: their level-0 index is ruler_elem0
-  KS_TRY(rank_sublist(ctx, rec1, r0, ruler_elem0, out1, 1, p, s));
 
   const uint32_t limit = t.limit < n ? t.limit : n;
   const uint32_t nb = (uint32_t)(((uint64_t)limit + WIN - 1) / WIN);
@@ -642,6 +662,7 @@ kascade_status rank_level0_log(kascade_ctx& ctx, const Rec* rec, uint32_t n, uin
                                                       ctx.d_status);
     KS_CHECK_LAUNCH();
   }
+  if (r0_dev) return report_dev_levels(ctx, lv, levels, n, s);
   return KASCADE_OK;
 }
 

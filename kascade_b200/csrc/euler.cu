@@ -316,8 +316,12 @@ kascade_status root_forest_impl(kascade_ctx& ctx, const uint64_t* parent, uint32
     KS_CHECK_LAUNCH();
   }
   SinkTour sink{root_out, depth_out, n, keep_roots};
-  if (device_levels && m > p.base_max && m < p.level0_log_min && p.max_levels > 0)
-    return rank_records_dev(ctx, rec, m, ctr, dev_cap_next(m, p.spacing0), ruler_elem, sink, p, s);
+  if (device_levels && m > p.base_max && p.max_levels > 0) {
+    if (m < p.level0_log_min)
+      return rank_records_dev(ctx, rec, m, ctr, dev_cap_next(m, p.spacing0), ruler_elem, sink, p, s);
+    if (!keep_roots)  // the write-free level 0 with the ruler count and the deeper levels on the device
+      return rank_level0_log(ctx, rec, m, dev_cap_next(m, p.spacing0), ruler_elem, sink.log_target(m), p, s, ctr);
+  }
   uint32_t r = 0;
   KS_TRY(read_u32(ctx, ctr, &r, s));
   return rank_records(ctx, rec, m, r, ruler_elem, sink, p, s);

@@ -989,7 +989,6 @@ kascade_status rank_records(kascade_ctx& ctx, Rec* rec, uint32_t n, uint32_t r0,
 // the host-driven path.  The sequence of launches depends only on n and the
 // capacities, so it can be captured in a CUDA graph.
 // ---------------------------------------------------------------------------
-constexpr int MAX_DEV_LEVELS = 8;
 constexpr uint32_t DEV_FINAL = 1u << 17;
 constexpr uint32_t DEV_ROOT_MARGIN = 1u << 16;
 
@@ -998,15 +997,14 @@ uint32_t dev_cap_next(uint32_t cap, uint32_t spacing) {
   return nx < cap ? (uint32_t)nx : cap;
 }
 
-template <class Sink>
-kascade_status rank_records_dev(kascade_ctx& ctx, Rec* rec, uint32_t n, const uint32_t* r0_dev, uint32_t cap1,
-                                uint32_t* ruler_elem0, const Sink& sink, const Params& p, cudaStream_t s) {
-  ctx.last_levels.clear();
-  ctx.last_levels.push_back(n);
-  if (n == 0) return KASCADE_OK;
+// Levels 1.. of the device-driven recursion.  rec1 / out1 hold caps1
+// elements; cnt[1] (device) holds level 1's size once the level-0 chase that
+// writes rec1 has run, already checked against caps1; elem0_1 gives each
+// level-1 element's level-0 index.  Fills out1 and cnt[2..L]; *levels = L.
+kascade_status rank_deep_dev(kascade_ctx& ctx, Rec* rec1, Out* out1, uint32_t cap1, uint32_t* cnt,
+                             const uint32_t* elem0_1, const Params& p, cudaStream_t s, int* levels) {
   uint32_t caps[MAX_DEV_LEVELS + 1];
-  caps[0] = n;
-  caps[1] = cap1 < n ? cap1 : n;
+  caps[1] = cap1;
   int L = 1;
   while (caps[L] > DEV_FINAL && L < MAX_DEV_LEVELS) {
     const uint32_t nx = dev_cap_next(caps[L], p.spacing_deep);
@@ -1014,22 +1012,21 @@ kascade_status rank_records_dev(kascade_ctx& ctx, Rec* rec, uint32_t n, const ui
     caps[L + 1] = nx;
     ++L;
   }
-  uint32_t* cnt = alloc<uint32_t>(ctx, MAX_DEV_LEVELS + 2);
-  if (!cnt) return KASCADE_ERR_OOM;
-  KS_CUDA(cudaMemsetAsync(cnt, 0, sizeof(uint32_t) * (MAX_DEV_LEVELS + 2), s));
   Rec* recs[MAX_DEV_LEVELS + 1];
   Out* outs[MAX_DEV_LEVELS + 1];
   uint32_t* rulers[MAX_DEV_LEVELS + 1];
   const uint32_t* elem0s[MAX_DEV_LEVELS + 1];
   const uint32_t* sizes[MAX_DEV_LEVELS + 1];
-  recs[0] = rec;
-  rulers[0] = ruler_elem0;
-  elem0s[1] = ruler_elem0;  // level-1 elements are level-0 rulers
-  sizes[1] = r0_dev;
+  recs[1] = rec1;
+  outs[1] = out1;
+  elem0s[1] = elem0_1;
+  sizes[1] = cnt + 1;
   for (int k = 1; k <= L; ++k) {
-    recs[k] = alloc<Rec>(ctx, caps[k]);
-    outs[k] = alloc<Out>(ctx, caps[k]);
-    if (!recs[k] || !outs[k]) return KASCADE_ERR_OOM;
+    if (k > 1) {
+      recs[k] = alloc<Rec>(ctx, caps[k]);
+      outs[k] = alloc<Out>(ctx, caps[k]);
+      if (!recs[k] || !outs[k]) return KASCADE_ERR_OOM;
+    }
     if (k < L) {
       rulers[k] = alloc<uint32_t>(ctx, caps[k + 1]);
       uint32_t* e0 = alloc<uint32_t>(ctx, caps[k + 1]);
@@ -1037,15 +1034,6 @@ kascade_status rank_records_dev(kascade_ctx& ctx, Rec* rec, uint32_t n, const ui
       elem0s[k + 1] = e0;
       sizes[k + 1] = cnt + k + 1;
     }
-  }
-  k_check_count<<<1, 1, 0, s>>>(r0_dev, caps[1], cnt + 1, ctx.d_status);
-  KS_CHECK_LAUNCH();
-  // level 0 chase: capacities as bounds, the ruler count from device memory
-  {
-    uint32_t* work = alloc<uint32_t>(ctx, 1);
-    if (!work) return KASCADE_ERR_OOM;
-    KS_CUDA(cudaMemsetAsync(work, 0, sizeof(uint32_t), s));
-    KS_TRY(launch_chase_dev(ctx, recs[0], n, nullptr, rulers[0], caps[1], r0_dev, recs[1], work, p, s));
   }
   for (int k = 1; k < L; ++k) {
     {
@@ -1088,7 +1076,7 @@ kascade_status rank_records_dev(kascade_ctx& ctx, Rec* rec, uint32_t n, const ui
     k_pd_final<SinkOut><<<grid, 256, 0, s>>>(a, m, sizes[L], elem0s[L], SinkOut{outs[L]});
     KS_CHECK_LAUNCH();
   }
-  // propagate back up
+  // propagate back up to level 1
   for (int k = L - 1; k >= 1; --k) {
     ProfScope ps(ctx, "propagate", s);
     const unsigned grid = grid_for(ctx, ((uint64_t)caps[k] + PROP_ITEMS - 1) / PROP_ITEMS, 256, 8);
@@ -1096,13 +1084,51 @@ kascade_status rank_records_dev(kascade_ctx& ctx, Rec* rec, uint32_t n, const ui
                                               SinkOut{outs[k]}, ctx.d_status);
     KS_CHECK_LAUNCH();
   }
-  KS_TRY(launch_propagate(ctx, rec, sink.limit(n), n, outs[1], caps[1], sink, s));
-  // the level sizes travel back with the call's status
+  *levels = L;
+  return KASCADE_OK;
+}
+
+kascade_status launch_check_count(kascade_ctx& ctx, const uint32_t* cnt, uint32_t cap, uint32_t* copy,
+                                  cudaStream_t s) {
+  k_check_count<<<1, 1, 0, s>>>(cnt, cap, copy, ctx.d_status);
+  KS_CHECK_LAUNCH();
+  return KASCADE_OK;
+}
+
+kascade_status report_dev_levels(kascade_ctx& ctx, const uint32_t* cnt, int L, uint32_t n, cudaStream_t s) {
   KS_CUDA(cudaMemcpyAsync(reinterpret_cast<uint32_t*>(ctx.h_pinned + KS_PINNED_LEVELS), cnt,
                           sizeof(uint32_t) * (L + 1), cudaMemcpyDeviceToHost, s));
   ctx.pending_levels = L;
   ctx.pending_n = n;
   return KASCADE_OK;
+}
+
+template <class Sink>
+kascade_status rank_records_dev(kascade_ctx& ctx, Rec* rec, uint32_t n, const uint32_t* r0_dev, uint32_t cap1,
+                                uint32_t* ruler_elem0, const Sink& sink, const Params& p, cudaStream_t s) {
+  ctx.last_levels.clear();
+  ctx.last_levels.push_back(n);
+  if (n == 0) return KASCADE_OK;
+  if (cap1 > n) cap1 = n;
+  uint32_t* cnt = alloc<uint32_t>(ctx, MAX_DEV_LEVELS + 2);
+  Rec* rec1 = alloc<Rec>(ctx, cap1);
+  Out* out1 = alloc<Out>(ctx, cap1);
+  if (!cnt || !rec1 || !out1) return KASCADE_ERR_OOM;
+  KS_CUDA(cudaMemsetAsync(cnt, 0, sizeof(uint32_t) * (MAX_DEV_LEVELS + 2), s));
+  KS_TRY(launch_check_count(ctx, r0_dev, cap1, cnt + 1, s));
+  // level 0 chase: capacities as bounds, the ruler count from device memory
+  {
+    uint32_t* work = alloc<uint32_t>(ctx, 1);
+    if (!work) return KASCADE_ERR_OOM;
+    KS_CUDA(cudaMemsetAsync(work, 0, sizeof(uint32_t), s));
+    KS_TRY(launch_chase_dev(ctx, rec, n, nullptr, ruler_elem0, cap1, r0_dev, rec1, work, p, s));
+  }
+  // level-1 elements are level-0 rulers: their level-0 index is ruler_elem0
+  int L = 1;
+  KS_TRY(rank_deep_dev(ctx, rec1, out1, cap1, cnt, ruler_elem0, p, s, &L));
+  KS_TRY(launch_propagate(ctx, rec, sink.limit(n), n, out1, cap1, sink, s));
+  // the level sizes travel back with the call's status
+  return report_dev_levels(ctx, cnt, L, n, s);
 }
 
 template kascade_status rank_records_dev<SinkBatch>(kascade_ctx&, Rec*, uint32_t, const uint32_t*, uint32_t,

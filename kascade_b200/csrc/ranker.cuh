@@ -162,9 +162,6 @@ kascade_status rank_records(kascade_ctx& ctx, Rec* rec, uint32_t n, uint32_t r0,
 kascade_status rank_sublist(kascade_ctx& ctx, Rec* rec, uint32_t n, const uint32_t* elem0, Out* out,
                             int level, const Params& p, cudaStream_t s);
 
-// Write-free level 0: read-only chase that logs (element, ruler, distance),
-// recursion on the ruler sub-list, then resolve + partition by element window
-// and a windowed scatter into the outputs.
 // The recursion without host waits (see ranker.cu): r0_dev holds the level-0
 // ruler count, cap1 bounds it.  Errors, including a level that outgrows its
 // capacity (KASCADE_ERR_TIMEOUT: rerun on the host-driven path), land in the
@@ -173,14 +170,33 @@ template <class Sink>
 kascade_status rank_records_dev(kascade_ctx& ctx, Rec* rec, uint32_t n, const uint32_t* r0_dev, uint32_t cap1,
                                 uint32_t* ruler_elem0, const Sink& sink, const Params& p, cudaStream_t s);
 uint32_t dev_cap_next(uint32_t cap, uint32_t spacing);
+constexpr int MAX_DEV_LEVELS = 8;
+// Levels 1.. of that recursion: rec1 / out1 hold cap1 elements, cnt (device,
+// MAX_DEV_LEVELS + 2 words) holds level 1's size in cnt[1] once the level-0
+// chase has run; fills out1 and cnt[2..L], *levels = L.
+kascade_status rank_deep_dev(kascade_ctx& ctx, Rec* rec1, Out* out1, uint32_t cap1, uint32_t* cnt,
+                             const uint32_t* elem0_1, const Params& p, cudaStream_t s, int* levels);
+// *copy = *cnt, and KASCADE_ERR_TIMEOUT in the status word when it exceeds cap.
+kascade_status launch_check_count(kascade_ctx& ctx, const uint32_t* cnt, uint32_t cap, uint32_t* copy,
+                                  cudaStream_t s);
+// Level sizes cnt[1..L] travel back with the call's status read.
+kascade_status report_dev_levels(kascade_ctx& ctx, const uint32_t* cnt, int L, uint32_t n, cudaStream_t s);
 
 kascade_status compute_stats(kascade_ctx& ctx, const uint64_t* root, const int64_t* rank, uint64_t n, int level,
                              kascade_stats* out, kascade_tree_stats* per_tree, uint64_t per_tree_cap,
                              uint64_t* per_tree_count, cudaStream_t s);
 
+// Write-free level 0: read-only chase that logs (element, ruler, distance),
+// recursion on the ruler sub-list, then two radix passes over the log by
+// element and a dense placement into the outputs.  With r0_dev the ruler
+// count stays on the device (r0 is then its capacity) and so does the
+// recursion: no host wait; a chain past the hop cap or a level past its
+// capacity reports KASCADE_ERR_TIMEOUT in the status word (rerun on the
+// host-driven path).  Without it, a chain past the hop cap returns
+// KASCADE_ERR_TIMEOUT directly (level 0 again on the stamping path).
 kascade_status rank_level0_log(kascade_ctx& ctx, const Rec* rec, uint32_t n, uint32_t r0,
                                const uint32_t* ruler_elem0, const LogTarget& t, const Params& p,
-                               cudaStream_t s);
+                               cudaStream_t s, const uint32_t* r0_dev = nullptr);
 
 // Pointer doubling on level-0 records (tags ignored).
 template <class Sink>
