@@ -88,15 +88,20 @@ def test_write_free_above_2_22(kb, oracle_mod, layout):
     np.testing.assert_array_equal(host_u64(rank), rank_o)
     times = ctx.kernel_times()
     assert "resolve" in times and "partition" in times and "place" in times
+    # the recursion ran on the device: its level sizes come back with the status
+    levels = ctx.levels()
+    assert levels[0] == n and len(levels) >= 3
+    assert all(a > b for a, b in zip(levels, levels[1:]))
     ctx.close()
 
 
 def test_write_free_many_lists_several_windows(kb, oracle_mod):
-    """The write-free level 0 on 30 000 lists over several 2^19-element
-    windows: thousands of list heads ahead of their first ruler, spread over
-    many sub-windows, walk to their first reached element."""
+    """The write-free level 0 on 30 000 lists over three 2^20-element output
+    windows (the last one partial): thousands of list heads ahead of their
+    first ruler, spread over many sub-windows, walk to their first reached
+    element."""
     rng = np.random.default_rng(0xE1)
-    n = 3 * (1 << 19) + 777
+    n = 2 * (1 << 20) + 777
     order = rng.permutation(n).astype(np.uint64)
     cuts = np.sort(rng.choice(np.arange(1, n), size=30_000 - 1, replace=False))
     succ_h = np.empty(n, np.uint64)
