@@ -384,7 +384,11 @@ __global__ void __launch_bounds__(FIN_THREADS, 2) k_place(const LogEnt* __restri
                                                             uint64_t* __restrict__ root_out,
                                                             uint64_t* __restrict__ rank_out, uint32_t* __restrict__ ulist,
                                                             uint32_t* __restrict__ ucount, uint32_t ucap,
+                                                            const uint64_t* __restrict__ seg_off,
+                                                            const uint32_t* __restrict__ hint, uint32_t nseg,
                                                             DevStatus* st) {
+  // a batch reports roots relative to their instance
+  const SinkBatch inst{nullptr, nullptr, 0, seg_off, hint, nseg};
   extern __shared__ __align__(16) unsigned char smraw[];
   unsigned long long* rank_s = reinterpret_cast<unsigned long long*>(smraw);  // SUB entries
   uint32_t* root_s = reinterpret_cast<uint32_t*>(rank_s + SUB);               // SUB entries
@@ -429,7 +433,8 @@ __global__ void __launch_bounds__(FIN_THREADS, 2) k_place(const LogEnt* __restri
       if (i < len) {
         const uint32_t r = root_s[i];
         un = r == NO_ROOT;
-        __stcs(reinterpret_cast<unsigned long long*>(root_out) + lo + i, un ? NOT_REACHED : (unsigned long long)r);
+        const unsigned long long base = (seg_off && !un) ? inst.base_of(lo + i) : 0ull;
+        __stcs(reinterpret_cast<unsigned long long*>(root_out) + lo + i, un ? NOT_REACHED : (unsigned long long)r - base);
         __stcs(reinterpret_cast<unsigned long long*>(rank_out) + lo + i, un ? 0ull : rank_s[i]);
       }
       const uint32_t m = __ballot_sync(FULL, un);
@@ -454,13 +459,16 @@ __global__ void __launch_bounds__(FIN_THREADS, 2) k_place(const LogEnt* __restri
 }
 
 // Each unreached element walks forward to the first element with outputs:
-// one the resolve wrote (root output not NOT_REACHED) or one another walker
-// finished.  Walkers write the rank, fence, then the root, and readers load
-// the root, fence, then the rank, so a root seen set comes with its rank.
-// Plain lists only (every element has outputs).
+// one the place step wrote (root output not NOT_REACHED) or one another
+// walker finished.  Walkers write the rank, fence, then the root, and readers
+// load the root, fence, then the rank, so a root seen set comes with its
+// rank.  Elements at or above `limit` (a batch's tour down edges) have no
+// outputs and are walked through.  Roots already relative to their instance
+// stay so: a walker and the element it stops at share an instance.
 __global__ void __launch_bounds__(256) k_walk_unreached(const Rec* __restrict__ rec, const uint32_t* __restrict__ ulist,
                                                         const uint32_t* __restrict__ ucount, uint32_t ucap, uint32_t n,
-                                                        uint64_t* root_out, uint64_t* rank_out, DevStatus* st) {
+                                                        uint32_t limit, uint64_t* root_out, uint64_t* rank_out,
+                                                        DevStatus* st) {
   const uint32_t cnt = min(*ucount, ucap);
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
     const uint32_t u = ulist[i];
@@ -477,8 +485,10 @@ __global__ void __launch_bounds__(256) k_walk_unreached(const Rec* __restrict__ 
         ok = false;
         break;
       }
-      base_root = __ldcg(reinterpret_cast<const unsigned long long*>(root_out) + y);
-      if (base_root != NOT_REACHED) break;
+      if (y < limit) {
+        base_root = __ldcg(reinterpret_cast<const unsigned long long*>(root_out) + y);
+        if (base_root != NOT_REACHED) break;
+      }
       if (y == mark || ++hops > n) {
         set_error(st, KASCADE_ERR_CYCLE, u);
         ok = false;
@@ -653,12 +663,12 @@ kascade_status rank_level0_log(kascade_ctx& ctx, const Rec* rec, uint32_t n, uin
     const size_t smem = SUB * (sizeof(unsigned long long) + sizeof(uint32_t));
     k_place<<<(unsigned)std::max<uint64_t>(1, std::min<uint64_t>(items, (uint64_t)ctx.usable_sms() * 2)),
                 FIN_THREADS, smem, s>>>(part2, cursor2, nb, limit, n, beyond, t.heads_are_rulers, t.root, t.rank,
-                                        ulist, ucount, ucap, ctx.d_status);
+                                        ulist, ucount, ucap, t.seg_off, t.hint, t.nseg, ctx.d_status);
     KS_CHECK_LAUNCH();
   }
   if (!t.heads_are_rulers) {
     ProfScope ps(ctx, "heads", s);
-    k_walk_unreached<<<ctx.usable_sms() * 4, 256, 0, s>>>(rec, ulist, ucount, ucap, n, t.root, t.rank,
+    k_walk_unreached<<<ctx.usable_sms() * 4, 256, 0, s>>>(rec, ulist, ucount, ucap, n, limit, t.root, t.rank,
                                                       ctx.d_status);
     KS_CHECK_LAUNCH();
   }

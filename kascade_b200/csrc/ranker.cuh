@@ -48,6 +48,12 @@ struct LogTarget {
   uint32_t limit;        // elements [0, limit) produce output
   int keep_roots;        // leave roots' entries untouched
   int heads_are_rulers;  // every list head is a ruler: no element is left unreached
+  // a batch of instances in one index space: roots are reported relative to
+  // their instance (seg_off: nseg instance offsets, hint[k]: the instance
+  // holding element k * 4096); null for a single instance
+  const uint64_t* seg_off = nullptr;
+  const uint32_t* hint = nullptr;
+  uint32_t nseg = 0;
 };
 
 // Plain arrays. keep_roots: leave root entries untouched (the reference's
@@ -103,7 +109,7 @@ struct SinkTour {
 // instance offsets (non-decreasing), hint[k] the instance containing element
 // k * 4096.  Elements at or beyond `total` (tour down edges) give no output.
 struct SinkBatch {
-  static constexpr bool kWriteFree = false;
+  static constexpr bool kWriteFree = true;
   uint64_t* root;
   uint64_t* rank;
   uint32_t total;
@@ -111,7 +117,7 @@ struct SinkBatch {
   const uint32_t* hint;
   uint32_t nseg;
   uint32_t limit(uint32_t n) const { return n < total ? n : total; }
-  LogTarget log_target(uint32_t n) const { return LogTarget{root, rank, limit(n), 0, 0}; }
+  LogTarget log_target(uint32_t n) const { return LogTarget{root, rank, limit(n), 0, 0, seg_off, hint, nseg}; }
   __device__ __forceinline__ uint64_t base_of(uint32_t x) const {
     uint32_t j = __ldg(hint + (x >> 12));
     while (j + 1 < nseg && __ldg(seg_off + j + 1) <= x) ++j;

@@ -35,7 +35,9 @@ def _check(kb, oracle_mod, inputs, w, sizes, kinds, root, rank):
         off += sz
 
 
-@pytest.mark.parametrize("tuning", [{}, DEEP, dict(base_case_size=64), dict(ruler_spacing=5)])
+@pytest.mark.parametrize("tuning", [{}, DEEP, dict(base_case_size=64), dict(ruler_spacing=5),
+                                    # the write-free level 0 (the default from 2^25 records), forced
+                                    dict(level0_mode=2), dict(DEEP, level0_mode=2)])
 @pytest.mark.parametrize("weighted", [False, True])
 def test_batch_mixed(kb, oracle_mod, tuning, weighted):
     sizes, kinds = kb.batch_sizes(300, seed=7, lo_log2=0, hi_log2=14)
@@ -45,13 +47,35 @@ def test_batch_mixed(kb, oracle_mod, tuning, weighted):
     _check(kb, oracle_mod, inputs, w if weighted else None, sizes, kinds, root, rank)
 
 
-def test_batch_large_instances(kb, oracle_mod):
+@pytest.mark.parametrize("level0_mode", [0, 1, 2])
+def test_batch_large_instances(kb, oracle_mod, level0_mode):
     sizes = np.array([1 << 20, 64, 3000, 1 << 19, 1, 2, 70000], np.int64)
     kinds = np.array([0, 1, 0, 1, 1, 0, 0])
     inputs, w = kb.gen_batch(sizes, kinds, seed=11)
     segs = kb.make_segments(sizes, kinds)
-    root, rank = kb.rank_batch(inputs, segs, w)
+    root, rank = kb.rank_batch(inputs, segs, w, tuning=kb.GpuTuning(level0_mode=level0_mode))
     _check(kb, oracle_mod, inputs, w, sizes, kinds, root, rank)
+
+
+def test_batch_write_free_overflow_and_profile(kb, oracle_mod):
+    """A batch on the write-free level 0: its kernels run (profile names), and
+    an all-roots batch, whose levels outgrow the device-driven capacities, is
+    ranked again on the host-driven path with the same exact results."""
+    sizes, kinds = kb.batch_sizes(64, seed=41, lo_log2=10, hi_log2=18)
+    inputs, w = kb.gen_batch(sizes, kinds, seed=43)
+    ctx = kb.Context()
+    root, rank = kb.rank_batch(inputs, kb.make_segments(sizes, kinds), w, ctx=ctx,
+                               tuning=kb.GpuTuning(level0_mode=2, profile=True))
+    _check(kb, oracle_mod, inputs, w, sizes, kinds, root, rank)
+    times = ctx.kernel_times()
+    assert "resolve" in times and "place" in times
+    sizes = np.full(40, 50_000, np.int64)
+    kinds = np.zeros(40, np.int64)
+    inputs = torch.cat([torch.arange(50_000, dtype=torch.int64, device="cuda") for _ in range(40)])
+    root, rank = kb.rank_batch(inputs, kb.make_segments(sizes, kinds), None, ctx=ctx,
+                               tuning=kb.GpuTuning(level0_mode=2))
+    _check(kb, oracle_mod, inputs, None, sizes, kinds, root, rank)
+    ctx.close()
 
 
 def test_batch_device_levels_and_fallback(kb, oracle_mod):
