@@ -69,27 +69,41 @@ __global__ void __launch_bounds__(BP_THREADS) k_batch_prepare(const Item* __rest
     if (sg.kind == KASCADE_SEG_LIST) {
       uint32_t sv[BP_PER];
       uint64_t wv[BP_PER];
+      unsigned long long lv[BP_PER];
       uint32_t rl = 0, cnt = 0;
+      // every load of the item first (independent, all in flight together),
+      // then the checks and the sampling
+#pragma unroll
+      for (int i = 0; i < BP_PER; ++i) {
+        const uint32_t k = item.start + i * BP_THREADS + threadIdx.x;
+        lv[i] = 0;
+        wv[i] = 0;
+        if (k < item.start + item.count) {
+          const uint64_t g = sg.off + k;
+          lv[i] = __ldcs(reinterpret_cast<const unsigned long long*>(in) + g);
+          wv[i] = w(g);
+        }
+      }
+      uint64_t bad = ~0ull;  // the first element whose successor is out of its instance
 #pragma unroll
       for (int i = 0; i < BP_PER; ++i) {
         const uint32_t k = item.start + i * BP_THREADS + threadIdx.x;
         sv[i] = 0;
-        wv[i] = 0;
         if (k < item.start + item.count) {
           const uint64_t g = sg.off + k;
-          unsigned long long loc = __ldcs(reinterpret_cast<const unsigned long long*>(in) + g);
+          unsigned long long loc = lv[i];
           if (loc >= sg.size) {
-            set_error(st, KASCADE_ERR_OUT_OF_RANGE, g);
+            if (bad == ~0ull) bad = g;
             loc = k;
           }
           sv[i] = (uint32_t)(sg.off + loc);
-          wv[i] = w(g);
           if (loc == k || sampled((uint32_t)g, salt, sg.thresh)) {
             rl |= 1u << i;
             cnt++;
           }
         }
       }
+      if (bad != ~0ull) set_error(st, KASCADE_ERR_OUT_OF_RANGE, bad);
       uint32_t total;
       const uint32_t pre = block_exclusive_scan(cnt, sm, &total);
       if (threadIdx.x == 0) {
@@ -119,15 +133,25 @@ __global__ void __launch_bounds__(BP_THREADS) k_batch_prepare(const Item* __rest
       }
       __syncthreads();
     } else {
-      for (uint32_t k = item.start + threadIdx.x; k < item.start + item.count; k += BP_THREADS) {
-        const uint64_t g = sg.off + k;
-        unsigned long long par = __ldcs(reinterpret_cast<const unsigned long long*>(in) + g);
+      unsigned long long pv[BP_PER];
+#pragma unroll
+      for (int i = 0; i < BP_PER; ++i) {
+        const uint32_t k = item.start + i * BP_THREADS + threadIdx.x;
+        pv[i] = k < item.start + item.count ? __ldcs(reinterpret_cast<const unsigned long long*>(in) + sg.off + k) : 0;
+      }
+      uint64_t bad = ~0ull;
+#pragma unroll
+      for (int i = 0; i < BP_PER; ++i) {
+        const uint32_t k = item.start + i * BP_THREADS + threadIdx.x;
+        if (k >= item.start + item.count) continue;
+        unsigned long long par = pv[i];
         if (par >= sg.size) {
-          set_error(st, KASCADE_ERR_OUT_OF_RANGE, g);
+          if (bad == ~0ull) bad = sg.off + k;
           par = k;
         }
-        fpar[sg.fd + k] = sg.fd + par;
+        __stcs(reinterpret_cast<unsigned long long*>(fpar) + sg.fd + k, (unsigned long long)(sg.fd + par));
       }
+      if (bad != ~0ull) set_error(st, KASCADE_ERR_OUT_OF_RANGE, bad);
     }
   }
 }
