@@ -127,6 +127,28 @@ def test_batch_plan_graph_replay(kb, oracle_mod):
     assert e.value.name == "UNSUPPORTED"
 
 
+def test_batch_plan_write_free(kb, oracle_mod):
+    """A plan over the write-free level 0 (the path of batches from 2^25
+    records, forced here): the captured graph holds the read-only chase, the
+    partition passes, the place step and the head walk, and its replays give
+    the oracle's results, also after the inputs change in place."""
+    sizes, kinds = kb.batch_sizes(120, seed=51, lo_log2=6, hi_log2=17)
+    inputs, w = kb.gen_batch(sizes, kinds, seed=53)
+    segs = kb.make_segments(sizes, kinds)
+    plan = kb.BatchPlan(inputs, segs, w, tuning=kb.GpuTuning(level0_mode=2))
+    for _ in range(2):
+        root, rank = plan.launch()
+        torch.cuda.synchronize()
+        _check(kb, oracle_mod, inputs, w, sizes, kinds, root, rank)
+    inputs2, w2 = kb.gen_batch(sizes, kinds, seed=55)
+    inputs.copy_(inputs2)
+    w.copy_(w2)
+    root, rank = plan.launch()
+    torch.cuda.synchronize()
+    _check(kb, oracle_mod, inputs, w, sizes, kinds, root, rank)
+    plan.close()
+
+
 def test_batch_only_lists_and_only_forests(kb, oracle_mod):
     for kind in (0, 1):
         sizes = np.array([5000, 1, 7, 20000, 333], np.int64)
