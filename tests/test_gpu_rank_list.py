@@ -20,7 +20,7 @@ def kb():
 
 TUNINGS = {"default": {}, "deep": DEEP, "sparse": SPARSE, "chains1": dict(DEEP, chains_per_thread=1),
            "chains4": dict(DEEP, chains_per_thread=4),
-           # the write-free level 0 (log + windowed scatter), forced at small sizes
+           # the write-free level 0 (log, radix partition by element, dense placement), forced at small sizes
            "log": dict(DEEP, level0_mode=2), "log_sparse": dict(SPARSE, level0_mode=2),
            "log_chains1": dict(DEEP, level0_mode=2, chains_per_thread=1),
            "log_chains4": dict(DEEP, level0_mode=2, chains_per_thread=4),
