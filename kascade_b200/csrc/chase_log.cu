@@ -374,21 +374,23 @@ __global__ void __launch_bounds__(PT_THREADS, BLOCKS) k_partition(const LogEnt* 
 
 // Place: one sub-window (SUB elements) per block iteration.  Its entries
 // (element, root, rank) are read in order and placed in shared memory by
-// element, then the sub-window's outputs are written densely.  Elements without an entry were reached by no chain: their root
-// output becomes NOT_REACHED and they join the unreached list (or, when
-// every list head is a ruler, they lie on a ruler-free cycle).
+// element, then the sub-window's outputs are written densely.  Elements
+// without an entry were reached by no chain: their root output becomes
+// NOT_REACHED and they join the unreached list (or, when every list head is
+// a ruler, they lie on a ruler-free cycle).  A batch's roots are written
+// relative to their instance.
 __global__ void __launch_bounds__(FIN_THREADS, 2) k_place(const LogEnt* __restrict__ part2,
                                                             const uint32_t* __restrict__ cursor2, uint32_t nb,
                                                             uint32_t limit, uint32_t n,
                                                             const uint32_t* __restrict__ beyond, int heads_are_rulers,
                                                             uint64_t* __restrict__ root_out,
-                                                            uint64_t* __restrict__ rank_out, uint32_t* __restrict__ ulist,
+                                                            uint64_t* __restrict__ rank_out,
+                                                            uint32_t* __restrict__ ulist,
                                                             uint32_t* __restrict__ ucount, uint32_t ucap,
                                                             const uint64_t* __restrict__ seg_off,
                                                             const uint32_t* __restrict__ hint, uint32_t nseg,
                                                             DevStatus* st) {
-  // a batch reports roots relative to their instance
-  const SinkBatch inst{nullptr, nullptr, 0, seg_off, hint, nseg};
+  const SinkBatch inst{nullptr, nullptr, 0, seg_off, hint, nseg};  // instance offsets of a batch
   extern __shared__ __align__(16) unsigned char smraw[];
   unsigned long long* rank_s = reinterpret_cast<unsigned long long*>(smraw);  // SUB entries
   uint32_t* root_s = reinterpret_cast<uint32_t*>(rank_s + SUB);               // SUB entries
@@ -433,8 +435,9 @@ __global__ void __launch_bounds__(FIN_THREADS, 2) k_place(const LogEnt* __restri
       if (i < len) {
         const uint32_t r = root_s[i];
         un = r == NO_ROOT;
-        const unsigned long long base = (seg_off && !un) ? inst.base_of(lo + i) : 0ull;
-        __stcs(reinterpret_cast<unsigned long long*>(root_out) + lo + i, un ? NOT_REACHED : (unsigned long long)r - base);
+        const unsigned long long ibase = (seg_off && !un) ? inst.base_of(lo + i) : 0ull;
+        __stcs(reinterpret_cast<unsigned long long*>(root_out) + lo + i,
+               un ? NOT_REACHED : (unsigned long long)r - ibase);
         __stcs(reinterpret_cast<unsigned long long*>(rank_out) + lo + i, un ? 0ull : rank_s[i]);
       }
       const uint32_t m = __ballot_sync(FULL, un);
