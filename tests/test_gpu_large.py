@@ -65,3 +65,36 @@ def test_forest_2_26(kb, kind, blocks, spine):
     assert bool((root[nr] == root[par[nr]]).all())
     if kind == 1:
         assert int(depth.max()) >= spine - 1
+
+
+def test_many_lists_2_26(kb):
+    """About 2^20 lists over 2^26 elements on the default (write-free) path:
+    every list head before its first ruler walks to it, in every window."""
+    n = 1 << 26
+    g = torch.Generator(device="cuda")
+    g.manual_seed(0xC5)
+    perm = torch.randperm(n, device="cuda", generator=g)
+    tail = torch.rand(n, device="cuda", generator=g) < (1.0 / 64)
+    tail[-1] = True
+    nxt = torch.roll(perm, -1)
+    succ = torch.where(tail, perm, nxt)
+    succ_by_elem = torch.empty_like(succ)
+    succ_by_elem[perm] = succ
+    w = kb.gen_weights(n, 0xC6, 16)
+    root, rank = kb.rank_list(succ_by_elem, w)
+    _check_list(succ_by_elem, w, root, rank)
+    assert int((succ_by_elem == torch.arange(n, device="cuda")).sum()) == int(tail.sum())
+
+
+def test_batch_2_25_write_free_equals_stamping(kb):
+    """A batch of 2^25 records (lists and forests) on its default write-free
+    level 0 gives exactly the stamping level 0's results."""
+    sizes, kinds = kb.batch_sizes(512, 0xC7, lo_log2=8, hi_log2=21, total=(1 << 25) + 4097)
+    inputs, w = kb.gen_batch(sizes, kinds, seed=0xC8)
+    segs = kb.make_segments(sizes, kinds)
+    ctx = kb.Context()
+    root, rank = kb.rank_batch(inputs, segs, w, ctx=ctx, tuning=kb.GpuTuning(profile=True))
+    assert "place" in ctx.kernel_times()  # the write-free path ran
+    root_s, rank_s = kb.rank_batch(inputs, segs, w, tuning=kb.GpuTuning(level0_mode=1))
+    assert torch.equal(root, root_s) and torch.equal(rank, rank_s)
+    ctx.close()
