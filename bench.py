@@ -68,6 +68,13 @@ SECTORS_LIST = {True: 0.25 + 0.125 + 0.5 + 2 + 2, False: 0.25 + 0.5 + 2 + 2}
 # ruler lookups hit L1 for the most part and are left out); partition: read +
 # write (1/2 + 1/2); place: read (1/2) + root and rank writes (1/2).
 SECTORS_LIST_LOG = {True: 0.25 + 0.125 + 0.5 + 1.5 + 1 + 1 + 1, False: 0.25 + 0.5 + 1.5 + 1 + 1 + 1}
+# DRAM bytes the write-free pipeline's kernels move, measured by ncu on a
+# weighted 2^25-element list (dram__bytes_read.sum + dram__bytes_write.sum;
+# profiles/write_free_level0_list25_ncu.md): per element for the streaming
+# kernels, per record read for the chase.  Scaled to a run, they give the
+# traffic the pipeline really moves (the measured form of "sectors touched").
+DRAM_PER_ELEM_LOG = {"prepare": (402.7e6 + 480.9e6) / 2**25, "resolve": (554.3e6 + 480.4e6) / 2**25,
+                     "partition": (537.1e6 + 480.8e6) / 2**25, "place": (537.0e6 + 480.8e6) / 2**25}
 # DRAM bytes the level-0 chase moves per record it reads, from ncu
 # (dram__bytes_read.sum + dram__bytes_write.sum of the level-0 k_chase launch
 # on a 2^25-element list: 3.924 GB + 1.036 GB over 2^25 + 2 797 812 record
@@ -600,6 +607,15 @@ def main():
                          "floor_ms": round(floor_ms, 3), "frac": round(floor_ms / ms_per_step, 4),
                          "sectors_min_design": sectors_min, "frac_min_design": round(floor_min_ms / ms_per_step, 4),
                          "peak_gbs": hbm}
+        if write_free and weighted:
+            # measured traffic of the level-0 kernels (deeper levels, ~2%, left out)
+            visits = sum(levels[:2]) if len(levels) > 1 else n
+            dram = n * sum(DRAM_PER_ELEM_LOG.values()) + visits * CHASE_LOG_DRAM_BYTES_PER_VISIT
+            random_access["measured"] = {
+                "bytes_per_element": round(dram / n, 1), "sectors_per_element": round(dram / n / 32, 2),
+                "achieved_gbs": round(dram / (ms_per_step / 1000.0) / 1e9, 1),
+                "frac": round(dram / (ms_per_step / 1000.0) / 1e9 / hbm, 4),
+                "source": "ncu DRAM bytes per kernel on a 2^25 list, scaled by elements and chase visits"}
 
     # end-to-end through the host-buffer API (pinned host memory)
     e2e = None
