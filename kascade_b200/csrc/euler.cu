@@ -15,6 +15,12 @@
 // coalesced pass over slots 0..n-1.  Rotation at a vertex: parent first, then
 // children in increasing id; the tour of a tree starts at the down edge to
 // the root's first child and ends in the root's terminal slot.
+//
+// A single forest's tour build reads each vertex's first child from a table
+// (read-only random access), writes the down records in sorted order and
+// stages the up records in sorted order; place_records then moves them to
+// their vertices' slots with two radix passes and a dense placement, so no
+// record is written at a random address.
 #include "ranker.cuh"
 #include "sort.cuh"
 
@@ -40,16 +46,14 @@ __global__ void __launch_bounds__(256) k_seg_bounds(const uint32_t* __restrict__
   }
 }
 
-// A single forest: the position of each parent's first child goes into the
-// tag word of that parent's up record (slot p), which the tour build then
-// reads and overwrites in one go (one sector, read then written back)
-// instead of reading a separate segment table.
+// A single forest: fc[p] = position of p's first child in the sorted array
+// (NO_CHILD where p has none).
 constexpr uint32_t NO_CHILD = 0xFFFFFFFFu;
-__global__ void __launch_bounds__(256) k_first_child(const uint32_t* __restrict__ keys, uint32_t n,
-                                                     Rec* __restrict__ rec) {
+__global__ void __launch_bounds__(256) k_first_child_table(const uint32_t* __restrict__ keys, uint32_t n,
+                                                           uint32_t* __restrict__ fc) {
   for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t k = keys[q];
-    if (q == 0 || keys[q - 1] != k) rec[k].c = (uint32_t)q;
+    if (q == 0 || keys[q - 1] != k) fc[k] = (uint32_t)q;
   }
 }
 
@@ -91,14 +95,21 @@ struct SlotsBatch {
   __device__ __forceinline__ uint32_t thresh(uint32_t j) const { return __ldg(fthresh + j); }
 };
 
+// Where the tour build finds a vertex's first child and puts its up record.
+enum TourMode {
+  TOUR_SEG = 0,    // first child from the segment table; up record to its slot (batches)
+  TOUR_STAGED = 1  // first child from a table; up record staged in sorted order for place_records
+};
+
 // Writes both tour records of every sorted entry q, samples rulers among the
 // written slots and numbers them (one atomic per tile, as in prepare).
-template <class Slots, bool FIRST_IN_REC>
+template <class Slots, int MODE>
 __global__ void __launch_bounds__(256) k_tour_build(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
                                                     uint32_t n, const uint2* __restrict__ seg,
                                                     const uint32_t* __restrict__ root_bits, Rec* __restrict__ rec,
                                                     uint32_t* __restrict__ ruler_elem, uint32_t* __restrict__ counter,
-                                                    uint32_t salt, Slots slots, DevStatus* st) {
+                                                    uint32_t salt, Slots slots, const uint32_t* __restrict__ fc,
+                                                    uint4* __restrict__ stage, DevStatus* st) {
   __shared__ uint32_t sm[33];
   __shared__ uint32_t sbase;
   const uint64_t tile_sz = (uint64_t)blockDim.x * TB_ITEMS;
@@ -137,8 +148,8 @@ __global__ void __launch_bounds__(256) k_tour_build(const uint32_t* __restrict__
         su[i] = slot_up;
         // down edge p -> c: descend to c's first child, else come back up
         uint32_t first_child = NO_CHILD;
-        if (FIRST_IN_REC) {
-          first_child = __ldcg(&rec[slot_up].c);  // c's own up slot, rewritten below
+        if (MODE == TOUR_STAGED) {
+          first_child = __ldg(fc + c);
         } else {
           const uint2 sg = seg[c];
           if (sg.x < sg.y) first_child = sg.x;
@@ -193,7 +204,10 @@ __global__ void __launch_bounds__(256) k_tour_build(const uint32_t* __restrict__
         }
         id++;
       }
-      rec[su[i]] = ru[i];
+      if (MODE == TOUR_STAGED)
+        __stcs(stage + q, make_uint4(su[i], ru[i].b, ru[i].c, (uint32_t)ru[i].a));
+      else
+        rec[su[i]] = ru[i];
       rec[sd[i]] = rd[i];
     }
     __syncthreads();
@@ -298,23 +312,30 @@ kascade_status root_forest_impl(kascade_ctx& ctx, const uint64_t* parent, uint32
   Rec* rec = alloc<Rec>(ctx, m);
   uint32_t* ruler_elem = alloc<uint32_t>(ctx, m);
   uint32_t* ctr = alloc<uint32_t>(ctx, 1);
-  if (!rec || !ruler_elem || !ctr) return KASCADE_ERR_OOM;
+  uint32_t* fc = alloc<uint32_t>(ctx, n);
+  uint4* stage = alloc<uint4>(ctx, ((uint64_t)n + 8191) / 8192 * 8192);
+  if (!rec || !ruler_elem || !ctr || !fc || !stage) return KASCADE_ERR_OOM;
   KS_CUDA(cudaMemsetAsync(ctr, 0, sizeof(uint32_t), s));
   {
-    // up slots start with "no child"; every parent then records its first child
+    // every parent records its first child's position; the rest stay "no child"
     ProfScope ps(ctx, "seg_bounds", s);
-    KS_CUDA(cudaMemsetAsync(rec, 0xFF, sizeof(Rec) * (size_t)n, s));
-    k_first_child<<<grid_for(ctx, n, 256, 8), 256, 0, s>>>(keys, n, rec);
+    KS_CUDA(cudaMemsetAsync(fc, 0xFF, sizeof(uint32_t) * (size_t)n, s));
+    k_first_child_table<<<grid_for(ctx, n, 256, 8), 256, 0, s>>>(keys, n, fc);
     KS_CHECK_LAUNCH();
   }
   {
+    // down records straight to their slots (sorted order); up records staged
+    // in sorted order, then placed at their vertices' slots by radix passes:
+    // the only random access left is the read-only first-child lookup
     ProfScope ps(ctx, "tour_build", s);
     const unsigned grid = grid_for(ctx, ((uint64_t)n + 256 * TB_ITEMS - 1) / (256 * TB_ITEMS) * 256, 256, 8);
     SlotsSingle slots{n, (uint32_t)(4294967296.0 / (double)(p.spacing0 < 2 ? 2 : p.spacing0))};
-    k_tour_build<SlotsSingle, true><<<grid, 256, 0, s>>>(keys, vals, n, nullptr, root_bits, rec, ruler_elem, ctr,
-                                                   mix32(p.seed ^ 0x70757254u), slots, ctx.d_status);
+    k_tour_build<SlotsSingle, TOUR_STAGED><<<grid, 256, 0, s>>>(keys, vals, n, nullptr, root_bits, rec, ruler_elem,
+                                                                ctr, mix32(p.seed ^ 0x70757254u), slots, fc, stage,
+                                                                ctx.d_status);
     KS_CHECK_LAUNCH();
   }
+  KS_TRY(place_records(ctx, stage, n, rec, s));
   SinkTour sink{root_out, depth_out, n, keep_roots};
   if (device_levels && m > p.base_max && p.max_levels > 0) {
     if (m < p.level0_log_min)
@@ -341,8 +362,8 @@ kascade_status batch_tours(kascade_ctx& ctx, const uint64_t* fpar, uint32_t F, c
   SlotsBatch slots{fd, foff, fthresh, nf, down_base};
   ProfScope ps(ctx, "tour_build", s);
   const unsigned grid = grid_for(ctx, ((uint64_t)F + 256 * TB_ITEMS - 1) / (256 * TB_ITEMS) * 256, 256, 8);
-  k_tour_build<SlotsBatch, false><<<grid, 256, 0, s>>>(keys, vals, F, seg, root_bits, rec, ruler_elem, counter, salt,
-                                                        slots, ctx.d_status);
+  k_tour_build<SlotsBatch, TOUR_SEG><<<grid, 256, 0, s>>>(keys, vals, F, seg, root_bits, rec, ruler_elem, counter,
+                                                           salt, slots, nullptr, nullptr, ctx.d_status);
   KS_CHECK_LAUNCH();
   return KASCADE_OK;
 }
