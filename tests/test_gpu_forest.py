@@ -72,6 +72,21 @@ def test_generated_forests(kb, oracle_mod, n, kind, blocks, spine):
     np.testing.assert_array_equal(host_u64(depth), depth_o)
 
 
+@pytest.mark.parametrize("level0_mode", [0, 2])
+@pytest.mark.parametrize("kind,blocks,spine", [(0, 40, 0), (1, 4, 1 << 18)])
+def test_forest_several_placement_windows(kb, oracle_mod, level0_mode, kind, blocks, spine):
+    """Forests whose up records span several 2^20-slot windows of the tour
+    placement (the last one partial), random recursive trees and deep
+    caterpillars, on both level-0 paths of the tour ranking, against the
+    oracle."""
+    n = 3 * (1 << 20) + 777
+    par_h = oracle_mod.gen_forest(n, 0xC9, kind, blocks, spine)
+    root_o, depth_o = oracle_mod.root_forest(par_h)
+    root, depth = kb.root_forest(dev64(par_h), tuning=kb.GpuTuning(level0_mode=level0_mode))
+    np.testing.assert_array_equal(host_u64(root), root_o)
+    np.testing.assert_array_equal(host_u64(depth), depth_o)
+
+
 def test_compute_euler_tour_kat(kb, kat):
     e = kat["euler_tour_small"]
     tour = kb.compute_euler_tour(dev64(np.array(e["parent"], np.uint64)))
