@@ -122,3 +122,25 @@ def test_root_forest_host(kb, oracle_mod):
     root, depth = kb.root_forest_host(par)
     np.testing.assert_array_equal(root, root_o)
     np.testing.assert_array_equal(depth, depth_o)
+
+
+@pytest.mark.parametrize("level0_mode", [0, 2])
+def test_forest_with_rootless_cycle_reports_error(kb, oracle_mod, level0_mode):
+    """Parents that close a cycle without a root (not a forest): the call
+    reports an error status instead of a result, for a short cycle (likely
+    without a ruler) and a long one, and the context stays usable."""
+    rng = np.random.default_rng(0xCA)
+    ctx = kb.Context()
+    for k in (3, 40_000):
+        par = oracle_mod.gen_forest(200_000, 0xCB, 0, 8).copy()
+        cyc = rng.permutation(200_000)[:k].astype(np.uint64)
+        par[cyc] = np.roll(cyc, -1)
+        with pytest.raises(kb.KascadeError) as e:
+            kb.root_forest(dev64(par), tuning=kb.GpuTuning(level0_mode=level0_mode), ctx=ctx)
+        assert e.value.name in ("CYCLE", "NOT_A_LIST")
+    good = oracle_mod.gen_forest(100_000, 0xCC, 0, 8)
+    root_o, depth_o = oracle_mod.root_forest(good)
+    root, depth = kb.root_forest(dev64(good), ctx=ctx)
+    np.testing.assert_array_equal(host_u64(root), root_o)
+    np.testing.assert_array_equal(host_u64(depth), depth_o)
+    ctx.close()
