@@ -216,3 +216,29 @@ def test_batch_size_classes_and_errors(kb, oracle_mod):
         kb.rank_batch(inputs, segs, w, ctx=ctx)
     assert e.value.name == "INVALID_ARG"
     ctx.close()
+
+
+def test_batch_write_free_errors(kb, oracle_mod):
+    """Invalid instances in a batch on the write-free level 0: an out-of-range
+    successor, and a forest whose parents close a rootless cycle, report
+    their error status; a valid batch afterwards is exact."""
+    sizes = np.array([5000, 3000, 20000, 64], np.int64)
+    kinds = np.array([kb.SEG_LIST, kb.SEG_FOREST, kb.SEG_LIST, kb.SEG_FOREST])
+    inputs, w = kb.gen_batch(sizes, kinds, seed=61)
+    segs = kb.make_segments(sizes, kinds)
+    t = kb.GpuTuning(level0_mode=2)
+    ctx = kb.Context()
+    bad = inputs.clone()
+    bad[10] = int(sizes[0]) + 3
+    with pytest.raises(kb.KascadeError) as e:
+        kb.rank_batch(bad, segs, w, tuning=t, ctx=ctx)
+    assert e.value.name == "OUT_OF_RANGE"
+    cyc = inputs.clone()
+    off = int(sizes[0])  # the first forest
+    cyc[off + 0], cyc[off + 1], cyc[off + 2] = 1, 2, 0
+    with pytest.raises(kb.KascadeError) as e:
+        kb.rank_batch(cyc, segs, w, tuning=t, ctx=ctx)
+    assert e.value.name in ("CYCLE", "NOT_A_LIST")
+    root, rank = kb.rank_batch(inputs, segs, w, tuning=t, ctx=ctx)
+    _check(kb, oracle_mod, inputs, w, sizes, kinds, root, rank)
+    ctx.close()
