@@ -129,7 +129,7 @@ KASCADE_API int kascade_ctx_last_levels(kascade_ctx* ctx, uint64_t* sizes, int c
  *   root_out  root of i;  rank_out: sum of weights from i to its root,
  *             excluding the root (0 at roots)
  * Replaces: set_initial_ranking_state + sparse_ruling_set / pointer_doubling
- * (lib/kascade/list_ranking.hpp:83-86, sparse_ruling_set.hpp:13-18,
+ * (lib/kascade/list_ranking.hpp:47-50, sparse_ruling_set.hpp:13-18,
  * pointer_doubling.hpp:18-23); outputs must not alias succ.
  * ------------------------------------------------------------------------- */
 KASCADE_API kascade_status kascade_rank_list(kascade_ctx* ctx, const uint64_t* succ,
@@ -159,11 +159,11 @@ KASCADE_API kascade_status kascade_sparse_ruling_set(kascade_ctx* ctx, const kas
 KASCADE_API kascade_status kascade_pointer_doubling(kascade_ctx* ctx, const kascade_opts* opts,
                                                     uint64_t* succ_array, int64_t* rank_array,
                                                     uint64_t n, void* stream);
-/* kascade::rank_on_root / local_pointer_chasing (list_ranking.hpp:55-64):
+/* kascade::rank_on_root / local_pointer_chasing (list_ranking.hpp:19-28):
  * the GatherChase contract, forests of trees allowed */
 KASCADE_API kascade_status kascade_rank_on_root(kascade_ctx* ctx, uint64_t* succ_array,
                                                 int64_t* rank_array, uint64_t n, void* stream);
-/* kascade::set_initial_ranking_state (list_ranking.hpp:83-86, .cpp:148-168):
+/* kascade::set_initial_ranking_state (list_ranking.hpp:47-50, .cpp:60-80):
  * root := succ, rank := 1 (0 at roots) */
 KASCADE_API kascade_status kascade_set_initial_ranking_state(kascade_ctx* ctx, const uint64_t* succ,
                                                              uint64_t* root_array,
@@ -176,13 +176,17 @@ KASCADE_API kascade_status kascade_is_list(kascade_ctx* ctx, const uint64_t* suc
 
 /* ----------------------------------------------------------------------------
  * Result statistics on the device: the bench's compute_stats
- * (bench/detail/stats.hpp:9-50, bench/detail/stats.cpp:24-162) over root and
+ * (bench/detail/stats.hpp:9-49, bench/detail/stats.cpp:24-162) over root and
  * rank arrays (a ranking's or a rooting's output).  Level values are the
  * reference's StatsLevel.  Basic: trees = elements with root[i] == i, max and
  * mean rank.  Extensive (both levels): per tree (keyed by root) size, rank sum
  * and max rank, reduced to the counts and means below; EXTENSIVE also lists
  * the non-trivial trees (size > 1) into per_tree (device memory, up to
  * per_tree_cap entries, ordered by root; *per_tree_count = how many exist).
+ * As in the reference: a tree's max_rank starts at 0 (TreeStats,
+ * stats.hpp:23-27), so a tree of negative ranks reports 0; avg_rank divides
+ * the rank sum taken as an unsigned 64-bit value (the std::size_t fold of
+ * stats.cpp:124-137) by n.
  * ---------------------------------------------------------------------------*/
 typedef enum {
   KASCADE_STATS_NONE = 1,
@@ -236,7 +240,7 @@ KASCADE_API kascade_status kascade_root_forest_host(kascade_ctx* ctx, const uint
                                                     void* stream);
 /* In-place form of kascade::rank_via_euler_tour: succ_array holds parents on
  * input and roots on output, rank_array receives depths; roots keep their
- * input values (eulertour.cpp:270-313 writes non-roots only). */
+ * input values (eulertour.cpp:249-277 writes non-roots only). */
 KASCADE_API kascade_status kascade_rank_via_euler_tour(kascade_ctx* ctx, const kascade_opts* opts,
                                                        uint64_t* succ_array, int64_t* rank_array,
                                                        uint64_t n, void* stream);

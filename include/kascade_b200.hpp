@@ -4,13 +4,13 @@
 //
 //  reference                                      here
 //  kascade::set_initial_ranking_state(...)        set_initial_ranking_state(ctx, ...)
-//    (lib/kascade/list_ranking.hpp:83-86)
+//    (lib/kascade/list_ranking.hpp:47-50)
 //  kascade::sparse_ruling_set(cfg, succ, rank..)  sparse_ruling_set(ctx, opts, succ, rank)
 //    (lib/kascade/sparse_ruling_set.hpp:13-18)
 //  kascade::pointer_doubling(cfg, succ, rank..)   pointer_doubling(ctx, opts, succ, rank)
 //    (lib/kascade/pointer_doubling.hpp:18-23)
 //  kascade::rank_on_root / local_pointer_chasing  rank_on_root(ctx, succ, rank)
-//    (lib/kascade/list_ranking.hpp:55-64)
+//    (lib/kascade/list_ranking.hpp:19-28)
 //  kascade::rank_via_euler_tour(cfg, succ, rank)  rank_via_euler_tour(ctx, opts, succ, rank)
 //    (lib/kascade/eulertour.hpp:22-27)
 //  kascade::compute_euler_tour(parent, comm, hd)  compute_euler_tour(ctx, parent, tour)
@@ -153,7 +153,7 @@ inline Ranked root_forest_host(Context& c, std::span<const idx_t> parent, const 
 // The reference benchmark's plug-in interface (bench/detail/algorithm.hpp:
 // 7-20), implemented on the GPU: ingest a successor (or, for EulerTour, a
 // parent) array, run, read roots and ranks -- exactly what GatherRank
-// (bench/detail/algorithm_impl.hpp:101-109) produces for the same input.
+// (bench/detail/algorithm_impl.hpp:81-89) produces for the same input.
 class B200Ranking {
  public:
   explicit B200Ranking(Algorithm a = Algorithm::SparseRulingSet, int device = 0) : algo_(a), ctx_(device) {}

@@ -298,7 +298,7 @@ def root_forest_host(parent: np.ndarray, *, tuning: Optional[GpuTuning] = None, 
 # ---------------------------------------------------------------------------
 def set_initial_ranking_state(succ_array: torch.Tensor, root_array: Optional[torch.Tensor] = None,
                               rank_array: Optional[torch.Tensor] = None, ctx: Optional[Context] = None):
-    """list_ranking.hpp:83-86: root := succ, rank := 1 (0 at roots)."""
+    """list_ranking.hpp:47-50: root := succ, rank := 1 (0 at roots)."""
     _dev64(succ_array, "succ_array")
     n = succ_array.numel()
     root_array = root_array if root_array is not None else torch.empty(n, dtype=torch.int64, device=succ_array.device)
@@ -356,12 +356,12 @@ def rma_pointer_doubling(config, succ_array: torch.Tensor, rank_array: torch.Ten
 
 
 def rank_on_root(succ_array: torch.Tensor, rank_array: torch.Tensor, ctx: Optional[Context] = None) -> None:
-    """kascade::rank_on_root (list_ranking.hpp:55-58): GatherChase contract."""
+    """kascade::rank_on_root (list_ranking.hpp:19-22): GatherChase contract."""
     _inplace(lib.kascade_rank_on_root, "kascade_rank_on_root", None, succ_array, rank_array, ctx)
 
 
 def local_pointer_chasing(succ_array: torch.Tensor, rank_array: torch.Tensor, ctx: Optional[Context] = None) -> None:
-    """kascade::local_pointer_chasing (list_ranking.hpp:60): same contract."""
+    """kascade::local_pointer_chasing (list_ranking.hpp:24): same contract."""
     rank_on_root(succ_array, rank_array, ctx)
 
 
@@ -380,7 +380,7 @@ STATS_NONE, STATS_BASIC, STATS_REDUCED_EXTENSIVE, STATS_EXTENSIVE = 1, 2, 3, 4
 
 def compute_stats(root_array: torch.Tensor, rank_array: torch.Tensor, level: int = STATS_EXTENSIVE,
                   ctx: Optional[Context] = None):
-    """The bench's compute_stats (bench/detail/stats.hpp:46-50) on the device:
+    """The bench's compute_stats (bench/detail/stats.hpp:46-49) on the device:
     (figures dict, non-trivial trees as an (k, 4) int64 array of root, size,
     max rank, rank sum ordered by root; empty below STATS_EXTENSIVE)."""
     _dev64(root_array, "root_array")

@@ -1,7 +1,7 @@
 // Tree rooting via an Euler tour of the forest.
 //
 // Reference: rank_via_euler_tour / compute_euler_tour_impl / map_euler_tour_back
-// (lib/kascade/eulertour.cpp:68-162, 230-313, 372-427) with the forest built
+// (lib/kascade/eulertour.cpp:33-127, 235-278, 337-392) with the forest built
 // by reverse_rooted_tree + make_graph (lib/kascade/successor_utils.cpp:236-300).
 //
 // Layout used for ranking (m = 2n elements):

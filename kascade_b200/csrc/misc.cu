@@ -30,7 +30,7 @@ __global__ void __launch_bounds__(256) k_gen_forest(uint64_t n, ks_perm perm, ui
   }
 }
 
-// list_ranking.cpp:148-168
+// list_ranking.cpp:60-80
 __global__ void __launch_bounds__(256) k_initial_state(const uint64_t* __restrict__ succ, uint64_t n,
                                                        uint64_t* __restrict__ root, int64_t* __restrict__ rank) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {

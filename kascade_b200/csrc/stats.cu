@@ -1,5 +1,5 @@
 // Device-side result statistics: the bench's compute_stats
-// (bench/detail/stats.cpp:110-162 basic, 24-108 per tree) over root and rank
+// (bench/detail/stats.cpp:110-143 basic, 24-108 per tree) over root and rank
 // arrays already in HBM.
 //
 //   pass 1  per element: warp-level aggregation of (size, rank sum, max rank)
@@ -9,6 +9,12 @@
 //   pass 2  per root: the extensive figures (trees, non-trivial trees, size
 //           and rank sums, max size) and a root-ordered list of the
 //           non-trivial trees (stream compaction by one exclusive scan)
+//
+// Semantics kept from the reference, quirks included: a tree's max_rank
+// starts at 0 (TreeStats, bench/detail/stats.hpp:23-27, updated with
+// std::max at stats.cpp:38), so a tree whose ranks are all negative reports
+// 0; the basic average divides the rank sum taken as an unsigned 64-bit value
+// (stats.cpp:124-137 fold into std::size_t) by n.
 #include <algorithm>
 #include <climits>
 #include <cstring>
@@ -100,7 +106,7 @@ __global__ void __launch_bounds__(256) k_stats_fill(unsigned long long* __restri
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
     tsize[i] = 0;
     tsum[i] = 0;
-    tmax[i] = LLONG_MIN;
+    tmax[i] = 0;  // TreeStats::max_rank = 0
   }
 }
 
@@ -208,7 +214,9 @@ kascade_status compute_stats(kascade_ctx& ctx, const uint64_t* root, const int64
   std::memset(out, 0, sizeof(*out));
   out->num_trees = h.num_roots;
   out->max_rank = n ? h.max_rank : 0;
-  out->avg_rank = safe_div((double)(long long)h.rank_sum, (double)n);
+  // the reference folds the int64 ranks into a std::size_t sum and divides
+  // that unsigned value (stats.cpp:124-137)
+  out->avg_rank = safe_div((double)h.rank_sum, (double)n);
   if (extensive) {
     out->ext_num_trees = h.trees;
     out->num_nontrivial_trees = h.nontrivial;

@@ -23,7 +23,7 @@
 
 #define ORACLE_API __attribute__((visibility("default")))
 
-/* list_ranking.cpp:148-168 (set_initial_ranking_state): root := succ,
+/* list_ranking.cpp:60-80 (set_initial_ranking_state): root := succ,
  * rank := 1, and 0 for roots. */
 ORACLE_API void oracle_set_initial_ranking_state(const uint64_t* succ, uint64_t n, uint64_t* root,
                                                  int64_t* rank) {
@@ -129,7 +129,7 @@ ORACLE_API int oracle_pointer_doubling(uint64_t* succ, int64_t* rank, uint64_t n
 /* Weighted list ranking in the clean form: weight[i] is the distance from i to
  * succ[i] (NULL = unit weights); a root's weight is ignored.  Output:
  * root[i], rank[i] = sum of weights on the path from i to its root, excluding
- * the root (0 at roots).  Initial state as list_ranking.cpp:148-168 with
+ * the root (0 at roots).  Initial state as list_ranking.cpp:60-80 with
  * weights instead of 1, then the GatherChase walk. */
 ORACLE_API int oracle_rank_list(const uint64_t* succ, const uint32_t* weight, uint64_t n,
                                 uint64_t* root, uint64_t* rank) {
@@ -146,7 +146,7 @@ ORACLE_API int oracle_rank_list(const uint64_t* succ, const uint32_t* weight, ui
   return rc;
 }
 
-/* Tree rooting by GatherRank (bench/detail/algorithm_impl.hpp:101-109): the
+/* Tree rooting by GatherRank (bench/detail/algorithm_impl.hpp:81-89): the
  * same initial state and chase on a parent array gives each vertex its root
  * and its depth (edge count). */
 ORACLE_API int oracle_root_forest(const uint64_t* parent, uint64_t n, uint64_t* root,
@@ -176,7 +176,7 @@ ORACLE_API int oracle_is_list(const uint64_t* succ, uint64_t n) {
  *  - make_graph, successor_utils.cpp:236-260: counting sort by source that
  *    fills each source's segment from its end, so a segment holds its edges in
  *    reverse insertion order.
- *  - compute_euler_tour_impl, eulertour.cpp:68-162: edge (v, nbr_i) gets the
+ *  - compute_euler_tour_impl, eulertour.cpp:33-127: edge (v, nbr_i) gets the
  *    id xadj[v] + i; succ[(u_prev, v)] = (v, nbr_i) with
  *    u_prev = nbr_{(i-1) mod deg}; for a root v and i == 0 the successor is a
  *    dummy element (ids num_edges, num_edges+1, ... in root order) with weight
@@ -254,7 +254,7 @@ ORACLE_API uint64_t oracle_euler_tour(const uint64_t* parent, uint64_t n, uint64
   return m;
 }
 
-/* rank_via_euler_tour (eulertour.cpp:372-412) with GatherChase as the list
+/* rank_via_euler_tour (eulertour.cpp:337-377) with GatherChase as the list
  * ranker, and map_euler_tour_back (:230-313): for every up edge (v, parent)
  * root[v] = the vertex of the dummy its list ends in, rank[v] = its rank.
  * Roots keep their input values.  succ_array holds the parent array on input

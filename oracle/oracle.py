@@ -12,7 +12,7 @@ ORACLE_SO = HERE / "_build" / "libkascade_oracle.so"
 REF_SO = HERE / "_ref" / "libkascade_ref.so"
 
 __all__ = [
-    "compute_stats",
+    "compute_stats", "compute_stats_transcribed",
     "build", "has_ref", "rank_list", "root_forest", "local_pointer_chasing", "pointer_doubling",
     "euler_tour", "rank_via_euler_tour", "is_list", "pack", "unpack", "gen_list", "gen_weights",
     "gen_forest", "ref_gather_rank", "ref_local_pointer_chasing",
@@ -172,7 +172,7 @@ def ref_local_pointer_chasing(succ: np.ndarray, rank: np.ndarray) -> None:
 
 
 def compute_stats(root: np.ndarray, rank: np.ndarray, level: int) -> tuple[dict, list]:
-    """The bench's compute_stats (bench/detail/stats.cpp:110-162 basic, 24-108
+    """The bench's compute_stats (bench/detail/stats.cpp:110-143 basic, 24-108
     per tree) on one rank: level 2 basic, 3 reduced extensive, 4 extensive
     (also the non-trivial trees, here ordered by root).  numpy restatement."""
     root = np.asarray(root, dtype=np.uint64)
@@ -183,18 +183,19 @@ def compute_stats(root: np.ndarray, rank: np.ndarray, level: int) -> tuple[dict,
         return out, []
     idx = np.arange(n, dtype=np.uint64)
     out["num_trees"] = int(np.count_nonzero(root == idx))  # stats.cpp:117-119 (is_root)
-    out["max_rank"] = int(rank.max())                        # stats.cpp:120-122
-    total = int(np.sum(rank, dtype=np.int64))                # stats.cpp:123-125, int64 wrap
-    out["avg_rank"] = float(total) / float(n)                # stats.cpp:133-134
+    out["max_rank"] = int(rank.max())                        # stats.cpp:121-123
+    # stats.cpp:124-126 fold into a std::size_t: the sum as an unsigned value
+    total = int(np.sum(rank.view(np.uint64), dtype=np.uint64))
+    out["avg_rank"] = float(total) / float(n)                # stats.cpp:136-137
     if level < 3:
         return out, []
     keys, inv = np.unique(root, return_inverse=True)         # one entry per tree (stats.cpp:32-39)
     size = np.bincount(inv, minlength=keys.size).astype(np.int64)
     rsum = np.zeros(keys.size, np.int64)
     np.add.at(rsum, inv, rank)
-    rmax = np.full(keys.size, np.iinfo(np.int64).min, np.int64)
+    rmax = np.zeros(keys.size, np.int64)                     # TreeStats::max_rank = 0 (stats.hpp:23-27)
     np.maximum.at(rmax, inv, rank)
-    nt = size > 1                                            # stats.cpp:58-64
+    nt = size > 1                                            # stats.cpp:58-68
     out["ext_num_trees"] = int(keys.size)
     out["num_nontrivial_trees"] = int(nt.sum())
     out["nontrivial_size_sum"] = int(size[nt].sum())
@@ -210,3 +211,67 @@ def compute_stats(root: np.ndarray, rank: np.ndarray, level: int) -> tuple[dict,
         trees = [(int(k), int(a), int(b), int(c)) for k, a, b, c in zip(keys[nt], size[nt], rmax[nt], rsum[nt])]
     return out, trees
 
+
+
+def compute_stats_transcribed(root, rank, level: int) -> tuple[dict, list]:
+    """compute_stats of bench/detail/stats.cpp transcribed statement by
+    statement for one rank (one Distribution slice = the whole array), in
+    plain Python loops for small inputs.  An independent check of the numpy
+    restatement above: a dict stands in for the absl hash map, C integer
+    widths are applied where the reference converts (std::size_t sums,
+    int64 per-tree sums), and the non-trivial trees come back ordered by root
+    (the reference's order is the hash map's iteration order, unspecified).
+    """
+    M64 = (1 << 64) - 1
+
+    def s64(x):  # two's complement int64 of a Python int
+        x &= M64
+        return x - (1 << 64) if x >> 63 else x
+
+    root = [int(x) for x in np.asarray(root, dtype=np.uint64)]
+    rank = [s64(int(x)) for x in np.asarray(rank).view(np.uint64)]
+    n = len(root)
+    if level < 2 or n == 0:  # StatsLevel::none (stats.cpp:150-152)
+        return {"num_trees": 0, "max_rank": 0, "avg_rank": 0.0}, []
+    # compute_basic_stats (stats.cpp:110-143)
+    local_num_roots = sum(1 for i in range(n) if root[i] == i)      # is_root, successor_utils.cpp:65-70
+    local_max_rank = max(rank) & M64                                # std::size_t (stats.cpp:121-123)
+    local_rank_sum = 0
+    for v in rank:                                                  # fold_left over int64 (stats.cpp:124-126)
+        local_rank_sum = s64(local_rank_sum + v)
+    global_rank_sum = local_rank_sum & M64                          # std::size_t (stats.cpp:132-134)
+    basic = {"num_trees": local_num_roots,
+             "avg_rank": float(global_rank_sum) / float(n),         # stats.cpp:136-137
+             "max_rank": s64(local_max_rank)}                       # stats.cpp:139-141
+    if level == 2:
+        return basic, []
+    # compute_per_tree_stats (stats.cpp:24-108)
+    local_stats: dict = {}
+    for i in range(n):
+        t = local_stats.setdefault(root[i], {"size": 0, "max_rank": 0, "rank_sum": 0})
+        t["size"] += 1
+        t["rank_sum"] = s64(t["rank_sum"] + rank[i])
+        t["max_rank"] = max(t["max_rank"], rank[i])
+    ext = {"ext_num_trees": 0, "num_nontrivial_trees": 0, "nontrivial_size_sum": 0, "nontrivial_rank_sum": 0,
+           "max_size": 0}
+    per_tree = []
+    for r in sorted(local_stats):
+        t = local_stats[r]
+        ext["ext_num_trees"] += 1
+        ext["max_size"] = max(ext["max_size"], t["size"])
+        if t["size"] > 1:
+            ext["num_nontrivial_trees"] += 1
+            ext["nontrivial_size_sum"] += t["size"]
+            ext["nontrivial_rank_sum"] = s64(ext["nontrivial_rank_sum"] + t["rank_sum"])
+            per_tree.append((r, t["size"], t["max_rank"], t["rank_sum"]))
+
+    def safe_division(a, b):  # stats.cpp:19-22
+        return 0.0 if b == 0 else float(a) / float(b)
+
+    trivial = ext["ext_num_trees"] - ext["num_nontrivial_trees"]
+    ext["avg_size"] = safe_division(ext["nontrivial_size_sum"] + trivial, ext["ext_num_trees"])
+    ext["nontrivial_avg_size"] = safe_division(ext["nontrivial_size_sum"], ext["num_nontrivial_trees"])
+    ext["nontrivial_avg_rank"] = safe_division(ext["nontrivial_rank_sum"], s64(ext["nontrivial_size_sum"]))
+    out = dict(basic)
+    out.update(ext)
+    return out, (per_tree if level >= 4 else [])

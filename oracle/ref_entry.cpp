@@ -16,8 +16,8 @@ extern "C" __attribute__((visibility("default"))) void ref_local_pointer_chasing
                                  std::span<kascade::rank_t>(rank, n));
 }
 
-// GatherRank (bench/detail/algorithm_impl.hpp:101-109) on one rank:
-// set_initial_ranking_state (list_ranking.cpp:148-168) then the chase.
+// GatherRank (bench/detail/algorithm_impl.hpp:81-89) on one rank:
+// set_initial_ranking_state (list_ranking.cpp:60-80) then the chase.
 extern "C" __attribute__((visibility("default"))) void ref_gather_rank(
     const std::uint64_t* succ, std::uint64_t n, std::uint64_t* root, std::int64_t* rank) {
   for (std::uint64_t i = 0; i < n; ++i) {

@@ -10,7 +10,7 @@
   kat.json         Known answers: the arrays of the reference's
                    tests/pack_test.cpp (PackTest.works on 4 ranks, concatenated
                    into one index space, and PackTest.sanity_check), and an
-                   Euler tour worked by hand from eulertour.cpp:68-162 and
+                   Euler tour worked by hand from eulertour.cpp:33-127 and
                    successor_utils.cpp:236-300.
 
 Run from the repository root with the reference tree present:
@@ -100,7 +100,7 @@ def main() -> None:
 
     kat = {
         "source": "reference tests/pack_test.cpp (PackTest.works, PackTest.sanity_check); "
-        "Euler tour worked by hand from lib/kascade/eulertour.cpp:68-162",
+        "Euler tour worked by hand from lib/kascade/eulertour.cpp:33-127",
         "pack_works": {
             # ranks 0..3 of the 4-rank test, concatenated: global indices
             # 0-7 | 8-13 | 14-15 | 16-19 (distribution.hpp block offsets)

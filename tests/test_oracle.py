@@ -129,3 +129,27 @@ def test_stats_restatement_small(oracle_mod):
     assert figs["nontrivial_avg_size"] == pytest.approx(5 / 2)
     assert figs["nontrivial_avg_rank"] == pytest.approx(6 / 5)
     assert trees == [(0, 3, 3, 4), (4, 2, 2, 2)]
+    assert oracle_mod.compute_stats_transcribed(root, rank, 4) == (figs, trees)
+
+
+@pytest.mark.parametrize("lo,hi", [(-1000, 1000), (-1000, -1), (0, 1 << 40)])
+def test_stats_restatement_equals_transcription(oracle_mod, lo, hi):
+    """The numpy restatement equals the statement-by-statement transcription
+    of stats.cpp, signed and all-negative ranks included (a tree of negative
+    ranks reports max_rank 0; a negative rank sum averages as unsigned)."""
+    rng = np.random.default_rng(lo & 0xFFFF)
+    n = 3000
+    root = rng.integers(0, 200, n).astype(np.uint64)
+    root[:200] = np.arange(200, dtype=np.uint64)
+    rank = rng.integers(lo, hi, n).astype(np.int64)
+    for level in (1, 2, 3, 4):
+        a = oracle_mod.compute_stats(root, rank, level)
+        b = oracle_mod.compute_stats_transcribed(root, rank, level)
+        assert a[0].keys() == b[0].keys()
+        for k in b[0]:
+            assert a[0][k] == b[0][k], (level, k)
+        assert a[1] == b[1]
+    if hi <= 0:
+        figs, trees = oracle_mod.compute_stats_transcribed(root, rank, 4)
+        assert all(t[2] == 0 for t in trees)
+        assert figs["avg_rank"] > 1e15
