@@ -51,10 +51,12 @@ WORKLOADS = {
 # sector for the dependent successor load.  Forest: 8 B parent + 16 B outputs
 # + 2 tour elements x (32 B random sector + 16 B streamed tour state).
 B_ALG = {"list": lambda w: 8 + (4 if w else 0) + 16 + 32, "forest": lambda w: 8 + 16 + 2 * (32 + 16)}
-# The chase kernel's own algorithmic bytes per element it visits: the
-# dependent 16 B record read lands in one random 32 B sector, and the 16 B
-# stamp it writes back.
-B_CHASE = 32 + 16
+# The chase kernel's algorithmic bytes per element it visits: the one random
+# 32 B sector its dependent 16 B record read lands in.  The implementation
+# also writes 16 B per visit (the log entry of the write-free chase, or the
+# stamp of the stamping chase); that figure is reported beside it.
+B_CHASE = 32
+B_CHASE_IMPL = 32 + 16
 # Random-access roofline, stated as 32 B sectors touched x 32 B / peak: the
 # sectors the ranking pipeline touches per level-0 list element.  prepare:
 # succ 8 B (1/4 sector) + weight 4 B (1/8) + record write 16 B (1/2); chase:
@@ -68,23 +70,24 @@ SECTORS_LIST = {True: 0.25 + 0.125 + 0.5 + 2 + 2, False: 0.25 + 0.5 + 2 + 2}
 # ruler lookups hit L1 for the most part and are left out); partition: read +
 # write (1/2 + 1/2); place: read (1/2) + root and rank writes (1/2).
 SECTORS_LIST_LOG = {True: 0.25 + 0.125 + 0.5 + 1.5 + 1 + 1 + 1, False: 0.25 + 0.5 + 1.5 + 1 + 1 + 1}
-# DRAM bytes the write-free pipeline's kernels move, measured by ncu on a
-# weighted 2^25-element list (dram__bytes_read.sum + dram__bytes_write.sum;
-# profiles/write_free_level0_list25_ncu.md): per element for the streaming
-# kernels, per record read for the chase.  Scaled to a run, they give the
-# traffic the pipeline really moves (the measured form of "sectors touched").
-DRAM_PER_ELEM_LOG = {"prepare": (402.7e6 + 480.9e6) / 2**25, "resolve": (554.3e6 + 480.4e6) / 2**25,
-                     "partition": (537.1e6 + 480.8e6) / 2**25, "place": (537.0e6 + 480.8e6) / 2**25}
-# DRAM bytes the level-0 chase moves per record it reads, from ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum of the level-0 k_chase launch
-# on a 2^25-element list: 3.924 GB + 1.036 GB over 2^25 + 2 797 812 record
-# reads, every element once plus each chain's closing ruler record; traffic
-# grows in proportion): profiles/chase_propagate_prepare_list25_ncu.md
-CHASE_DRAM_BYTES_PER_VISIT = (3.924e9 + 1.036e9) / (33_554_432 + 2_797_812)
+# DRAM bytes the write-free pipeline's kernels move, measured by ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum) on a weighted 2^25-element
+# list: per element for the streaming kernels, per record read for the chase.
+# Scaled to a run, they give the traffic the pipeline really moves (the
+# measured form of "sectors touched").
+NCU_LIST_N = 1 << 25
+DRAM_PER_ELEM_LOG = {"prepare": (402.7e6 + 480.9e6) / NCU_LIST_N, "resolve": (554.3e6 + 480.4e6) / NCU_LIST_N,
+                     "partition": (537.1e6 + 480.8e6) / NCU_LIST_N, "place": (537.0e6 + 480.8e6) / NCU_LIST_N}
+# DRAM bytes the level-0 stamping chase moves per record it reads (ncu on a
+# 2^25-element list: 3.924 GB read + 1.036 GB written over 2^25 + 2 797 812
+# record reads, every element once plus each chain's closing ruler record).
+CHASE_NCU_VISITS = NCU_LIST_N + 2_797_812
+CHASE_DRAM_BYTES_PER_VISIT = (3.924e9 + 1.036e9) / CHASE_NCU_VISITS
 # The same for the write-free chase (k_chase_log), which reads each record
 # and appends a 16 B log entry: 3.901 GB read + 0.560 GB written over 2^25 +
-# 1 048 211 record reads (profiles/write_free_level0_list25_ncu.md)
-CHASE_LOG_DRAM_BYTES_PER_VISIT = (3.900669e9 + 0.560097e9) / (33_554_432 + 1_048_211)
+# 1 048 211 record reads.
+CHASE_LOG_NCU_VISITS = NCU_LIST_N + 1_048_211
+CHASE_LOG_DRAM_BYTES_PER_VISIT = (3.900669e9 + 0.560097e9) / CHASE_LOG_NCU_VISITS
 
 
 def log(*a):
@@ -206,36 +209,95 @@ def whole_job(n_per_rank: int, t_ms_local: float, steps: int, world: int) -> tup
     return ms_per_step, n_per_rank * world / (ms_per_step / 1000.0)
 
 
-def cpu_reference_time(n_sample: int, wl: str, reps: int = 1) -> tuple[float, str, str]:
-    """The reference's own GatherChase (oracle/_ref, built from the reference
-    source) when present, else the oracle restatement; one host core."""
+def cpu_inputs(wl: str, n: int, seed: int):
+    """The workload's seeded input built on the host cores (bit-identical to
+    the device generators): (succ or parent, rank array in the reference's
+    in-place form: distance to the successor, 0 at roots)."""
     import numpy as np
 
     import oracle
 
     _, _, kind, arg, weighted = WORKLOADS[wl]
     if kind == "list":
-        succ = oracle.gen_list(n_sample, 0xC1, arg)
-        rank = (oracle.gen_weights(n_sample, 0xC1 + 1, 16).astype(np.int64) if weighted
-                else np.ones(n_sample, np.int64))
-        rank[succ == np.arange(n_sample, dtype=np.uint64)] = 0
+        succ = oracle.cpu_gen_list(n, seed, arg)
+        rank = (oracle.cpu_gen_weights(n, seed + 1, 16).astype(np.int64) if weighted else np.ones(n, np.int64))
     else:
-        succ = oracle.gen_forest(n_sample, 0xC2, arg, 64, n_sample // 128)
-        rank = np.where(succ == np.arange(n_sample, dtype=np.uint64), 0, 1).astype(np.int64)
-    use_ref = oracle.has_ref()
-    best = float("inf")
-    for _ in range(reps):
-        s, r = succ.copy(), rank.copy()
-        t0 = time.perf_counter()
-        if use_ref:
+        succ = oracle.cpu_gen_forest(n, seed, arg, 64, (n // 64) // 2 if arg == 1 else 0)
+        rank = np.ones(n, np.int64)
+    rank[succ == np.arange(n, dtype=np.uint64)] = 0
+    return succ, rank
+
+
+def cpu_time(variant: str, succ, rank, threads: int = 0):
+    """Seconds of one in-place CPU ranking of (succ, rank) on copies, and the
+    result.  Variants: the reference's own GatherChase (oracle/_ref, compiled
+    from lib/kascade/local_pointer_chasing.cpp; its restatement when absent;
+    one core), and the multi-core restatements of the sparse ruling set and
+    of pointer doubling over `threads` host threads (0 = all)."""
+    import oracle
+
+    s, r = succ.copy(), rank.copy()
+    t0 = time.perf_counter()
+    if variant == "gather_chase":
+        if oracle.has_ref():
             oracle.ref_local_pointer_chasing(s, r)
         else:
             oracle.local_pointer_chasing(s, r)
-        best = min(best, time.perf_counter() - t0)
-    return n_sample / best, ("reference" if use_ref else "port"), (
-        f"{n_sample}-element instance of the same generator, GatherChase "
-        f"(lib/kascade/local_pointer_chasing.cpp{' compiled from the reference source' if use_ref else ' restated'}),"
-        f" best of {reps}")
+    elif variant == "sparse_ruling_set":
+        oracle.cpu_sparse_ruling_set(s, r, spacing=32, threads=threads)
+    else:
+        oracle.cpu_pointer_doubling(s, r, threads=threads)
+    return time.perf_counter() - t0, s, r
+
+
+def cpu_variant_meta(variant: str, threads: int) -> tuple[str, int, str]:
+    """(kind, cores, description) of a CPU variant."""
+    import oracle
+
+    if variant == "gather_chase":
+        return (("reference" if oracle.has_ref() else "port"), 1,
+                "GatherChase, lib/kascade/local_pointer_chasing.cpp " +
+                ("compiled from the reference source" if oracle.has_ref() else "restated") + ", 1 core")
+    t = threads or oracle.cpu_threads()
+    name = {"sparse_ruling_set": "sparse ruling set (post-invert chase from rulers and leaves, recursion, pull "
+                                 "propagation)", "pointer_doubling": "synchronous pointer doubling"}[variant]
+    return "port", t, f"multi-core CPU restatement of the reference's {name}, {t} threads"
+
+
+def cpu_baseline(wl: str, n: int, seed: int, full=None, sample_n: int = 1 << 24, check=None) -> dict:
+    """The best of the reference's CPU variants on the host cores: the
+    multi-core sparse ruling set on the full workload (`full` = its host
+    arrays, else generated here), the sequential GatherChase and multi-core
+    pointer doubling on a `sample_n`-element instance of the same generator.
+    `check` = (root, rank) host arrays of the GPU result of the full
+    workload, compared with the CPU ruling set's result."""
+    import numpy as np
+
+    _, _, kind, _, _ = WORKLOADS[wl]
+    variants = {}
+    if kind == "list":
+        succ, rank = full if full is not None else cpu_inputs(wl, n, seed)
+        dt, s, r = cpu_time("sparse_ruling_set", succ, rank)
+        k, c, d = cpu_variant_meta("sparse_ruling_set", 0)
+        variants["sparse_ruling_set"] = {"value": n / dt, "seconds": round(dt, 3), "n": n, "kind": k, "cores": c,
+                                         "what": d}
+        if check is not None:
+            variants["sparse_ruling_set"]["equals_gpu_result"] = bool(
+                np.array_equal(s, check[0]) and np.array_equal(r.view(np.uint64), check[1]))
+        del s, r, succ, rank
+    m = min(sample_n, n)
+    succ, rank = cpu_inputs(wl, m, seed)
+    for v in ("gather_chase", "pointer_doubling"):
+        dt, _, _ = cpu_time(v, succ, rank)
+        k, c, d = cpu_variant_meta(v, 0)
+        variants[v] = {"value": m / dt, "seconds": round(dt, 3), "n": m, "kind": k, "cores": c, "what": d}
+    best = max(variants, key=lambda v: variants[v]["value"])
+    b = variants[best]
+    return {"value": b["value"], "unit": "elements/s" if kind == "list" else "vertices/s", "cores": b["cores"],
+            "kind": b["kind"], "best": best,
+            "sample": f"{b['what']}, on a {b['n']}-element instance of the same seeded generator"
+                      + (" (the full workload)" if b["n"] == n else ""),
+            "same_config": b["n"] == n, "variants": variants}
 
 
 def calibrate(local: int) -> None:
@@ -330,11 +392,16 @@ def measure_batched(kb, ctx, dev, steps: int = 3) -> dict:
             "speedup_vs_plain": round(tp / tb, 2), "results_equal_plain": same, "graph_replay": graph}
 
 
-def measure_served(kb, dev, n_requests: int = 1000, rate: float = 20000.0, **server_kw) -> dict:
+def measure_served(kb, dev, n_requests: int = 1000, rate: float = 20000.0, batched_rate: float | None = None,
+                   **server_kw) -> dict:
     """Poisson arrivals (mean 20k req/s) of sizes
     log-uniform in [2^8, 2^24], 70% weighted lists / 30% random recursive
     forests, served under a 40 GB HBM budget with device-resident inputs;
-    p50 / p99 latency and throughput, against plain per-request calls."""
+    p50 / p99 latency and throughput, against plain per-request calls.  Every
+    served result is copied (device to device) into a result store before its
+    release and compared, on the device, with a plain call on the same input
+    after the run.  `batched_rate`: the batched form's elements/s on this
+    GPU, the served form's ceiling."""
     import numpy as np
     import torch
 
@@ -344,6 +411,11 @@ def measure_served(kb, dev, n_requests: int = 1000, rate: float = 20000.0, **ser
     arrivals = np.cumsum(rng.exponential(1.0 / rate, n_requests))
     inputs, w = kb.gen_batch(sizes, kinds, seed=0xC4, device=dev)
     offs = np.concatenate([[0], np.cumsum(sizes)])
+    total = int(sizes.sum())
+    # the result store, allocated before the run: an allocation inside it
+    # could synchronise the device and stall the lanes
+    store_root = torch.empty(total, dtype=torch.int64, device=dev)
+    store_rank = torch.empty(total, dtype=torch.int64, device=dev)
     torch.cuda.synchronize()
     kw = dict(hbm_budget=40 << 30, small_max=1 << 20, small_batch_elements=1 << 23)
     kw.update(server_kw)
@@ -358,28 +430,26 @@ def measure_served(kb, dev, n_requests: int = 1000, rate: float = 20000.0, **ser
 
     ids = [None] * n_requests
     done_q: "queue.Queue" = queue.Queue()
-    check_at = {0, n_requests // 2, n_requests - 1}
-    # destinations for the spot checks, allocated before the run: an
-    # allocation inside it could synchronise the device and stall the lanes
-    checks = {i: (torch.empty(int(sizes[i]), dtype=torch.int64, device=dev),
-                  torch.empty(int(sizes[i]), dtype=torch.int64, device=dev)) for i in check_at}
-    torch.cuda.synchronize()
+    copy_stream = torch.cuda.Stream(dev, priority=0)
     errors = []
 
     def collector():
-        # waits in submission order and releases each result once read, so
-        # the budget holds only requests in flight
-        for i in range(n_requests):
-            rid = done_q.get()
-            try:
-                srv.wait(rid, 300.0)
-                if i in check_at:
+        # waits in submission order, copies each result into the store and
+        # releases it once the copy is done, so the budget holds only
+        # requests in flight
+        with torch.cuda.stream(copy_stream):
+            for i in range(n_requests):
+                rid = done_q.get()
+                try:
+                    srv.wait(rid, 300.0)
                     r_dev, k_dev = srv.result_device(rid)
-                    checks[i][0].copy_(r_dev.view(torch.int64))
-                    checks[i][1].copy_(k_dev.view(torch.int64))
-                srv.release(rid)
-            except Exception as e:  # noqa: BLE001
-                errors.append(e)
+                    a, b = int(offs[i]), int(offs[i + 1])
+                    store_root[a:b].copy_(r_dev.view(torch.int64), non_blocking=True)
+                    store_rank[a:b].copy_(k_dev.view(torch.int64), non_blocking=True)
+                    copy_stream.synchronize()
+                    srv.release(rid)
+                except Exception as e:  # noqa: BLE001
+                    errors.append(e)
 
     th = threading.Thread(target=collector, daemon=True)
     th.start()
@@ -396,71 +466,273 @@ def measure_served(kb, dev, n_requests: int = 1000, rate: float = 20000.0, **ser
         raise RuntimeError(f"served run did not complete: {errors[:1]}")
     st = srv.stats()
     srv.close()
-    # spot-check three results against plain calls
-    ok = True
-    for i, (r_dev, k_dev) in checks.items():
-        a, b = int(offs[i]), int(offs[i + 1])
-        if kinds[i] == kb.SEG_LIST:
-            r_p, k_p = kb.rank_list(inputs[a:b], w[a:b])
-        else:
-            r_p, k_p = kb.root_forest(inputs[a:b])
-        ok &= bool(torch.equal(r_dev, r_p) and torch.equal(k_dev, k_p))
     # plain per-request calls of the same requests, back to back
     ctx = kb.Context(dev.index or 0)
     root = torch.empty(int(sizes.max()), dtype=torch.int64, device=dev)
     rk = torch.empty_like(root)
-    torch.cuda.synchronize()
-    p0 = time.perf_counter()
-    for i in range(n_requests):
+
+    def plain(i):
         a, b = int(offs[i]), int(offs[i + 1])
         n = b - a
         if kinds[i] == kb.SEG_LIST:
             kb.rank_list(inputs[a:b], w[a:b], root_out=root[:n], rank_out=rk[:n], ctx=ctx)
         else:
             kb.root_forest(inputs[a:b], root_out=root[:n], depth_out=rk[:n], ctx=ctx)
+        return a, b
+
+    torch.cuda.synchronize()
+    p0 = time.perf_counter()
+    for i in range(n_requests):
+        plain(i)
     torch.cuda.synchronize()
     tp = time.perf_counter() - p0
+    # every served result against its plain call, compared on the device
+    equal = 0
+    for i in range(n_requests):
+        a, b = plain(i)
+        equal += bool(torch.equal(store_root[a:b], root[:b - a]) and torch.equal(store_rank[a:b], rk[:b - a]))
     ctx.close()
-    total = int(sizes.sum())
-    return {"workload": f"{n_requests} requests, Poisson arrivals at {rate:.0f}/s, sizes log-uniform in [2^8,2^24], "
-                        "70% weighted lists / 30% random recursive forests, 40 GB admission budget, device-resident "
-                        "inputs",
-            "requests": n_requests, "elements": total, "req_per_s": round(st["requests_per_s"], 1),
-            "elements_per_s": st["elements_per_s"], "p50_ms": round(st["p50_ms"], 3), "p99_ms": round(st["p99_ms"], 3),
-            "p50_ms_le_2^20": round(st["p50_small_ms"], 3), "p99_ms_le_2^20": round(st["p99_small_ms"], 3),
-            "requests_le_2^20": int(st["completed_small"]), "batches": int(st["batches"]),
-            "plain_elements_per_s": total / tp, "plain_req_per_s": round(n_requests / tp, 1),
-            "throughput_vs_plain": round(st["elements_per_s"] / (total / tp), 2), "spot_check_equal": ok,
-            "lanes": {k: st[k] for k in ("lane_batches", "lane_elements", "lane_busy_ms", "lane_max_batch_ms",
-                                         "partition_sms", "partition_batches")}}
+    del store_root, store_rank, inputs, w
+    served_rate = st["elements_per_s"]
+    plain_rate = total / tp
+    out = {"workload": f"{n_requests} requests, Poisson arrivals at {rate:.0f}/s, sizes log-uniform in [2^8,2^24], "
+                       "70% weighted lists / 30% random recursive forests, 40 GB admission budget, device-resident "
+                       "inputs",
+           "requests": n_requests, "elements": total, "req_per_s": round(st["requests_per_s"], 1),
+           "elements_per_s": served_rate, "p50_ms": round(st["p50_ms"], 3), "p99_ms": round(st["p99_ms"], 3),
+           "p50_ms_le_2^20": round(st["p50_small_ms"], 3), "p99_ms_le_2^20": round(st["p99_small_ms"], 3),
+           "requests_le_2^20": int(st["completed_small"]), "batches": int(st["batches"]),
+           "plain_elements_per_s": plain_rate, "plain_req_per_s": round(n_requests / tp, 1),
+           "throughput_vs_plain": round(served_rate / plain_rate, 2),
+           "results_checked": n_requests, "results_equal_plain": equal,
+           "lanes": {k: st[k] for k in ("lane_batches", "lane_elements", "lane_busy_ms", "lane_max_batch_ms",
+                                        "partition_sms", "partition_batches")}}
+    if batched_rate:
+        # the whole GPU's batched rate bounds what serving can reach: this
+        # mix's ceiling against plain calls, and the share of it reached
+        out["ceiling_vs_plain"] = round(batched_rate / plain_rate, 2)
+        out["frac_of_batched_rate"] = round(served_rate / batched_rate, 3)
+    return out
 
 
 def run_reference(args, world, rank):
+    """The reference's CPU path on the host cores: each step one in-place
+    ranking of the full workload by the multi-core sparse ruling set (the
+    reference's own MPI binary cannot be built here), the sequential
+    GatherChase (the reference's own source, oracle/_ref) and multi-core
+    pointer doubling measured once on a 2^24-element sample; the value is the
+    best of the three.  Tree-rooting workloads have no ruling-set leg (the
+    reference's ruling set takes lists only)."""
     if rank != 0:
         return
+    import oracle
+
     wl = args.workload
-    n_sample = args.cpu_sample
+    desc, n, kind, _, _ = WORKLOADS[wl]
+    if args.n:
+        n = args.n
+    seed = 0xC1
+    succ, rk = cpu_inputs(wl, n, seed)
+    steps_variant = "sparse_ruling_set" if kind == "list" else "pointer_doubling"
+    if kind != "list":
+        succ, rk = cpu_inputs(wl, min(n, args.cpu_sample), seed)
+    m = succ.size
     for _ in range(args.warmup):
-        cpu_reference_time(n_sample // 4, wl)
-    vals = []
+        cpu_time(steps_variant, succ, rk)
+    times = []
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        v, kind, sample = cpu_reference_time(n_sample, wl)
-        vals.append(v)
+        dt, _, _ = cpu_time(steps_variant, succ, rk)
+        times.append(dt)
     wall = time.perf_counter() - t0
-    v = statistics.median(vals)
+    variants = {}
+    k, c, d = cpu_variant_meta(steps_variant, 0)
+    variants[steps_variant] = {"value": m / statistics.median(times), "n": m, "kind": k, "cores": c, "what": d,
+                               "steps": args.steps}
+    del succ, rk
+    succ, rk = cpu_inputs(wl, min(n, args.cpu_sample), seed)
+    for v in ("gather_chase", "pointer_doubling"):
+        if v in variants:
+            continue
+        dt, _, _ = cpu_time(v, succ, rk)
+        k, c, d = cpu_variant_meta(v, 0)
+        variants[v] = {"value": succ.size / dt, "n": int(succ.size), "kind": k, "cores": c, "what": d}
+    best = max(variants, key=lambda v: variants[v]["value"])
+    b = variants[best]
+    unit = "elements/s"
+    secondary = {}
+    if kind == "list" and not args.no_secondary and not args.n:
+        # tree rooting (the forests of the rooting workload): the reference's
+        # GatherRank chase on one core and multi-core pointer doubling
+        for fw in ("forest_rrt", "forest_cat"):
+            fs, fr = cpu_inputs(fw, args.cpu_sample, seed)
+            fv = {}
+            for v in ("gather_chase", "pointer_doubling"):
+                dt, _, _ = cpu_time(v, fs, fr)
+                k, c, d = cpu_variant_meta(v, 0)
+                fv[v] = {"value": fs.size / dt, "n": int(fs.size), "kind": k, "cores": c, "what": d}
+            fb = max(fv, key=lambda v: fv[v]["value"])
+            secondary[fw] = {"workload": WORKLOADS[fw][0], "value": fv[fb]["value"], "unit": "vertices/s",
+                             "best": fb, "variants": fv}
     out = {
-        "impl": "reference", "metric": METRIC, "value": v, "unit": "elements/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * wall / args.steps,
+        "impl": "reference", "metric": METRIC, "value": b["value"], "unit": unit, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * wall / max(args.steps, 1),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
-        "config": {"workload": WORKLOADS[wl][0], "n": WORKLOADS[wl][1], "sample_n": n_sample,
-                   "parallelism": "one host core (GatherChase is sequential)"},
-        "cpu_baseline": {"value": v, "unit": "elements/s", "cores": 1, "kind": kind, "sample": sample},
-        "e2e": {"value": v, "unit": "elements/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "config": {"workload": desc, "n": n, "sample_n": b["n"],
+                   "parallelism": f"{b['cores']} host thread(s), {oracle.cpu_threads()} available"},
+        "cpu_baseline": {"value": b["value"], "unit": unit, "cores": b["cores"], "kind": b["kind"],
+                         "sample": f"{b['what']}, {b['n']}-element instance of the same seeded generator"
+                                   + (" (the full workload)" if b["n"] == n else ""),
+                         "same_config": b["n"] == n, "best": best, "variants": variants},
+        "e2e": {"value": b["value"], "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "secondary": secondary or None,
         "note": "the reference's MPI binary cannot be built here (no MPI, no network for its FetchContent "
-                "dependencies); its GatherChase source compiles standalone and is what runs",
+                "dependencies, GCC 13); its GatherChase source compiles standalone (oracle/_ref) and its "
+                "sparse ruling set and pointer doubling run as multi-core CPU restatements",
     }
     print(json.dumps(out), flush=True)
+
+
+def measure_device(kb, ctx, dev, wl: str, n: int, tuning, steps: int, warmup: int, world: int, seed: int,
+                   clocks: bool = False) -> dict:
+    """Device-timed ranking of one workload with inputs resident in HBM: CUDA
+    events on the launching stream around `steps` calls (barrier and
+    synchronize on both sides), kernel times from the library's own events,
+    the dominant kernel's roofline."""
+    import torch
+
+    desc, _, kind, arg, weighted = WORKLOADS[wl]
+    stream = torch.cuda.current_stream(dev)
+    if kind == "list":
+        inp = kb.gen_list(n, seed, arg, device=dev)
+        w = kb.gen_weights(n, seed + 1, 16, device=dev) if weighted else None
+        ctx.reserve(kb.lib.kascade_scratch_bytes_rank_list(n))
+    else:
+        spine = (n // 64) // 2 if arg == 1 else 0
+        inp = kb.gen_forest(n, seed, arg, 64, spine, device=dev)
+        w = None
+        ctx.reserve(kb.lib.kascade_scratch_bytes_root_forest(n))
+    root = torch.empty(n, dtype=torch.int64, device=dev)
+    rk = torch.empty(n, dtype=torch.int64, device=dev)
+
+    def step():
+        if kind == "list":
+            kb.rank_list(inp, w, tuning=tuning, root_out=root, rank_out=rk, ctx=ctx)
+        else:
+            kb.root_forest(inp, tuning=tuning, root_out=root, depth_out=rk, ctx=ctx)
+
+    torch.cuda.synchronize()
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    ctx.reset_kernel_times()
+    sampler = ClockSampler(dev.index or 0) if clocks else None
+    if sampler:
+        sampler.start()
+        time.sleep(0.3)
+    barrier(world)
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = sampler.stop() if sampler else None
+    ms_per_step, value = whole_job(n, ev0.elapsed_time(ev1), steps, world)
+    ktimes = ctx.kernel_times()
+    levels = ctx.levels()
+    hbm, hbm_src = peaks()
+    b_alg = B_ALG[kind](weighted)
+    pipe_gbs = n * b_alg / (ms_per_step / 1000.0) / 1e9
+    return {"desc": desc, "n": n, "kind": kind, "weighted": weighted, "inp": inp, "w": w, "root": root, "rank": rk,
+            "ms_per_step": ms_per_step, "value": value, "ktimes": ktimes, "levels": levels, "clocks": clk,
+            "launches": sum(c for (_, c) in ktimes.values()),
+            "kernels_ms_per_step": {k: round(v[0] / steps, 4) for k, v in sorted(ktimes.items())},
+            "roofline": kernel_roofline(ktimes, levels, steps, kind, n, weighted, hbm, hbm_src),
+            "pipeline": {"b_alg_per_elem": b_alg, "achieved_gbs": round(pipe_gbs, 1),
+                         "frac": round(pipe_gbs / hbm, 4), "peak_gbs": hbm, "peak_source": hbm_src},
+            "write_free": "place" in ktimes}
+
+
+def kernel_roofline(ktimes, levels, steps, kind, n, weighted, hbm, hbm_src) -> dict | None:
+    """Roofline of the step's dominant kernel.  For the chase: one random
+    32 B sector per element visited (all levels' visits, over the chase
+    launches of one step); the 16 B log entry or stamp the implementation
+    writes per visit is reported beside it.  `traffic`: ncu DRAM bytes per
+    visit from a 2^25-element capture, scaled to the visits per launch."""
+    if not ktimes:
+        return None
+    dominant = max(ktimes, key=lambda k: ktimes[k][0])
+    d_ms, d_cnt = ktimes[dominant]
+    per_launch_s = d_ms / d_cnt / 1000.0
+    launches_per_step = d_cnt / steps
+    write_free = "place" in ktimes
+    out = {"bound": "hbm", "kernel": dominant, "peak": hbm, "unit": "GB/s",
+           "peak_source": ("measured (MEASURED_PEAKS.json hbm_gbs)" if hbm_src == "measured"
+                           else "fallback 6.65 TB/s"), "ms_per_launch": round(per_launch_s * 1e3, 4),
+           "launches_per_step": round(launches_per_step, 2)}
+    if dominant == "chase":
+        units = levels[0] if levels else n
+        total_units = sum(levels[:-1]) if len(levels) > 1 else units
+        per_launch_units = total_units / launches_per_step
+        ach = B_CHASE * per_launch_units / per_launch_s / 1e9
+        impl = B_CHASE_IMPL * per_launch_units / per_launch_s / 1e9
+        per_visit = CHASE_LOG_DRAM_BYTES_PER_VISIT if write_free else CHASE_DRAM_BYTES_PER_VISIT
+        ncu_visits = CHASE_LOG_NCU_VISITS if write_free else CHASE_NCU_VISITS
+        out.update({"achieved": round(ach, 1), "frac": round(ach / hbm, 4),
+                    "algorithmic_bytes": f"{B_CHASE} B per element visited (one random 32 B sector) x "
+                                         f"{per_launch_units:.0f} visits per launch",
+                    "implementation_bytes": {"bytes_per_visit": B_CHASE_IMPL,
+                                             "what": "the random sector + the 16 B " +
+                                                     ("log entry" if write_free else "stamp") + " per visit",
+                                             "achieved": round(impl, 1), "frac": round(impl / hbm, 4)},
+                    "traffic": round(per_visit * per_launch_units),
+                    "traffic_note": f"ncu dram bytes per visit ({per_visit:.1f} B) of the level-0 "
+                                    f"{'write-free' if write_free else 'stamping'} chase on a 2^25-element list "
+                                    f"({ncu_visits} visits), scaled to this launch's visits",
+                    "traffic_scale": round(per_launch_units / ncu_visits, 4)})
+    else:
+        b_alg = B_ALG[kind](weighted)
+        per_launch_bytes = n * b_alg / launches_per_step
+        ach = per_launch_bytes / per_launch_s / 1e9
+        out.update({"achieved": round(ach, 1), "frac": round(ach / hbm, 4), "traffic": None,
+                    "algorithmic_bytes": f"{b_alg} B per unit x n per step, over this kernel's launches"})
+    return out
+
+
+def random_access_roofline(r: dict, hbm: float) -> dict | None:
+    """The north-star form: sectors touched x 32 B / peak, with the sectors
+    the pipeline that ran touches per list element."""
+    if r["kind"] != "list":
+        return None
+    n, weighted, write_free, levels = r["n"], r["weighted"], r["write_free"], r["levels"]
+    ms = r["ms_per_step"]
+    sectors = (SECTORS_LIST_LOG if write_free else SECTORS_LIST)[bool(weighted)]
+    floor_ms = n * 32 * sectors / (hbm * 1e9) * 1000.0
+    sectors_min = min(SECTORS_LIST[bool(weighted)], SECTORS_LIST_LOG[bool(weighted)])
+    floor_min_ms = n * 32 * sectors_min / (hbm * 1e9) * 1000.0
+    out = {"level0": "write-free" if write_free else "stamping", "sectors_per_element": sectors,
+           "bytes_per_element": 32 * sectors, "floor_ms": round(floor_ms, 3), "frac": round(floor_ms / ms, 4),
+           "sectors_min_design": sectors_min, "frac_min_design": round(floor_min_ms / ms, 4), "peak_gbs": hbm}
+    if write_free and weighted:
+        visits = sum(levels[:2]) if len(levels) > 1 else n
+        dram = n * sum(DRAM_PER_ELEM_LOG.values()) + visits * CHASE_LOG_DRAM_BYTES_PER_VISIT
+        out["measured"] = {"bytes_per_element": round(dram / n, 1), "sectors_per_element": round(dram / n / 32, 2),
+                           "achieved_gbs": round(dram / (ms / 1000.0) / 1e9, 1),
+                           "frac": round(dram / (ms / 1000.0) / 1e9 / hbm, 4),
+                           "source": "ncu DRAM bytes per kernel on a 2^25 list, scaled by elements and chase visits"}
+    return out
+
+
+def summary(r: dict) -> dict:
+    """The figures of one workload for the JSON line."""
+    return {"workload": r["desc"], "n": r["n"], "value": r["value"],
+            "unit": "elements/s" if r["kind"] == "list" else "vertices/s", "ms_per_step": round(r["ms_per_step"], 4),
+            "pipeline_frac": r["pipeline"]["frac"], "b_alg_per_unit": r["pipeline"]["b_alg_per_elem"],
+            "roofline": r["roofline"], "levels": r["levels"], "kernels_ms_per_step": r["kernels_ms_per_step"]}
 
 
 def main():
@@ -496,6 +768,8 @@ def main():
             dist.destroy_process_group()
         return
 
+    import ctypes
+
     import numpy as np
     import torch
 
@@ -504,118 +778,19 @@ def main():
     desc, n, kind, arg, weighted = WORKLOADS[args.workload]
     if args.n:
         n = args.n
-        desc = f"{desc} [size overridden: n={n}]"
     dev = torch.device(f"cuda:{local}")
     ctx = kb.Context(local)
     stream = torch.cuda.current_stream(dev)
     seed = 0xC1 + 1000 * rank
-    tuning = kb.GpuTuning(profile=True, ruler_spacing=args.spacing, chains_per_thread=args.chains,
-                          block_size=args.block,
-                          level0_mode=args.level0_mode)
-    if kind == "list":
-        inp = kb.gen_list(n, seed, arg, device=dev)
-        w = kb.gen_weights(n, seed + 1, 16, device=dev) if weighted else None
-        root = torch.empty(n, dtype=torch.int64, device=dev)
-        rk = torch.empty(n, dtype=torch.int64, device=dev)
-        ctx.reserve(kb.lib.kascade_scratch_bytes_rank_list(n))
-
-        def step():
-            kb.rank_list(inp, w, tuning=tuning, root_out=root, rank_out=rk, ctx=ctx)
-    else:
-        blocks = 64
-        spine = (n // blocks) // 2 if arg == 1 else 0
-        inp = kb.gen_forest(n, seed, arg, blocks, spine, device=dev)
-        w = None
-        root = torch.empty(n, dtype=torch.int64, device=dev)
-        rk = torch.empty(n, dtype=torch.int64, device=dev)
-        ctx.reserve(kb.lib.kascade_scratch_bytes_root_forest(n))
-
-        def step():
-            kb.root_forest(inp, tuning=tuning, root_out=root, depth_out=rk, ctx=ctx)
-
-    torch.cuda.synchronize()
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    ctx.reset_kernel_times()
-    clocks = ClockSampler(local)
-    clocks.start()
-    time.sleep(0.3)
-    barrier(world)
-    torch.cuda.synchronize()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    for _ in range(args.steps):
-        step()
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    barrier(world)
-    clk = clocks.stop()
-    ms_per_step, value = whole_job(n, ev0.elapsed_time(ev1), args.steps, world)
-    ktimes = ctx.kernel_times()
-    launches = sum(c for (_, c) in ktimes.values())
-    step_kernel_ms = {k: v[0] / args.steps for k, v in ktimes.items()}
-    dominant = max(ktimes, key=lambda k: ktimes[k][0]) if ktimes else None
-    levels = ctx.levels()
-    write_free = "place" in ktimes  # level 0 ran the write-free chase
-
-    hbm, hbm_src = peaks()
-    b_alg = B_ALG[kind](weighted)
-    pipe_gbs = n * b_alg / (ms_per_step / 1000.0) / 1e9
-    roofline = None
-    if dominant:
-        d_ms, d_cnt = ktimes[dominant]
-        per_launch_s = d_ms / d_cnt / 1000.0
-        if dominant == "chase":
-            # elements visited by the level-0 chase launch (every non-ruler
-            # element plus each ruler's own start record)
-            units = levels[0] if levels else n
-            per_launch_units = units * (1 if kind == "list" else 1)
-            launches_per_step = d_cnt / args.steps
-            # deeper-level chases are far smaller; attribute bytes of all
-            # levels, divided over the chase launches of one step
-            total_units = sum(levels[:-1]) if len(levels) > 1 else units
-            per_launch_bytes = B_CHASE * total_units / launches_per_step
-            per_visit = CHASE_LOG_DRAM_BYTES_PER_VISIT if write_free else CHASE_DRAM_BYTES_PER_VISIT
-            traffic = per_visit * total_units / launches_per_step if per_visit else None
-            second = "16 B log entry" if write_free else "16 B stamp"
-            bytes_note = (f"{B_CHASE} B per element visited (one random 32 B sector for the 16 B record + {second}) "
-                          f"x {total_units} elements over {launches_per_step:.0f} chase launches per step")
-        else:
-            per_launch_bytes = n * b_alg / (d_cnt / args.steps)
-            traffic = None
-            bytes_note = f"{b_alg} B/element x n per step, over this kernel's launches"
-        ach = per_launch_bytes / per_launch_s / 1e9
-        roofline = {"bound": "hbm", "kernel": dominant, "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
-                    "frac": round(ach / hbm, 4), "peak_source": f"{hbm_src} (MEASURED_PEAKS.json hbm_gbs)"
-                    if hbm_src == "measured" else "fallback 6.65 TB/s",
-                    "traffic": round(traffic) if traffic else None,
-                    "traffic_note": ("ncu dram bytes per visited element on a 2^25 list, scaled by the visits per "
-                                     "launch" if traffic else None),
-                    "algorithmic_bytes": bytes_note}
-    pipeline = {"b_alg_per_elem": b_alg, "achieved_gbs": round(pipe_gbs, 1), "frac": round(pipe_gbs / hbm, 4)}
-    random_access = None
-    if kind == "list":
-        sectors = (SECTORS_LIST_LOG if write_free else SECTORS_LIST)[bool(weighted)]
-        floor_ms = n * 32 * sectors / (hbm * 1e9) * 1000.0
-        # the fewer-sector design (stamping level 0) as a conservative floor
-        sectors_min = min(SECTORS_LIST[bool(weighted)], SECTORS_LIST_LOG[bool(weighted)])
-        floor_min_ms = n * 32 * sectors_min / (hbm * 1e9) * 1000.0
-        random_access = {"level0": "write-free" if write_free else "stamping",
-                         "sectors_per_element": sectors, "bytes_per_element": 32 * sectors,
-                         "floor_ms": round(floor_ms, 3), "frac": round(floor_ms / ms_per_step, 4),
-                         "sectors_min_design": sectors_min, "frac_min_design": round(floor_min_ms / ms_per_step, 4),
-                         "peak_gbs": hbm}
-        if write_free and weighted:
-            # measured traffic of the level-0 kernels (deeper levels, ~2%, left out)
-            visits = sum(levels[:2]) if len(levels) > 1 else n
-            dram = n * sum(DRAM_PER_ELEM_LOG.values()) + visits * CHASE_LOG_DRAM_BYTES_PER_VISIT
-            random_access["measured"] = {
-                "bytes_per_element": round(dram / n, 1), "sectors_per_element": round(dram / n / 32, 2),
-                "achieved_gbs": round(dram / (ms_per_step / 1000.0) / 1e9, 1),
-                "frac": round(dram / (ms_per_step / 1000.0) / 1e9 / hbm, 4),
-                "source": "ncu DRAM bytes per kernel on a 2^25 list, scaled by elements and chase visits"}
+    tune = dict(ruler_spacing=args.spacing, chains_per_thread=args.chains, block_size=args.block,
+                level0_mode=args.level0_mode)
+    tuning = kb.GpuTuning(profile=True, **tune)
+    main_r = measure_device(kb, ctx, dev, args.workload, n, tuning, args.steps, args.warmup, world, seed,
+                            clocks=True)
+    if args.n:
+        main_r["desc"] = f"{main_r['desc']} [size overridden: n={n}]"
+    inp, w, root, rk = main_r["inp"], main_r["w"], main_r["root"], main_r["rank"]
+    hbm, _ = peaks()
 
     # end-to-end through the host-buffer API (pinned host memory)
     e2e = None
@@ -628,9 +803,7 @@ def main():
             pin_w.copy_(w.cpu())
         pin_root = torch.empty(n, dtype=torch.int64, pin_memory=True)
         pin_rank = torch.empty(n, dtype=torch.int64, pin_memory=True)
-        o = kb.GpuTuning(ruler_spacing=args.spacing, chains_per_thread=args.chains, block_size=args.block,
-                         level0_mode=args.level0_mode).to_opts()
-        import ctypes
+        o = kb.GpuTuning(**tune).to_opts()
 
         def e2e_step():
             if kind == "list":
@@ -657,60 +830,61 @@ def main():
         e1.record(stream)
         torch.cuda.synchronize()
         te = max_over_ranks(e0.elapsed_time(e1), world) / args.e2e_steps
-        # correctness spot check of the host result against the device result
-        ok = bool(np.array_equal(pin_rank[:4096].numpy(), rk[:4096].cpu().numpy()))
+        ok = bool(torch.equal(pin_rank, rk.cpu()) and torch.equal(pin_root, root.cpu()))
         h2d = n * 8 + (n * 4 if w is not None else 0)
-        e2e = {"value": n * world / (te / 1000.0), "unit": "elements/s", "h2d_bytes_per_step": h2d,
-               "d2h_bytes_per_step": 16 * n, "ms_per_step": round(te, 3), "host_matches_device": ok}
+        e2e = {"value": n * world / (te / 1000.0), "unit": "elements/s" if kind == "list" else "vertices/s",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 16 * n, "ms_per_step": round(te, 3),
+               "host_matches_device": ok}
+        del pin_in, pin_w, pin_root, pin_rank
 
-    secondary = {}
-    if not args.no_secondary and kind == "list" and args.workload == "list" and world == 1:
-        # the locality-biased layout of the same configuration
-        inp2 = kb.gen_list(n, seed, 1, device=dev)
-        tun2 = kb.GpuTuning(ruler_spacing=args.spacing, chains_per_thread=args.chains, block_size=args.block,
-                            level0_mode=args.level0_mode)
-        for _ in range(2):
-            kb.rank_list(inp2, w, tuning=tun2, root_out=root, rank_out=rk, ctx=ctx)
-        torch.cuda.synchronize()
-        a0 = torch.cuda.Event(enable_timing=True)
-        a1 = torch.cuda.Event(enable_timing=True)
-        a0.record(stream)
-        for _ in range(3):
-            kb.rank_list(inp2, w, tuning=tun2, root_out=root, rank_out=rk, ctx=ctx)
-        a1.record(stream)
-        torch.cuda.synchronize()
-        tl = a0.elapsed_time(a1) / 3
-        secondary["list_local"] = {"workload": WORKLOADS["list_local"][0], "value": n / (tl / 1000.0),
-                                   "ms_per_step": round(tl, 3),
-                                   "pipeline_frac": round(n * b_alg / (tl / 1000.0) / 1e9 / hbm, 4)}
-        del inp2
-
-    batched = served = None
-    if world == 1 and not args.no_secondary and args.workload == "list" and not args.n:
-        del inp
-        torch.cuda.empty_cache()
-        batched = measure_batched(kb, ctx, dev)
-        torch.cuda.empty_cache()
-        served = measure_served(kb, dev)
-
+    # CPU baseline on the same seeded input (host copy of the device arrays),
+    # its full-size ruling-set result compared with the GPU result
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, kd, sample = cpu_reference_time(args.cpu_sample, args.workload)
-        cpu = {"value": v, "unit": "elements/s", "cores": 1, "kind": kd, "sample": sample}
+        succ_h = inp.cpu().numpy().view(np.uint64)
+        rank_h = (w.cpu().numpy().view(np.uint32).astype(np.int64) if w is not None
+                  else np.ones(n, np.int64))
+        rank_h[succ_h == np.arange(n, dtype=np.uint64)] = 0
+        check = (root.cpu().numpy().view(np.uint64), rk.cpu().numpy().view(np.uint64))
+        cpu = cpu_baseline(args.workload, n, seed, full=(succ_h, rank_h) if kind == "list" else None,
+                           sample_n=args.cpu_sample, check=check if kind == "list" else None)
+        del succ_h, rank_h, check
+
+    secondary = {}
+    batched = served = None
+    full_default = world == 1 and not args.no_secondary and args.workload == "list" and not args.n
+    del inp, w, root, rk
+    main_r.update(inp=None, w=None, root=None, rank=None)
+    torch.cuda.empty_cache()
+    if full_default:
+        # the locality-biased layout of the same configuration, the 2^20 unit
+        # list of the reference's own small case, and the 2^26-vertex forests
+        for wl2, steps2 in (("list_local", args.steps), ("list20", 5 * args.steps), ("forest_rrt", args.steps),
+                            ("forest_cat", args.steps)):
+            r2 = measure_device(kb, ctx, dev, wl2, WORKLOADS[wl2][1], kb.GpuTuning(profile=True, **tune), steps2,
+                                args.warmup, world, seed)
+            secondary[wl2] = summary(r2)
+            secondary[wl2]["steps"] = steps2
+            del r2
+            torch.cuda.empty_cache()
+        batched = measure_batched(kb, ctx, dev)
+        torch.cuda.empty_cache()
+        served = measure_served(kb, dev, batched_rate=batched["elements_per_s"])
 
     if rank == 0:
         out = {
-            "metric": METRIC, "value": value, "unit": "elements/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded device generator)",
-            "config": {"workload": desc, "n": n, "global_elements": n * world,
+            "metric": METRIC, "value": main_r["value"], "unit": "elements/s" if kind == "list" else "vertices/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(main_r["ms_per_step"], 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded device generator)",
+            "config": {"workload": main_r["desc"], "n": n, "global_elements": n * world,
                        "parallelism": f"replicas x{world} (independent instances, no collective)",
                        "l2": "inputs larger than L2 (16 B records x n = %.1f GiB)" % (16 * n / 2**30),
-                       "ruler_spacing": args.spacing or "auto", "levels": levels},
-            "roofline": roofline, "pipeline_roofline": pipeline, "random_access_roofline": random_access,
-            "cpu_baseline": cpu, "e2e": e2e,
-            "clocks": clk, "gpu_launches": launches,
-            "kernels_ms_per_step": {k: round(v, 4) for k, v in sorted(step_kernel_ms.items())},
+                       "ruler_spacing": args.spacing or "auto", "levels": main_r["levels"]},
+            "roofline": main_r["roofline"], "pipeline_roofline": main_r["pipeline"],
+            "random_access_roofline": random_access_roofline(main_r, hbm),
+            "cpu_baseline": cpu, "e2e": e2e, "clocks": main_r["clocks"], "gpu_launches": main_r["launches"],
+            "kernels_ms_per_step": main_r["kernels_ms_per_step"],
             "secondary": secondary or None, "batched": batched, "served": served,
         }
         print(json.dumps(out), flush=True)

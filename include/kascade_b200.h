@@ -403,6 +403,11 @@ typedef struct kascade_server_stats {
   uint64_t partition_sms;      /* SMs of the throughput lane's partition (0: the
                                   driver offers none; grid budgets only)        */
   uint64_t partition_batches;  /* throughput-lane batches run in the partition  */
+  uint64_t admitted_while_running;      /* requests admitted while a batch was
+                                           in flight (between its start and
+                                           completion)                        */
+  uint64_t batches_started_overlapping; /* batches started while the other
+                                           lane's batch was in flight         */
 } kascade_server_stats;
 
 KASCADE_API void kascade_server_config_init(kascade_server_config* cfg);
@@ -438,6 +443,88 @@ KASCADE_API kascade_status kascade_server_get_stats(kascade_server* server, kasc
 KASCADE_API kascade_status kascade_server_reset_stats(kascade_server* server);
 
 /* ----------------------------------------------------------------------------
+ * Sharded list ranking: one list spread over several GPUs (one process each)
+ * by contiguous index ranges.  Replaces the reference's Distribution
+ * (lib/kascade/distribution.hpp:16-113: shard s holds global indices
+ * [offsets[s], offsets[s+1])) and its synchronous ruler chasing engine
+ * (sparse_ruling_set_detail/ruler_chasing_engine.hpp:57-101: rounds of one
+ * all-to-all exchange of ruler messages, local targets worked on at once).
+ * These calls are one shard's device work; kascade_b200/shard.py drives the
+ * rounds and exchanges over torch.distributed (NCCL over NVLink).  Protocol:
+ *   1. kascade_shard_prepare: records (rec: 16 B x n_local) and rulers (roots
+ *      and a counter-hash sample by global index; local ids)
+ *   2. ruler_base / num_sampled from every shard's ruler count; then rounds of
+ *      kascade_shard_chase (first from the shard's rulers, then from the
+ *      messages received) and one all-to-all of the send buffer, until no
+ *      shard sends
+ *   3. kascade_shard_unreached turns unreached elements (list heads ahead of
+ *      their first ruler: fixup_unreached, post_invert.hpp:195-264) into
+ *      rulers; fixup_base from every shard's count; their chains are chased
+ *   4. every shard gathers all chain ends and ruler elements, builds the
+ *      ruler sub-list (kascade_shard_sublist) and ranks it
+ *      (kascade_sparse_ruling_set, in place)
+ *   5. kascade_shard_propagate writes the shard's roots (global indices) and
+ *      ranks (the plain contract: 0 at roots)
+ * The global list has fewer than 2^32 - 1 elements.  Messages and chain ends
+ * are 16 B records; each call returns once its work and status are complete.
+ * ------------------------------------------------------------------------- */
+typedef struct kascade_shard_desc {
+  uint64_t lo;          /* first global index of this shard                  */
+  uint64_t n_local;     /* elements of this shard                            */
+  uint64_t n_global;    /* elements of all shards                            */
+  uint32_t num_shards;
+  uint32_t self;        /* this shard's number                               */
+  const uint64_t* offsets; /* device: num_shards + 1 range starts            */
+  uint64_t ruler_base;  /* global id of this shard's first sampled ruler     */
+  uint64_t num_sampled; /* this shard's sampled rulers (local ids below it)  */
+  uint64_t fixup_base;  /* global id of this shard's first fix-up ruler      */
+} kascade_shard_desc;
+typedef struct kascade_shard_msg {
+  uint32_t target; /* global index of the chain's next element */
+  uint32_t ruler;  /* global ruler id of the chain             */
+  uint64_t dist;   /* distance from the ruler to target        */
+} kascade_shard_msg;
+typedef struct kascade_shard_end {
+  uint32_t ruler; /* global ruler id                            */
+  uint32_t next;  /* the next ruler's global id (self at roots)  */
+  uint64_t dist;  /* distance between them                       */
+} kascade_shard_end;
+KASCADE_API kascade_status kascade_shard_prepare(kascade_ctx* ctx, const kascade_shard_desc* desc,
+                                                 const uint64_t* succ, const uint32_t* weights, uint64_t n_global,
+                                                 uint32_t spacing, uint32_t seed, void* rec, uint32_t* ruler_elem,
+                                                 uint64_t* num_rulers, void* stream);
+/* Chains from start_rulers (local element indices of rulers) and from
+ * incoming messages.  regions: num_shards x region_cap messages of scratch
+ * (region_cap >= num_start + num_in); send receives the outgoing messages
+ * grouped by destination shard, sent_counts[d] their counts; chain ends are
+ * appended to ends (*num_ends in: entries so far, out: the new total). */
+KASCADE_API kascade_status kascade_shard_chase(kascade_ctx* ctx, const kascade_shard_desc* desc, void* rec,
+                                               const uint32_t* start_rulers, uint64_t num_start,
+                                               const kascade_shard_msg* incoming, uint64_t num_in,
+                                               kascade_shard_msg* regions, uint64_t region_cap,
+                                               kascade_shard_msg* send, uint64_t* sent_counts,
+                                               kascade_shard_end* ends, uint64_t* num_ends, uint64_t end_cap,
+                                               void* stream);
+/* Unreached elements become rulers with local ids first_lid.. (appended to
+ * ruler_elem); *count = how many. */
+KASCADE_API kascade_status kascade_shard_unreached(kascade_ctx* ctx, const kascade_shard_desc* desc, void* rec,
+                                                   uint32_t* ruler_elem, uint64_t first_lid, uint64_t* count,
+                                                   void* stream);
+/* out[k] = lo + ruler_elem[first + k]: the global elements of local rulers. */
+KASCADE_API kascade_status kascade_shard_ruler_globals(kascade_ctx* ctx, const uint32_t* ruler_elem, uint64_t lo,
+                                                       uint64_t first, uint64_t count, uint64_t* out, void* stream);
+/* All chain ends -> succ2[ruler] = next, w2[ruler] = distance. */
+KASCADE_API kascade_status kascade_shard_sublist(kascade_ctx* ctx, const kascade_shard_end* ends, uint64_t num_ends,
+                                                 uint64_t num_rulers, uint64_t* succ2, int64_t* w2, void* stream);
+/* Outputs of the shard's elements from the ranked sub-list (sub_root: root
+ * ruler id per ruler, sub_rank: distance to the root per ruler,
+ * elem_of_ruler: global element of each ruler id). */
+KASCADE_API kascade_status kascade_shard_propagate(kascade_ctx* ctx, const kascade_shard_desc* desc, const void* rec,
+                                                   const uint64_t* sub_root, const int64_t* sub_rank,
+                                                   const uint64_t* elem_of_ruler, uint64_t num_rulers,
+                                                   uint64_t* root_out, uint64_t* rank_out, void* stream);
+
+/* ----------------------------------------------------------------------------
  * Ranking without allocation -- no counterpart in the reference.
  * For callers that may not allocate device memory (a host framework that owns
  * all device memory through its own pool, or a latency-critical path where an
@@ -448,7 +535,9 @@ KASCADE_API kascade_status kascade_server_reset_stats(kascade_server* server);
  * n <= KASCADE_NOALLOC_MAX_ELEMENTS; larger n returns KASCADE_ERR_TOO_LARGE.
  * All calls share the array: calls that overlap on the GPU race, so order
  * them.  The first call on a device looks up the array's address; make it
- * before any stream capture.  Synchronises `stream` before returning.
+ * before any stream capture.  Synchronises `stream` before returning.  The
+ * outputs are undefined unless the status is KASCADE_OK; a CUDA error left
+ * pending by earlier work returns KASCADE_ERR_CUDA and is not cleared.
  * ------------------------------------------------------------------------- */
 #define KASCADE_NOALLOC_MAX_ELEMENTS 65536u
 KASCADE_API kascade_status kascade_rank_list_noalloc(const uint64_t* succ, const uint32_t* weights,

@@ -35,6 +35,13 @@ class Segment(ctypes.Structure):
                 ("reserved", ctypes.c_uint32)]
 
 
+class ShardDesc(ctypes.Structure):
+    """Mirror of ``kascade_shard_desc``."""
+
+    _fields_ = [("lo", c_u64), ("n_local", c_u64), ("n_global", c_u64), ("num_shards", c_u32), ("self", c_u32),
+                ("offsets", c_void_p), ("ruler_base", c_u64), ("num_sampled", c_u64), ("fixup_base", c_u64)]
+
+
 class ServerConfig(ctypes.Structure):
     """Mirror of ``kascade_server_config``."""
 
@@ -53,7 +60,8 @@ class ServerStats(ctypes.Structure):
                 ("requests_per_s", ctypes.c_double), ("bytes_in_use", c_u64), ("lane_batches", c_u64 * 2),
                 ("lane_elements", c_u64 * 2), ("lane_busy_ms", ctypes.c_double * 2),
                 ("lane_max_batch_ms", ctypes.c_double * 2), ("partition_sms", c_u64),
-                ("partition_batches", c_u64)]
+                ("partition_batches", c_u64), ("admitted_while_running", c_u64),
+                ("batches_started_overlapping", c_u64)]
 
 
 class Stats(ctypes.Structure):
@@ -160,6 +168,15 @@ _SIGS = {
                                         P(c_u64), c_void_p]),
     "kascade_ctx_get_class_launch": (c_int, [_ctx_p, P(c_u32), P(c_u32), P(c_u32), c_int]),
     "kascade_ctx_set_sm_budget": (_status, [_ctx_p, c_int]),
+    "kascade_shard_prepare": (_status, [_ctx_p, P(ShardDesc), c_void_p, c_void_p, c_u64, c_u32, c_u32, c_void_p,
+                                        c_void_p, P(c_u64), c_void_p]),
+    "kascade_shard_chase": (_status, [_ctx_p, P(ShardDesc), c_void_p, c_void_p, c_u64, c_void_p, c_u64, c_void_p,
+                                      c_u64, c_void_p, P(c_u64), c_void_p, P(c_u64), c_u64, c_void_p]),
+    "kascade_shard_unreached": (_status, [_ctx_p, P(ShardDesc), c_void_p, c_void_p, c_u64, P(c_u64), c_void_p]),
+    "kascade_shard_ruler_globals": (_status, [_ctx_p, c_void_p, c_u64, c_u64, c_u64, c_void_p, c_void_p]),
+    "kascade_shard_sublist": (_status, [_ctx_p, c_void_p, c_u64, c_u64, c_void_p, c_void_p, c_void_p]),
+    "kascade_shard_propagate": (_status, [_ctx_p, P(ShardDesc), c_void_p, c_void_p, c_void_p, c_void_p, c_u64,
+                                          c_void_p, c_void_p, c_void_p]),
     "kascade_server_config_init": (None, [P(ServerConfig)]),
     "kascade_server_create": (_status, [P(ServerConfig), P(c_void_p)]),
     "kascade_server_destroy": (_status, [c_void_p]),

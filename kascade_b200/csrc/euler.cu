@@ -4,23 +4,28 @@
 // (lib/kascade/eulertour.cpp:33-127, 235-278, 337-392) with the forest built
 // by reverse_rooted_tree + make_graph (lib/kascade/successor_utils.cpp:236-300).
 //
-// Layout used for ranking (m = 2n elements):
-//   slot v        (v < n)  : the up edge v -> parent(v); for a root r it is
-//                            the tour's terminal element (weight 0, the
-//                            reference's dummy root element)
-//   slot n + q    (q < n)  : the down edge parent -> child of the q-th entry
-//                            of the children array sorted by parent; a root's
-//                            own entry (key = value = r) is an unused self loop
-// so that the depth of v is the rank of slot v and the final map-back is a
-// coalesced pass over slots 0..n-1.  Rotation at a vertex: parent first, then
-// children in increasing id; the tour of a tree starts at the down edge to
-// the root's first child and ends in the root's terminal slot.
+// Layout used for ranking a single forest (m = 2n elements): slot v (v < n)
+// is the up edge v -> parent(v), and for a root r the tour's terminal
+// element (weight 0, the reference's dummy root element); slot n + v is the
+// down edge parent(v) -> v, a root's an unused self loop.  The depth of v is
+// the rank of slot v (up edges weigh +1, down edges -1), so the final
+// map-back is a coalesced pass over slots 0..n-1; the tour of a tree starts
+// at the down edge into the root's first child and ends in the root's
+// terminal slot.
 //
-// A single forest's tour build reads each vertex's first child from a table
-// (read-only random access), writes the down records in sorted order and
-// stages the up records in sorted order; place_records then moves them to
-// their vertices' slots with two radix passes and a dense placement, so no
-// record is written at a random address.
+// A single forest needs no sort: ranking only needs each vertex's children
+// grouped, in any order (depth and root are unique whatever the rotation).
+// One pass links every vertex into its parent's child list (one atomic
+// exchange per warp group of siblings on the parent's list head); a second,
+// purely streaming pass writes both tour records of every vertex at slots
+// indexed by the vertex itself:
+//   slot v      : up edge v -> p, successor the down edge into v's next
+//                 sibling, else p's up slot
+//   slot n + v  : down edge p -> v, successor the down edge into v's first
+//                 child, else v's own up slot
+// The tour's rotation is then the list order, which depends on the order of
+// the atomic exchanges; results do not.  A batch of forests and
+// compute_euler_tour (the reference's numbering) sort the children instead.
 #include "ranker.cuh"
 #include "sort.cuh"
 
@@ -46,32 +51,15 @@ __global__ void __launch_bounds__(256) k_seg_bounds(const uint32_t* __restrict__
   }
 }
 
-// A single forest: fc[p] = position of p's first child in the sorted array
-// (NO_CHILD where p has none).
 constexpr uint32_t NO_CHILD = 0xFFFFFFFFu;
-__global__ void __launch_bounds__(256) k_first_child_table(const uint32_t* __restrict__ keys, uint32_t n,
-                                                           uint32_t* __restrict__ fc) {
-  for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t k = keys[q];
-    if (q == 0 || keys[q - 1] != k) fc[k] = (uint32_t)q;
-  }
-}
 
-// Where the records of a forest's tour live.  A single forest of n vertices:
-// up edge of v at slot v, down edge of sorted entry q at slot n + q.  A batch
-// of forests (compacted into one vertex space with per-forest bases fd[j]):
-// up edge of compact vertex c of forest j at that vertex's position in the
-// caller's concatenated arrays (foff[j] + c - fd[j]), down edges after all
-// input elements (down_base + q).  Ruler sampling thresholds can differ per
-// forest (size classes).
-struct SlotsSingle {
-  uint32_t n;
-  uint32_t th;
-  __device__ __forceinline__ uint32_t seg_of(uint32_t) const { return 0; }
-  __device__ __forceinline__ uint32_t up(uint32_t v, uint32_t) const { return v; }
-  __device__ __forceinline__ uint32_t down(uint64_t q) const { return n + (uint32_t)q; }
-  __device__ __forceinline__ uint32_t thresh(uint32_t) const { return th; }
-};
+// Where the records of a batch's forest tours live.  The forests are
+// compacted into one vertex space with per-forest bases fd[j]; the up edge of
+// compact vertex c of forest j sits at that vertex's position in the caller's
+// concatenated arrays (foff[j] + c - fd[j]), the down edge of sorted child
+// entry q after all input elements (down_base + q).  Ruler sampling
+// thresholds can differ per forest (size classes).  Rotation at a vertex:
+// parent first, then children in increasing id.
 
 struct SlotsBatch {
   const uint32_t* fd;       // nf + 1 compact starts
@@ -95,19 +83,16 @@ struct SlotsBatch {
   __device__ __forceinline__ uint32_t thresh(uint32_t j) const { return __ldg(fthresh + j); }
 };
 
-// Writes both tour records of every sorted entry q, samples rulers among the
-// written slots and numbers them (one atomic per tile, as in prepare).  The
-// first child comes from a first-child table (FC_TABLE) or the segment table;
-// the up record goes into stage[q] as (slot, successor, tag, weight) for
-// place_records (STAGE_UP; single forests, where a vertex's up slot is its
-// id), or straight to its slot.
-template <class Slots, bool FC_TABLE, bool STAGE_UP>
+// Writes both tour records of every sorted child entry q of a batch's
+// forests, samples rulers among the written slots and numbers them (one
+// atomic per tile, as in prepare).  The first child comes from the segment
+// table.
+template <class Slots>
 __global__ void __launch_bounds__(256) k_tour_build(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
                                                     uint32_t n, const uint2* __restrict__ seg,
                                                     const uint32_t* __restrict__ root_bits, Rec* __restrict__ rec,
                                                     uint32_t* __restrict__ ruler_elem, uint32_t* __restrict__ counter,
-                                                    uint32_t salt, Slots slots, const uint32_t* __restrict__ fc,
-                                                    uint4* __restrict__ stage, DevStatus* st) {
+                                                    uint32_t salt, Slots slots, DevStatus* st) {
   __shared__ uint32_t sm[33];
   __shared__ uint32_t sbase;
   const uint64_t tile_sz = (uint64_t)blockDim.x * TB_ITEMS;
@@ -146,12 +131,8 @@ __global__ void __launch_bounds__(256) k_tour_build(const uint32_t* __restrict__
         su[i] = slot_up;
         // down edge p -> c: descend to c's first child, else come back up
         uint32_t first_child = NO_CHILD;
-        if (FC_TABLE) {
-          first_child = __ldg(fc + c);
-        } else {
-          const uint2 sg = seg[c];
-          if (sg.x < sg.y) first_child = sg.x;
-        }
+        const uint2 sg = seg[c];
+        if (sg.x < sg.y) first_child = sg.x;
         rd[i].a = ~0ull;  // -1
         rd[i].b = (first_child != NO_CHILD) ? slots.down(first_child) : slot_up;
         sd[i] = slot_down;
@@ -202,11 +183,131 @@ __global__ void __launch_bounds__(256) k_tour_build(const uint32_t* __restrict__
         }
         id++;
       }
-      if (STAGE_UP)
-        __stcs(stage + q, make_uint4(su[i], ru[i].b, ru[i].c, (uint32_t)ru[i].a));
-      else
-        rec[su[i]] = ru[i];
+      rec[su[i]] = ru[i];
       rec[sd[i]] = rd[i];
+    }
+    __syncthreads();
+  }
+}
+
+// Child lists of a single forest: fc[p] = one child of p (NO_CHILD: a leaf),
+// nsib[v] = v's next sibling (NO_CHILD: the last one).  A warp's vertices that
+// share a parent link to each other in lane order and the group's first lane
+// exchanges the list head once.  root_bits gets one bit per vertex (warp
+// ballots over 32 consecutive vertices: no atomics, no clearing).  An
+// out-of-range parent is reported and the vertex treated as a root.
+__global__ void __launch_bounds__(256) k_link_children(const uint64_t* __restrict__ parent, uint32_t n,
+                                                       uint32_t* __restrict__ fc, uint32_t* __restrict__ nsib,
+                                                       uint32_t* __restrict__ root_bits, DevStatus* st) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
+    const uint64_t v = base + threadIdx.x;  // base and blockDim are multiples of 32
+    const bool valid = v < n;
+    uint64_t p = valid ? __ldcs(reinterpret_cast<const unsigned long long*>(parent) + v) : v;
+    if (valid && p >= n) {
+      set_error(st, KASCADE_ERR_OUT_OF_RANGE, v);
+      p = v;
+    }
+    const bool root = valid && p == v;
+    const uint32_t rb = __ballot_sync(0xffffffffu, root);
+    if (lane == 0 && (v >> 5) <= ((uint64_t)n - 1) >> 5) root_bits[v >> 5] = rb;
+    const bool link = valid && !root;
+    // lanes that do not link get distinct keys
+    const unsigned long long key = link ? p : (0xFFFFFFFF00000000ull | lane);
+    const uint32_t peers = __match_any_sync(0xffffffffu, key);
+    const int leader = __ffs(peers) - 1;
+    uint32_t old = NO_CHILD;
+    if (link && (int)lane == leader) old = atomicExch(fc + p, (uint32_t)v);
+    old = __shfl_sync(0xffffffffu, old, leader);
+    if (valid) {
+      const uint32_t after = peers & ~((2u << lane) - 1u);  // higher lanes of my group
+      const uint32_t next = after ? (uint32_t)(base + (uint32_t)(__ffs(after) - 1)) : old;
+      __stcs(nsib + v, link ? next : NO_CHILD);
+    }
+  }
+}
+
+// Both tour records of every vertex, at slots v and n + v, from the child
+// lists; rulers sampled among the slots and numbered (one atomic per tile).
+// The down edge into a root's first child is the head of that tree's tour
+// and always a ruler, so no tour element is left unreached; roots' slots are
+// self loops (the terminal, and an unused down slot) and rulers.
+__global__ void __launch_bounds__(256) k_tour_links(const uint64_t* __restrict__ parent, uint32_t n,
+                                                    const uint32_t* __restrict__ fc,
+                                                    const uint32_t* __restrict__ nsib,
+                                                    const uint32_t* __restrict__ root_bits, Rec* __restrict__ rec,
+                                                    uint32_t* __restrict__ ruler_elem, uint32_t* __restrict__ counter,
+                                                    uint32_t salt, uint32_t th, DevStatus* st) {
+  __shared__ uint32_t sm[33];
+  __shared__ uint32_t sbase;
+  const uint64_t tile_sz = (uint64_t)blockDim.x * TB_ITEMS;
+  for (uint64_t tile = (uint64_t)blockIdx.x * tile_sz; tile < n; tile += (uint64_t)gridDim.x * tile_sz) {
+    Rec ru[TB_ITEMS], rd[TB_ITEMS];
+    uint32_t rl = 0, cnt = 0;
+#pragma unroll
+    for (int i = 0; i < TB_ITEMS; ++i) {
+      const uint64_t v = tile + (uint64_t)i * blockDim.x + threadIdx.x;
+      if (v >= n) continue;
+      uint64_t p = __ldcs(reinterpret_cast<const unsigned long long*>(parent) + v);
+      if (p >= n) p = v;  // reported by k_link_children
+      const uint32_t sib = __ldcs(nsib + v), first = __ldcs(fc + v);
+      const uint32_t up = (uint32_t)v, down = n + (uint32_t)v;
+      if (p == v) {
+        ru[i].a = 0;
+        ru[i].b = up;
+        rd[i].a = 0;
+        rd[i].b = down;
+        rl |= 3u << (2 * i);
+        cnt += 2;
+        continue;
+      }
+      ru[i].a = 1ull;
+      ru[i].b = (sib != NO_CHILD) ? n + sib : (uint32_t)p;
+      rd[i].a = ~0ull;  // -1
+      rd[i].b = (first != NO_CHILD) ? n + first : up;
+      bool head = false;
+      if ((__ldg(root_bits + (p >> 5)) >> (p & 31)) & 1u) head = __ldg(fc + p) == (uint32_t)v;
+      if (sampled(up, salt, th)) {
+        rl |= 1u << (2 * i);
+        cnt++;
+      }
+      if (head || sampled(down, salt, th)) {
+        rl |= 2u << (2 * i);
+        cnt++;
+      }
+    }
+    uint32_t total;
+    uint32_t pre = block_exclusive_scan(cnt, sm, &total);
+    if (threadIdx.x == 0) {
+      uint32_t b = total ? atomicAdd(counter, total) : 0u;
+      if ((uint64_t)b + total > MAX_RULERS) set_error(st, KASCADE_ERR_TOO_LARGE, b);
+      sbase = b;
+    }
+    __syncthreads();
+    uint32_t id = sbase + pre;
+#pragma unroll
+    for (int i = 0; i < TB_ITEMS; ++i) {
+      const uint64_t v = tile + (uint64_t)i * blockDim.x + threadIdx.x;
+      if (v >= n) continue;
+      ru[i].c = TAG_UNREACHED;
+      rd[i].c = TAG_UNREACHED;
+      if ((rl >> (2 * i)) & 1u) {
+        if (id < MAX_RULERS) {
+          ru[i].c = TAG_RULER | id;
+          ruler_elem[id] = (uint32_t)v;
+        }
+        id++;
+      }
+      if ((rl >> (2 * i)) & 2u) {
+        if (id < MAX_RULERS) {
+          rd[i].c = TAG_RULER | id;
+          ruler_elem[id] = n + (uint32_t)v;
+        }
+        id++;
+      }
+      st_rec_cs(rec + v, ru[i]);
+      st_rec_cs(rec + n + v, rd[i]);
     }
     __syncthreads();
   }
@@ -278,7 +379,6 @@ __global__ void __launch_bounds__(256) k_ref_tour(const uint64_t* __restrict__ p
 
 kascade_status sort_children(kascade_ctx& ctx, const uint64_t* parent, uint32_t n, uint32_t** keys, uint32_t** vals,
                              uint2** seg, uint32_t** root_bits, cudaStream_t s) {
-  // seg == nullptr: no segment table (a single forest keeps first children in its records)
   SortSource src;
   src.parent = parent;
   if (root_bits) {
@@ -303,37 +403,29 @@ kascade_status root_forest_impl(kascade_ctx& ctx, const uint64_t* parent, uint32
                                 uint64_t* depth_out, int keep_roots, const Params& p, cudaStream_t s,
                                 bool device_levels) {
   if (n == 0) return KASCADE_OK;
-  uint32_t *keys, *vals;
-  uint32_t* root_bits = nullptr;
-  KS_TRY(sort_children(ctx, parent, n, &keys, &vals, nullptr, &root_bits, s));
   const uint32_t m = 2 * n;
   Rec* rec = alloc<Rec>(ctx, m);
   uint32_t* ruler_elem = alloc<uint32_t>(ctx, m);
   uint32_t* ctr = alloc<uint32_t>(ctx, 1);
   uint32_t* fc = alloc<uint32_t>(ctx, n);
-  uint4* stage = alloc<uint4>(ctx, ((uint64_t)n + 8191) / 8192 * 8192);
-  if (!rec || !ruler_elem || !ctr || !fc || !stage) return KASCADE_ERR_OOM;
+  uint32_t* nsib = alloc<uint32_t>(ctx, n);
+  uint32_t* root_bits = alloc<uint32_t>(ctx, ((uint64_t)n + 31) / 32);
+  if (!rec || !ruler_elem || !ctr || !fc || !nsib || !root_bits) return KASCADE_ERR_OOM;
   KS_CUDA(cudaMemsetAsync(ctr, 0, sizeof(uint32_t), s));
   {
-    // every parent records its first child's position; the rest stay "no child"
-    ProfScope ps(ctx, "seg_bounds", s);
+    ProfScope ps(ctx, "link_children", s);
     KS_CUDA(cudaMemsetAsync(fc, 0xFF, sizeof(uint32_t) * (size_t)n, s));
-    k_first_child_table<<<grid_for(ctx, n, 256, 8), 256, 0, s>>>(keys, n, fc);
+    k_link_children<<<grid_for(ctx, n, 256, 8), 256, 0, s>>>(parent, n, fc, nsib, root_bits, ctx.d_status);
     KS_CHECK_LAUNCH();
   }
   {
-    // down records straight to their slots (sorted order); up records staged
-    // in sorted order, then placed at their vertices' slots by radix passes:
-    // the only random access left is the read-only first-child lookup
     ProfScope ps(ctx, "tour_build", s);
     const unsigned grid = grid_for(ctx, ((uint64_t)n + 256 * TB_ITEMS - 1) / (256 * TB_ITEMS) * 256, 256, 8);
-    SlotsSingle slots{n, (uint32_t)(4294967296.0 / (double)(p.spacing0 < 2 ? 2 : p.spacing0))};
-    k_tour_build<SlotsSingle, true, true><<<grid, 256, 0, s>>>(keys, vals, n, nullptr, root_bits, rec, ruler_elem,
-                                                               ctr, mix32(p.seed ^ 0x70757254u), slots, fc, stage,
-                                                               ctx.d_status);
+    const uint32_t th = (uint32_t)(4294967296.0 / (double)(p.spacing0 < 2 ? 2 : p.spacing0));
+    k_tour_links<<<grid, 256, 0, s>>>(parent, n, fc, nsib, root_bits, rec, ruler_elem, ctr,
+                                      mix32(p.seed ^ 0x70757254u), th, ctx.d_status);
     KS_CHECK_LAUNCH();
   }
-  KS_TRY(place_records(ctx, stage, n, rec, s));
   SinkTour sink{root_out, depth_out, n, keep_roots};
   if (device_levels && m > p.base_max && p.max_levels > 0) {
     if (m < p.level0_log_min)
@@ -363,8 +455,8 @@ kascade_status batch_tours(kascade_ctx& ctx, const uint64_t* fpar, uint32_t F, c
   // 4.4 vs 3.0 ms on the 2^28 batch)
   ProfScope ps(ctx, "tour_build", s);
   const unsigned grid = grid_for(ctx, ((uint64_t)F + 256 * TB_ITEMS - 1) / (256 * TB_ITEMS) * 256, 256, 8);
-  k_tour_build<SlotsBatch, false, false><<<grid, 256, 0, s>>>(keys, vals, F, seg, root_bits, rec, ruler_elem, counter,
-                                                              salt, slots, nullptr, nullptr, ctx.d_status);
+  k_tour_build<SlotsBatch><<<grid, 256, 0, s>>>(keys, vals, F, seg, root_bits, rec, ruler_elem, counter, salt, slots,
+                                                ctx.d_status);
   KS_CHECK_LAUNCH();
   return KASCADE_OK;
 }

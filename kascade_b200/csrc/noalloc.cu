@@ -24,6 +24,9 @@
 //  - The first call on a device looks up the array's device address with
 //    cudaGetSymbolAddress (once per device, with that device current); make
 //    that first call before any stream capture.
+//  - When the status is not KASCADE_OK the outputs hold partial values.  An
+//    error already pending on the calling thread is reported as
+//    KASCADE_ERR_CUDA and left in place.
 #include <mutex>
 
 #include "common.cuh"
@@ -136,6 +139,10 @@ extern "C" KASCADE_API kascade_status kascade_rank_list_noalloc(const uint64_t* 
   if (n > KS_NOALLOC_MAX) return KASCADE_ERR_TOO_LARGE;
   if (n == 0) return KASCADE_OK;
   if (!succ || !root_out || !rank_out) return KASCADE_ERR_INVALID_ARG;
+  // an error left pending by the caller's earlier work stays the caller's:
+  // report it without clearing it, so the error checks below see only this
+  // call's own
+  if (cudaPeekAtLastError() != cudaSuccess) return KASCADE_ERR_CUDA;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   unsigned char* base = nullptr;
   kascade_status st = scratch_address(&base);

@@ -224,6 +224,10 @@ struct kascade_server {
   char* lane1_arena = nullptr;  // shared by lane 1's two contexts
   bool lane0_running = false;
   double lane0_last = -1e9;
+  // continuous batching evidence: batches between take and completion, and
+  // what was admitted or started while another batch was in flight
+  int lanes_running = 0;
+  uint64_t admitted_while_running = 0, batches_started_overlapping = 0;
   uint64_t partition_batches = 0;
   struct Driver {
     CUresult (*DeviceGet)(CUdevice*, int) = nullptr;
@@ -380,6 +384,7 @@ void kascade_server::admit_locked() {
     it = waiting.erase(it);
     bytes_in_use += r->footprint;
     r->admitted = true;
+    if (lanes_running > 0) admitted_while_running++;
     r->state = 1;
     ready.push_back(r);
     cv_work.notify_all();
@@ -425,6 +430,8 @@ void kascade_server::lane_loop(int lane) {
       if (stop) break;
       continue;
     }
+    if (lanes_running > 0) batches_started_overlapping++;
+    lanes_running++;
     // while the latency lane has work, the throughput lane's next launches
     // leave it latency_sms SMs, and its next batch runs in the partition
     const double t0 = now_s();
@@ -562,6 +569,7 @@ void kascade_server::lane_loop(int lane) {
     }
     const double t1 = now_s();
     lk.lock();
+    lanes_running--;
     if (lane == 0) {
       lane0_running = false;
       lane0_last = t1;
@@ -926,6 +934,8 @@ KASCADE_API kascade_status kascade_server_get_stats(kascade_server* s, kascade_s
   }
   out->partition_sms = (uint64_t)s->partition_sms;
   out->partition_batches = s->partition_batches;
+  out->admitted_while_running = s->admitted_while_running;
+  out->batches_started_overlapping = s->batches_started_overlapping;
   return KASCADE_OK;
 }
 
@@ -941,6 +951,8 @@ KASCADE_API kascade_status kascade_server_reset_stats(kascade_server* s) {
     s->lane_busy[i] = s->lane_max[i] = 0;
   }
   s->partition_batches = 0;
+  s->admitted_while_running = 0;
+  s->batches_started_overlapping = 0;
   s->t_first_submit = 0;
   s->t_last_done = 0;
   return KASCADE_OK;

@@ -16,6 +16,8 @@ __all__ = [
     "build", "has_ref", "rank_list", "root_forest", "local_pointer_chasing", "pointer_doubling",
     "euler_tour", "rank_via_euler_tour", "is_list", "pack", "unpack", "gen_list", "gen_weights",
     "gen_forest", "ref_gather_rank", "ref_local_pointer_chasing",
+    "cpu_threads", "cpu_sparse_ruling_set", "cpu_pointer_doubling", "cpu_gen_list", "cpu_gen_weights",
+    "cpu_gen_forest",
 ]
 
 
@@ -135,6 +137,50 @@ def unpack(sp: np.ndarray, rp: np.ndarray, active: np.ndarray, succ: np.ndarray,
     rp = np.ascontiguousarray(rp, np.int64)
     active = np.ascontiguousarray(active, np.uint64)
     _o().oracle_unpack(_p(sp), _p(rp), _p(active), U64(active.size), _p(succ), _p(rank))
+
+
+def cpu_threads() -> int:
+    """Host threads the multi-core rankers use (all online cores, or
+    KASCADE_CPU_THREADS)."""
+    return int(_o().cpu_threads())
+
+
+def cpu_sparse_ruling_set(succ: np.ndarray, rank: np.ndarray, spacing: int = 32, seed: int = 42,
+                          threads: int = 0) -> None:
+    """In place, the multi-core restatement of the reference's sparse ruling
+    set (oracle/cpu_parallel.c): succ -> root, rank -> distance to the root."""
+    assert succ.dtype == np.uint64 and rank.dtype == np.int64 and succ.flags.c_contiguous and rank.flags.c_contiguous
+    rc = _o().cpu_sparse_ruling_set(_p(succ), _p(rank), U64(succ.size), U32(spacing), U64(seed),
+                                    ctypes.c_int(threads))
+    if rc != 0:
+        raise ValueError("cpu_sparse_ruling_set: index out of range or a cycle without a root")
+
+
+def cpu_pointer_doubling(succ: np.ndarray, rank: np.ndarray, threads: int = 0) -> int:
+    """In place, multi-core synchronous pointer doubling; returns the rounds."""
+    assert succ.dtype == np.uint64 and rank.dtype == np.int64 and succ.flags.c_contiguous and rank.flags.c_contiguous
+    rounds = _o().cpu_pointer_doubling(_p(succ), _p(rank), U64(succ.size), ctypes.c_int(threads))
+    if rounds < 0:
+        raise ValueError("cpu_pointer_doubling: index out of range or a cycle without a root")
+    return rounds
+
+
+def cpu_gen_list(n: int, seed: int, layout: int = 0) -> np.ndarray:
+    out = np.empty(n, np.uint64)
+    _o().cpu_gen_list(U64(n), U64(seed), U32(layout), _p(out))
+    return out
+
+
+def cpu_gen_weights(n: int, seed: int, wbits: int = 16) -> np.ndarray:
+    out = np.empty(n, np.uint32)
+    _o().cpu_gen_weights(U64(n), U64(seed), U32(wbits), _p(out))
+    return out
+
+
+def cpu_gen_forest(n: int, seed: int, kind: int = 0, blocks: int = 64, spine: int = 0) -> np.ndarray:
+    out = np.empty(n, np.uint64)
+    _o().cpu_gen_forest(U64(n), U64(seed), U32(kind), U64(blocks), U64(spine), _p(out))
+    return out
 
 
 def gen_list(n: int, seed: int, layout: int = 0) -> np.ndarray:

@@ -70,3 +70,15 @@ def test_config_mapping():
     t = c.tuning()
     assert t.ruler_spacing == 64 and t.max_levels == 3
     assert SparseRulingSetConfig().tuning().ruler_spacing == 0
+
+
+def test_noalloc_source_names_no_allocating_call():
+    """The no-allocation entry point's source calls no device or host
+    allocator: no cudaMalloc* (pool and async forms included), cudaFree*,
+    cudaHostAlloc / cudaMallocHost, and no allocation through the library's
+    context arena."""
+    src = (Path(__file__).resolve().parents[1] / "kascade_b200" / "csrc" / "noalloc.cu").read_text()
+    code = "\n".join(line.split("//")[0] for line in src.splitlines())
+    banned = re.findall(r"\b(cudaMalloc\w*|cudaFree\w*|cudaHostAlloc|cudaMallocHost|cuMem\w*|alloc<|malloc|"
+                        r"new\s+\w+\[|kascade_ctx_create)\b", code)
+    assert banned == [], banned

@@ -54,7 +54,7 @@ def test_whole_job_takes_the_slowest_rank_and_every_ranks_elements(tmp_path):
 
 def test_reference_arm_prints_one_line_from_rank_zero(oracle_mod):
     res = _torchrun(["bench.py", "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "0",
-                     "--cpu-sample", "65536"])
+                     "--cpu-sample", "65536", "--n", "1048576"])
     assert res.returncode == 0, res.stderr[-2000:]
     lines = [d for d in _json_lines(res.stdout) if d.get("impl") == "reference"]
     assert len(lines) == 1
@@ -62,3 +62,7 @@ def test_reference_arm_prints_one_line_from_rank_zero(oracle_mod):
     assert d["n_gpus"] == 2 and d["value"] > 0 and d["unit"] == "elements/s"
     assert d["cpu_baseline"]["kind"] in ("reference", "port")
     assert d["e2e"]["h2d_bytes_per_step"] == 0
+    # the multi-core ruling set ran on the whole (here reduced) list
+    v = d["cpu_baseline"]["variants"]
+    assert set(v) == {"sparse_ruling_set", "gather_chase", "pointer_doubling"}
+    assert v["sparse_ruling_set"]["n"] == 1048576 and v["sparse_ruling_set"]["cores"] >= 1

@@ -242,3 +242,38 @@ def test_batch_write_free_errors(kb, oracle_mod):
     root, rank = kb.rank_batch(inputs, segs, w, tuning=t, ctx=ctx)
     _check(kb, oracle_mod, inputs, w, sizes, kinds, root, rank)
     ctx.close()
+
+
+def test_batch_4096_instances_full_size_against_reference_chase(kb, oracle_mod):
+    """The batched workload at full size (4096 instances, sizes log-uniform in
+    [2^6, 2^22], sum 2^28, 70% weighted lists / 30% random recursive forests)
+    in one call, every instance against the reference's own GatherChase
+    (oracle/_ref, one core): the instances are shifted into one global index
+    space by their offsets and ranked by one chase (lists with their weights,
+    forests with unit weights, as the reference's GatherRank does)."""
+    sizes, kinds = kb.batch_sizes(4096, 0xC3, lo_log2=6, hi_log2=22, total=1 << 28)
+    inputs, w = kb.gen_batch(sizes, kinds, seed=0xC3)
+    segs = kb.make_segments(sizes, kinds)
+    root, rank = kb.rank_batch(inputs, segs, w)
+    dev = inputs.device
+    sz = torch.from_numpy(np.asarray(sizes, np.int64)).to(dev)
+    starts = torch.cumsum(sz, 0) - sz
+    seg = torch.repeat_interleave(torch.arange(len(sizes), device=dev), sz)
+    off = starts[seg]
+    is_list = torch.from_numpy(np.asarray(kinds) == kb.SEG_LIST).to(dev)[seg]
+    del seg
+    g_succ = inputs + off
+    g_rank = torch.where(is_list, w.to(torch.int64) & 0xFFFFFFFF, torch.ones_like(inputs))
+    g_rank[g_succ == torch.arange(g_succ.numel(), device=dev)] = 0
+    del is_list
+    s_h = g_succ.cpu().numpy().view(np.uint64).copy()
+    r_h = g_rank.cpu().numpy().copy()
+    del g_succ, g_rank
+    if oracle_mod.has_ref():
+        oracle_mod.ref_local_pointer_chasing(s_h, r_h)
+    else:
+        oracle_mod.local_pointer_chasing(s_h, r_h)
+    exp_root = torch.from_numpy(s_h.view(np.int64)).to(dev) - off
+    exp_rank = torch.from_numpy(r_h).to(dev)
+    bad = (exp_root != root) | (exp_rank != rank)
+    assert not bool(bad.any()), f"{int(bad.sum())} elements differ, first at {int(bad.nonzero()[0])}"

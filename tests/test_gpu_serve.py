@@ -4,6 +4,7 @@ release; statistics."""
 from __future__ import annotations
 
 import threading
+import time
 
 import numpy as np
 import pytest
@@ -115,3 +116,39 @@ def test_device_submission_and_results(kb, oracle_mod):
     srv.release(a)
     srv.release(b)
     srv.close()
+
+
+def test_continuous_batching_overlaps_and_results_exact(kb, oracle_mod):
+    """Requests up to 2^22 elements, large ones submitted first and small ones
+    streamed while the large batches run: both lanes run batches, some
+    requests are admitted and some batches start while another batch is in
+    flight (the server's own counters), and every result equals the oracle
+    and the same request ranked alone."""
+    rng = np.random.default_rng(0x5E)
+    large = _requests(oracle_mod, 16, seed=21, lo=18, hi=22)
+    small = _requests(oracle_mod, 120, seed=22, lo=8, hi=16)
+    srv = kb.Server(small_max=1 << 16, small_batch_elements=1 << 19)
+    ids_l = [srv.submit(kind, inp, w) for kind, inp, w in large]
+    ids_s = []
+    for kind, inp, w in small:
+        ids_s.append(srv.submit(kind, inp, w))
+        time.sleep(float(rng.exponential(2e-4)))
+    for rid, (kind, inp, w) in zip(ids_l + ids_s, large + small):
+        srv.wait(rid, 300.0)
+        root, rank = srv.fetch(rid)
+        r_o, k_o = _expected(oracle_mod, kind, inp, w)
+        np.testing.assert_array_equal(root, r_o)
+        np.testing.assert_array_equal(rank, k_o)
+        if kind == 0:
+            r_a, k_a = kb.rank_list_host(inp, w)
+        else:
+            r_a, k_a = kb.root_forest_host(inp)
+        np.testing.assert_array_equal(root, r_a)
+        np.testing.assert_array_equal(rank, k_a)
+        srv.release(rid)
+    st = srv.stats()
+    srv.close()
+    assert st["completed"] == len(large) + len(small)
+    assert st["lane_batches"][0] > 0 and st["lane_batches"][1] > 0, st
+    assert st["admitted_while_running"] > 0, st
+    assert st["batches_started_overlapping"] > 0, st

@@ -94,3 +94,34 @@ def test_noalloc_allocates_no_device_memory():
     exp_root, exp_rank = oracle.rank_list(oracle.gen_list(n, 0xA4, 1))
     assert np.array_equal(rank.cpu().numpy().view(np.uint64), exp_rank)
     assert np.array_equal(root.cpu().numpy().view(np.uint64), exp_root)
+
+
+def test_noalloc_error_statuses_then_a_valid_call():
+    """An out-of-range successor and rootless cycles (two elements, and one
+    long cycle) return their statuses; the next valid call still equals
+    kascade_rank_list."""
+    import kascade_b200 as kb
+    import oracle
+
+    names = kb._lib.STATUS_NAMES
+    n = 5000
+    bad = oracle.gen_list(n, 0xA5, 0)
+    bad[123] = n + 9
+    st, _, _ = _noalloc_rank(kb.lib, torch.from_numpy(bad.view(np.int64)).cuda(), None)
+    assert names[st] == "OUT_OF_RANGE"
+    two = np.arange(n, dtype=np.uint64)
+    two[10], two[11] = 11, 10  # a rootless 2-cycle beside n - 2 roots
+    st, _, _ = _noalloc_rank(kb.lib, torch.from_numpy(two.view(np.int64)).cuda(), None)
+    assert names[st] == "CYCLE"
+    ring = np.roll(np.arange(40000, dtype=np.uint64), 1)  # one rootless cycle
+    st, _, _ = _noalloc_rank(kb.lib, torch.from_numpy(ring.view(np.int64)).cuda(), None)
+    assert names[st] == "CYCLE"
+    ctx = ctypes.c_void_p()
+    assert kb.lib.kascade_ctx_create(0, ctypes.byref(ctx)) == 0
+    try:
+        s = torch.from_numpy(oracle.gen_list(20000, 0xA6, 1).view(np.int64)).cuda()
+        r_ref, k_ref = _reference_rank(kb.lib, ctx, s, None)
+        st, r, k = _noalloc_rank(kb.lib, s, None)
+        assert st == 0 and torch.equal(r, r_ref) and torch.equal(k, k_ref)
+    finally:
+        kb.lib.kascade_ctx_destroy(ctx)
