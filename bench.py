@@ -749,7 +749,8 @@ def main():
     ap.add_argument("--spacing", type=int, default=0)
     ap.add_argument("--chains", type=int, default=0)
     ap.add_argument("--block", type=int, default=0, help="chase block size override (128, 256 or 512)")
-    ap.add_argument("--n", type=int, default=0, help="override the workload size (profiling runs)")
+    ap.add_argument("--n", "--elements", dest="n", type=int, default=0,
+                    help="override the workload size (profiling runs)")
     ap.add_argument("--level0-mode", type=int, default=0, help="0 auto, 1 stamping chase, 2 write-free chase")
     ap.add_argument("--calibrate", action="store_true",
                     help="measure the random 16 B access rate of this GPU (2^28 records) and exit")

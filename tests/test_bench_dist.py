@@ -54,7 +54,7 @@ def test_whole_job_takes_the_slowest_rank_and_every_ranks_elements(tmp_path):
 
 def test_reference_arm_prints_one_line_from_rank_zero(oracle_mod):
     res = _torchrun(["bench.py", "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "0",
-                     "--cpu-sample", "65536", "--n", "1048576"])
+                     "--cpu-sample", "65536", "--elements", "1048576"])
     assert res.returncode == 0, res.stderr[-2000:]
     lines = [d for d in _json_lines(res.stdout) if d.get("impl") == "reference"]
     assert len(lines) == 1
