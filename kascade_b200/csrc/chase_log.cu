@@ -267,9 +267,6 @@ __device__ uint32_t block_exclusive_scan(uint32_t* v, uint32_t m) {
 //     holds the entries of a few hundred chains, so most of these lookups
 //     hit L1.  Entries of elements at or above `limit` (tour down edges: no
 //     output) are only counted, in `beyond`
-//     With no fill table the source is a flat array of `limit` entries, and
-//     with no ruler results the entries pass through unchanged (tour records
-//     on their way to their slots).
 //   otherwise (second pass): tiles inside one window's region, buckets are
 //     its SUBS sub-windows
 // More entries than a bucket holds means some element was logged twice.
@@ -522,45 +519,6 @@ __global__ void k_hop_cap_status(DevStatus* st) {
   if (st->counter[0]) set_error(st, KASCADE_ERR_TIMEOUT, st->counter[0]);
 }
 
-// Records to their slots: one sub-window (SUB slots) per block iteration.
-// Every slot receives exactly one entry (slot, successor, tag, weight); the
-// records are assembled in shared memory and written densely.
-__global__ void __launch_bounds__(FIN_THREADS, 2) k_place_rec(const LogEnt* __restrict__ part2,
-                                                                const uint32_t* __restrict__ cursor2, uint32_t nb,
-                                                                uint32_t n, Rec* __restrict__ rec, DevStatus* st) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  uint32_t* b_s = reinterpret_cast<uint32_t*>(smraw);  // successors (NO_ROOT: slot not seen yet)
-  uint32_t* c_s = b_s + SUB;                            // tags
-  uint32_t* a_s = c_s + SUB;                            // weights
-  const uint32_t items = nb * SUBS;
-  for (uint32_t it = blockIdx.x; it < items; it += gridDim.x) {
-    const uint32_t lo = it * SUB;
-    if (lo >= n) continue;  // block-uniform
-    const uint32_t len = min(SUB, n - lo);
-    const uint32_t cnt = min(__ldcg(cursor2 + (uint64_t)it * CURSOR_STRIDE), SUB);
-    for (uint32_t i = threadIdx.x; i < SUB; i += FIN_THREADS) b_s[i] = NO_ROOT;
-    __syncthreads();
-    const LogEnt* src = part2 + (uint64_t)it * SUB;
-    for (uint32_t i = threadIdx.x; i < cnt; i += FIN_THREADS) {
-      const uint4 e = __ldcs(reinterpret_cast<const uint4*>(src + i));
-      const uint32_t xl = e.x - lo;
-      if (xl >= len || atomicExch(&b_s[xl], e.y) != NO_ROOT) {
-        set_error(st, KASCADE_ERR_NOT_A_LIST, e.x);  // a slot given twice (or not this sub-window's)
-        continue;
-      }
-      c_s[xl] = e.z;
-      a_s[xl] = e.w;
-    }
-    __syncthreads();
-    for (uint32_t i = threadIdx.x; i < len; i += FIN_THREADS) {
-      const uint32_t b = b_s[i];
-      if (b == NO_ROOT) set_error(st, KASCADE_ERR_NOT_A_LIST, lo + i);  // a slot without its record
-      __stcg(reinterpret_cast<uint4*>(rec + lo + i), make_uint4(a_s[i], 0u, b == NO_ROOT ? lo + i : b, c_s[i]));
-    }
-    __syncthreads();
-  }
-}
-
 constexpr uint32_t TILE1 = PT_THREADS * P1_ITEMS, TILE2 = PT_THREADS * P2_ITEMS;
 auto k_part1 = k_partition<true, P1_ITEMS, P1_BLOCKS>;
 auto k_part2 = k_partition<false, P2_ITEMS, P2_BLOCKS>;
@@ -579,8 +537,6 @@ kascade_status raise_smem_limits() {
                                (int)(TILE2 * sizeof(LogEnt) + 2 * sizeof(uint32_t) * SUBS)));
   KS_CUDA(cudaFuncSetAttribute(k_place, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)(SUB * (sizeof(unsigned long long) + sizeof(uint32_t)))));
-  KS_CUDA(cudaFuncSetAttribute(k_place_rec, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)(SUB * 3 * sizeof(uint32_t))));
   raised.fetch_or(bit);
   return KASCADE_OK;
 }
@@ -728,38 +684,6 @@ kascade_status rank_level0_log(kascade_ctx& ctx, const Rec* rec, uint32_t n, uin
     KS_CHECK_LAUNCH();
   }
   if (r0_dev) return report_dev_levels(ctx, lv, levels, n, s);
-  return KASCADE_OK;
-}
-
-kascade_status place_records(kascade_ctx& ctx, uint4* entries, uint32_t n, Rec* rec, cudaStream_t s) {
-  if (n == 0) return KASCADE_OK;
-  const uint32_t nb = (uint32_t)(((uint64_t)n + WIN - 1) / WIN);
-  const uint32_t nchunks = (uint32_t)(((uint64_t)n + LOG_CHUNK - 1) / LOG_CHUNK);
-  LogEnt* src = reinterpret_cast<LogEnt*>(entries);
-  LogEnt* part = alloc<LogEnt>(ctx, (uint64_t)nb * WIN);
-  uint32_t* cursor = alloc<uint32_t>(ctx, (uint64_t)nb * (SUBS + 1) * CURSOR_STRIDE + CURSOR_STRIDE);
-  if (!part || !cursor) return KASCADE_ERR_OOM;
-  uint32_t* cursor1 = cursor;
-  uint32_t* cursor2 = cursor + (uint64_t)nb * CURSOR_STRIDE;
-  uint32_t* beyond = cursor2 + (uint64_t)nb * SUBS * CURSOR_STRIDE;  // stays 0: every slot is below n
-  KS_CUDA(cudaMemsetAsync(cursor, 0, sizeof(uint32_t) * ((uint64_t)nb * (SUBS + 1) * CURSOR_STRIDE + CURSOR_STRIDE),
-                          s));
-  KS_TRY(raise_smem_limits());
-  ProfScope ps(ctx, "tour_place", s);
-  const size_t smem1 = TILE1 * sizeof(LogEnt) + 2 * sizeof(uint32_t) * nb;
-  const size_t smem2 = TILE2 * sizeof(LogEnt) + 2 * sizeof(uint32_t) * SUBS;
-  const uint32_t tiles1 = (nchunks + TILE1 / LOG_CHUNK - 1) / (TILE1 / LOG_CHUNK);
-  k_part1<<<(unsigned)std::min<uint64_t>(tiles1, (uint64_t)ctx.usable_sms() * P1_BLOCKS), PT_THREADS, smem1, s>>>(
-      src, nullptr, nchunks, nullptr, n, nb, part, cursor1, beyond, ctx.d_status);
-  KS_CHECK_LAUNCH();
-  // the entries are dead after the first pass: the second writes over them
-  const uint32_t tiles2 = nb * (WIN / TILE2);
-  k_part2<<<(unsigned)std::min<uint64_t>(tiles2, (uint64_t)ctx.usable_sms() * P2_BLOCKS), PT_THREADS, smem2, s>>>(
-      part, cursor1, 0, nullptr, n, nb, src, cursor2, beyond, ctx.d_status);
-  KS_CHECK_LAUNCH();
-  k_place_rec<<<(unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)nb * SUBS, (uint64_t)ctx.usable_sms() * 2)),
-                FIN_THREADS, SUB * 3 * sizeof(uint32_t), s>>>(src, cursor2, nb, n, rec, ctx.d_status);
-  KS_CHECK_LAUNCH();
   return KASCADE_OK;
 }
 

@@ -53,13 +53,21 @@ __global__ void __launch_bounds__(256) k_seg_bounds(const uint32_t* __restrict__
 
 constexpr uint32_t NO_CHILD = 0xFFFFFFFFu;
 
-// Where the records of a batch's forest tours live.  The forests are
-// compacted into one vertex space with per-forest bases fd[j]; the up edge of
-// compact vertex c of forest j sits at that vertex's position in the caller's
-// concatenated arrays (foff[j] + c - fd[j]), the down edge of sorted child
-// entry q after all input elements (down_base + q).  Ruler sampling
-// thresholds can differ per forest (size classes).  Rotation at a vertex:
-// parent first, then children in increasing id.
+// Where a forest's tour records live, by vertex.  A single forest of n
+// vertices: up edge of v at slot v, down edge into v at slot n + v.  A batch
+// of forests, compacted into one vertex space with per-forest bases fd[j]:
+// the up edge of compact vertex c of forest j at that vertex's position in
+// the caller's concatenated arrays (foff[j] + c - fd[j]), the down edge into
+// c after all input elements (down_base + c).  Ruler sampling thresholds can
+// differ per forest (size classes).
+struct SlotsSingle {
+  uint32_t n;
+  uint32_t th;
+  __device__ __forceinline__ uint32_t seg_of(uint32_t) const { return 0; }
+  __device__ __forceinline__ uint32_t up(uint32_t v, uint32_t) const { return v; }
+  __device__ __forceinline__ uint32_t down(uint32_t v) const { return n + v; }
+  __device__ __forceinline__ uint32_t thresh(uint32_t) const { return th; }
+};
 
 struct SlotsBatch {
   const uint32_t* fd;       // nf + 1 compact starts
@@ -79,116 +87,9 @@ struct SlotsBatch {
     return lo;
   }
   __device__ __forceinline__ uint32_t up(uint32_t c, uint32_t j) const { return c - __ldg(fd + j) + __ldg(foff + j); }
-  __device__ __forceinline__ uint32_t down(uint64_t q) const { return down_base + (uint32_t)q; }
+  __device__ __forceinline__ uint32_t down(uint32_t c) const { return down_base + c; }
   __device__ __forceinline__ uint32_t thresh(uint32_t j) const { return __ldg(fthresh + j); }
 };
-
-// Writes both tour records of every sorted child entry q of a batch's
-// forests, samples rulers among the written slots and numbers them (one
-// atomic per tile, as in prepare).  The first child comes from the segment
-// table.
-template <class Slots>
-__global__ void __launch_bounds__(256) k_tour_build(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
-                                                    uint32_t n, const uint2* __restrict__ seg,
-                                                    const uint32_t* __restrict__ root_bits, Rec* __restrict__ rec,
-                                                    uint32_t* __restrict__ ruler_elem, uint32_t* __restrict__ counter,
-                                                    uint32_t salt, Slots slots, DevStatus* st) {
-  __shared__ uint32_t sm[33];
-  __shared__ uint32_t sbase;
-  const uint64_t tile_sz = (uint64_t)blockDim.x * TB_ITEMS;
-  for (uint64_t tile = (uint64_t)blockIdx.x * tile_sz; tile < n; tile += (uint64_t)gridDim.x * tile_sz) {
-    Rec ru[TB_ITEMS], rd[TB_ITEMS];
-    uint32_t su[TB_ITEMS], sd[TB_ITEMS];
-    uint32_t rl = 0, cnt = 0;
-#pragma unroll
-    for (int i = 0; i < TB_ITEMS; ++i) {
-      const uint64_t q = tile + (uint64_t)i * blockDim.x + threadIdx.x;
-      su[i] = sd[i] = 0;
-      if (q >= n) continue;
-      const uint32_t p = keys[q], c = vals[q];
-      const uint32_t j = slots.seg_of(p);  // p and c belong to the same forest
-      const uint32_t th = slots.thresh(j);
-      const uint32_t slot_down = slots.down(q);
-      if (p == c) {
-        // root r = p: terminal slot of r and the unused down slot, both self loops
-        const uint32_t slot_root = slots.up(p, j);
-        ru[i].a = 0;
-        ru[i].b = slot_root;
-        su[i] = slot_root;
-        rd[i].a = 0;
-        rd[i].b = slot_down;
-        sd[i] = slot_down;
-        rl |= 3u << (2 * i);
-        cnt += 2;
-      } else {
-        // up edge c -> p: continue with p's next child, else leave p
-        uint64_t q1 = q + 1;
-        if (q1 < n && keys[q1] == p && vals[q1] == p) q1++;
-        const uint32_t succ_up = (q1 < n && keys[q1] == p) ? slots.down(q1) : slots.up(p, j);
-        const uint32_t slot_up = slots.up(c, j);
-        ru[i].a = 1ull;
-        ru[i].b = succ_up;
-        su[i] = slot_up;
-        // down edge p -> c: descend to c's first child, else come back up
-        uint32_t first_child = NO_CHILD;
-        const uint2 sg = seg[c];
-        if (sg.x < sg.y) first_child = sg.x;
-        rd[i].a = ~0ull;  // -1
-        rd[i].b = (first_child != NO_CHILD) ? slots.down(first_child) : slot_up;
-        sd[i] = slot_down;
-        // the down edge to a root's first child is the head of that tree's
-        // tour: make it a ruler so that no tour element is left unreached
-        bool head = false;
-        bool first = true;
-        if (q > 0 && keys[q - 1] == p) first = (vals[q - 1] == p) && (q < 2 || keys[q - 2] != p);
-        // p is a root: its bit came from the sort's first pass (an L2-resident
-        // bitmap instead of a search of p's children)
-        if (first) head = (__ldg(root_bits + (p >> 5)) >> (p & 31)) & 1u;
-        if (sampled(slot_up, salt, th)) {
-          rl |= 1u << (2 * i);
-          cnt++;
-        }
-        if (head || sampled(slot_down, salt, th)) {
-          rl |= 2u << (2 * i);
-          cnt++;
-        }
-      }
-    }
-    uint32_t total;
-    uint32_t pre = block_exclusive_scan(cnt, sm, &total);
-    if (threadIdx.x == 0) {
-      uint32_t b = total ? atomicAdd(counter, total) : 0u;
-      if ((uint64_t)b + total > MAX_RULERS) set_error(st, KASCADE_ERR_TOO_LARGE, b);
-      sbase = b;
-    }
-    __syncthreads();
-    uint32_t id = sbase + pre;
-#pragma unroll
-    for (int i = 0; i < TB_ITEMS; ++i) {
-      const uint64_t q = tile + (uint64_t)i * blockDim.x + threadIdx.x;
-      if (q >= n) continue;
-      ru[i].c = TAG_UNREACHED;
-      rd[i].c = TAG_UNREACHED;
-      if ((rl >> (2 * i)) & 1u) {
-        if (id < MAX_RULERS) {
-          ru[i].c = TAG_RULER | id;
-          ruler_elem[id] = su[i];
-        }
-        id++;
-      }
-      if ((rl >> (2 * i)) & 2u) {
-        if (id < MAX_RULERS) {
-          rd[i].c = TAG_RULER | id;
-          ruler_elem[id] = sd[i];
-        }
-        id++;
-      }
-      rec[su[i]] = ru[i];
-      rec[sd[i]] = rd[i];
-    }
-    __syncthreads();
-  }
-}
 
 // Child lists of a single forest: fc[p] = one child of p (NO_CHILD: a leaf),
 // nsib[v] = v's next sibling (NO_CHILD: the last one).  A warp's vertices that
@@ -233,26 +134,33 @@ __global__ void __launch_bounds__(256) k_link_children(const uint64_t* __restric
 // The down edge into a root's first child is the head of that tree's tour
 // and always a ruler, so no tour element is left unreached; roots' slots are
 // self loops (the terminal, and an unused down slot) and rulers.
+template <class Slots>
 __global__ void __launch_bounds__(256) k_tour_links(const uint64_t* __restrict__ parent, uint32_t n,
                                                     const uint32_t* __restrict__ fc,
                                                     const uint32_t* __restrict__ nsib,
                                                     const uint32_t* __restrict__ root_bits, Rec* __restrict__ rec,
                                                     uint32_t* __restrict__ ruler_elem, uint32_t* __restrict__ counter,
-                                                    uint32_t salt, uint32_t th, DevStatus* st) {
+                                                    uint32_t salt, Slots slots, DevStatus* st) {
   __shared__ uint32_t sm[33];
   __shared__ uint32_t sbase;
   const uint64_t tile_sz = (uint64_t)blockDim.x * TB_ITEMS;
   for (uint64_t tile = (uint64_t)blockIdx.x * tile_sz; tile < n; tile += (uint64_t)gridDim.x * tile_sz) {
     Rec ru[TB_ITEMS], rd[TB_ITEMS];
+    uint32_t su[TB_ITEMS], sd[TB_ITEMS];
     uint32_t rl = 0, cnt = 0;
 #pragma unroll
     for (int i = 0; i < TB_ITEMS; ++i) {
       const uint64_t v = tile + (uint64_t)i * blockDim.x + threadIdx.x;
+      su[i] = sd[i] = 0;
       if (v >= n) continue;
       uint64_t p = __ldcs(reinterpret_cast<const unsigned long long*>(parent) + v);
       if (p >= n) p = v;  // reported by k_link_children
       const uint32_t sib = __ldcs(nsib + v), first = __ldcs(fc + v);
-      const uint32_t up = (uint32_t)v, down = n + (uint32_t)v;
+      const uint32_t j = slots.seg_of((uint32_t)v);  // v and p belong to the same forest
+      const uint32_t th = slots.thresh(j);
+      const uint32_t up = slots.up((uint32_t)v, j), down = slots.down((uint32_t)v);
+      su[i] = up;
+      sd[i] = down;
       if (p == v) {
         ru[i].a = 0;
         ru[i].b = up;
@@ -263,9 +171,9 @@ __global__ void __launch_bounds__(256) k_tour_links(const uint64_t* __restrict__
         continue;
       }
       ru[i].a = 1ull;
-      ru[i].b = (sib != NO_CHILD) ? n + sib : (uint32_t)p;
+      ru[i].b = (sib != NO_CHILD) ? slots.down(sib) : slots.up((uint32_t)p, j);
       rd[i].a = ~0ull;  // -1
-      rd[i].b = (first != NO_CHILD) ? n + first : up;
+      rd[i].b = (first != NO_CHILD) ? slots.down(first) : up;
       bool head = false;
       if ((__ldg(root_bits + (p >> 5)) >> (p & 31)) & 1u) head = __ldg(fc + p) == (uint32_t)v;
       if (sampled(up, salt, th)) {
@@ -295,19 +203,19 @@ __global__ void __launch_bounds__(256) k_tour_links(const uint64_t* __restrict__
       if ((rl >> (2 * i)) & 1u) {
         if (id < MAX_RULERS) {
           ru[i].c = TAG_RULER | id;
-          ruler_elem[id] = (uint32_t)v;
+          ruler_elem[id] = su[i];
         }
         id++;
       }
       if ((rl >> (2 * i)) & 2u) {
         if (id < MAX_RULERS) {
           rd[i].c = TAG_RULER | id;
-          ruler_elem[id] = n + (uint32_t)v;
+          ruler_elem[id] = sd[i];
         }
         id++;
       }
-      st_rec_cs(rec + v, ru[i]);
-      st_rec_cs(rec + n + v, rd[i]);
+      st_rec_cs(rec + su[i], ru[i]);
+      st_rec_cs(rec + sd[i], rd[i]);
     }
     __syncthreads();
   }
@@ -377,22 +285,43 @@ __global__ void __launch_bounds__(256) k_ref_tour(const uint64_t* __restrict__ p
   }
 }
 
+// The reference-numbered tour's children array: (parent, child) pairs
+// sorted by parent (stable, so children in increasing id), and each
+// vertex's segment of it.
 kascade_status sort_children(kascade_ctx& ctx, const uint64_t* parent, uint32_t n, uint32_t** keys, uint32_t** vals,
-                             uint2** seg, uint32_t** root_bits, cudaStream_t s) {
+                             uint2** seg, cudaStream_t s) {
   SortSource src;
   src.parent = parent;
-  if (root_bits) {
-    *root_bits = alloc<uint32_t>(ctx, ((uint64_t)n + 31) / 32 + 1);
-    if (!*root_bits) return KASCADE_ERR_OOM;
-    src.root_bits = *root_bits;
-  }
   KS_TRY(radix_sort_pairs(ctx, src, n, bits_for(n), keys, vals, s));
-  if (!seg) return KASCADE_OK;
   *seg = alloc<uint2>(ctx, n);
   if (!*seg) return KASCADE_ERR_OOM;
   KS_CUDA(cudaMemsetAsync(*seg, 0, sizeof(uint2) * (size_t)n, s));
   ProfScope ps(ctx, "seg_bounds", s);
   k_seg_bounds<<<grid_for(ctx, n, 256, 8), 256, 0, s>>>(*keys, n, *seg);
+  KS_CHECK_LAUNCH();
+  return KASCADE_OK;
+}
+
+// Child lists of the forest (parent[v], n vertices, one vertex space) and
+// both tour records of every vertex at the slots `slots` gives; ruler ids
+// continue `counter`.
+template <class Slots>
+kascade_status build_tour(kascade_ctx& ctx, const uint64_t* parent, uint32_t n, const Slots& slots, Rec* rec,
+                          uint32_t* ruler_elem, uint32_t* counter, uint32_t salt, cudaStream_t s) {
+  uint32_t* fc = alloc<uint32_t>(ctx, n);
+  uint32_t* nsib = alloc<uint32_t>(ctx, n);
+  uint32_t* root_bits = alloc<uint32_t>(ctx, ((uint64_t)n + 31) / 32);
+  if (!fc || !nsib || !root_bits) return KASCADE_ERR_OOM;
+  {
+    ProfScope ps(ctx, "link_children", s);
+    KS_CUDA(cudaMemsetAsync(fc, 0xFF, sizeof(uint32_t) * (size_t)n, s));
+    k_link_children<<<grid_for(ctx, n, 256, 8), 256, 0, s>>>(parent, n, fc, nsib, root_bits, ctx.d_status);
+    KS_CHECK_LAUNCH();
+  }
+  ProfScope ps(ctx, "tour_build", s);
+  const unsigned grid = grid_for(ctx, ((uint64_t)n + 256 * TB_ITEMS - 1) / (256 * TB_ITEMS) * 256, 256, 8);
+  k_tour_links<Slots><<<grid, 256, 0, s>>>(parent, n, fc, nsib, root_bits, rec, ruler_elem, counter, salt, slots,
+                                           ctx.d_status);
   KS_CHECK_LAUNCH();
   return KASCADE_OK;
 }
@@ -407,25 +336,10 @@ kascade_status root_forest_impl(kascade_ctx& ctx, const uint64_t* parent, uint32
   Rec* rec = alloc<Rec>(ctx, m);
   uint32_t* ruler_elem = alloc<uint32_t>(ctx, m);
   uint32_t* ctr = alloc<uint32_t>(ctx, 1);
-  uint32_t* fc = alloc<uint32_t>(ctx, n);
-  uint32_t* nsib = alloc<uint32_t>(ctx, n);
-  uint32_t* root_bits = alloc<uint32_t>(ctx, ((uint64_t)n + 31) / 32);
-  if (!rec || !ruler_elem || !ctr || !fc || !nsib || !root_bits) return KASCADE_ERR_OOM;
+  if (!rec || !ruler_elem || !ctr) return KASCADE_ERR_OOM;
   KS_CUDA(cudaMemsetAsync(ctr, 0, sizeof(uint32_t), s));
-  {
-    ProfScope ps(ctx, "link_children", s);
-    KS_CUDA(cudaMemsetAsync(fc, 0xFF, sizeof(uint32_t) * (size_t)n, s));
-    k_link_children<<<grid_for(ctx, n, 256, 8), 256, 0, s>>>(parent, n, fc, nsib, root_bits, ctx.d_status);
-    KS_CHECK_LAUNCH();
-  }
-  {
-    ProfScope ps(ctx, "tour_build", s);
-    const unsigned grid = grid_for(ctx, ((uint64_t)n + 256 * TB_ITEMS - 1) / (256 * TB_ITEMS) * 256, 256, 8);
-    const uint32_t th = (uint32_t)(4294967296.0 / (double)(p.spacing0 < 2 ? 2 : p.spacing0));
-    k_tour_links<<<grid, 256, 0, s>>>(parent, n, fc, nsib, root_bits, rec, ruler_elem, ctr,
-                                      mix32(p.seed ^ 0x70757254u), th, ctx.d_status);
-    KS_CHECK_LAUNCH();
-  }
+  const SlotsSingle slots{n, (uint32_t)(4294967296.0 / (double)(p.spacing0 < 2 ? 2 : p.spacing0))};
+  KS_TRY(build_tour(ctx, parent, n, slots, rec, ruler_elem, ctr, mix32(p.seed ^ 0x70757254u), s));
   SinkTour sink{root_out, depth_out, n, keep_roots};
   if (device_levels && m > p.base_max && p.max_levels > 0) {
     if (m < p.level0_log_min)
@@ -445,20 +359,8 @@ kascade_status batch_tours(kascade_ctx& ctx, const uint64_t* fpar, uint32_t F, c
                            const uint32_t* fthresh, uint32_t nf, uint32_t down_base, Rec* rec, uint32_t* ruler_elem,
                            uint32_t* counter, uint32_t salt, cudaStream_t s) {
   if (F == 0) return KASCADE_OK;
-  uint32_t *keys, *vals;
-  uint2* seg;
-  uint32_t* root_bits = nullptr;
-  KS_TRY(sort_children(ctx, fpar, F, &keys, &vals, &seg, &root_bits, s));
-  SlotsBatch slots{fd, foff, fthresh, nf, down_base};
-  // up records straight to their slots: a batch's forests are small, so these
-  // writes stay in L2 (staging them for place_records measured slower here:
-  // 4.4 vs 3.0 ms on the 2^28 batch)
-  ProfScope ps(ctx, "tour_build", s);
-  const unsigned grid = grid_for(ctx, ((uint64_t)F + 256 * TB_ITEMS - 1) / (256 * TB_ITEMS) * 256, 256, 8);
-  k_tour_build<SlotsBatch><<<grid, 256, 0, s>>>(keys, vals, F, seg, root_bits, rec, ruler_elem, counter, salt, slots,
-                                                ctx.d_status);
-  KS_CHECK_LAUNCH();
-  return KASCADE_OK;
+  const SlotsBatch slots{fd, foff, fthresh, nf, down_base};
+  return build_tour(ctx, fpar, F, slots, rec, ruler_elem, counter, salt, s);
 }
 
 kascade_status compute_euler_tour_impl(kascade_ctx& ctx, const uint64_t* parent, uint32_t n, uint64_t* tour,
@@ -467,7 +369,7 @@ kascade_status compute_euler_tour_impl(kascade_ctx& ctx, const uint64_t* parent,
   if (n == 0) return KASCADE_OK;
   uint32_t *keys, *vals;
   uint2* seg;
-  KS_TRY(sort_children(ctx, parent, n, &keys, &vals, &seg, nullptr, s));
+  KS_TRY(sort_children(ctx, parent, n, &keys, &vals, &seg, s));
   uint32_t* deg = alloc<uint32_t>(ctx, n);
   uint32_t* droot = alloc<uint32_t>(ctx, n);
   uint32_t* xadj = alloc<uint32_t>(ctx, n);

@@ -204,11 +204,6 @@ kascade_status rank_level0_log(kascade_ctx& ctx, const Rec* rec, uint32_t n, uin
                                const uint32_t* ruler_elem0, const LogTarget& t, const Params& p,
                                cudaStream_t s, const uint32_t* r0_dev = nullptr);
 
-// Records built out of order -- entries (slot, successor, tag, weight), one
-// per slot 0..n-1, in any order -- placed at their slots: two radix passes
-// by slot and a dense placement, no random store.  `entries` is overwritten
-// and must hold ceil(n / 2^13) * 2^13 entries.
-kascade_status place_records(kascade_ctx& ctx, uint4* entries, uint32_t n, Rec* rec, cudaStream_t s);
 
 // Pointer doubling on level-0 records (tags ignored).
 template <class Sink>

@@ -123,11 +123,6 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_hist(SortSource src, cons
           kv[i] = keys[x];
         }
       }
-      if (FROM_PARENT && src.root_bits) {
-        // a warp's 32 consecutive elements make one word of root bits
-        const uint32_t bits = __ballot_sync(0xffffffffu, x < n && kv[i] == (uint32_t)x);
-        if ((threadIdx.x & 31) == 0 && x < n) src.root_bits[x >> 5] = bits;
-      }
     }
 #pragma unroll
     for (int i = 0; i < SORT_ITEMS; ++i) {

@@ -18,9 +18,6 @@ struct SortSource {
   const uint64_t* parent = nullptr;
   const uint32_t* keys = nullptr;
   const uint32_t* vals = nullptr;
-  // with parent: receives bit i = (parent[i] == i), one word per 32
-  // elements, written by the first pass (optional)
-  uint32_t* root_bits = nullptr;
 };
 
 // Stable sort of n pairs by key, keys < 2^key_bits.  Scratch comes from the
