@@ -12,7 +12,7 @@ ORACLE_SO = HERE / "_build" / "libkascade_oracle.so"
 REF_SO = HERE / "_ref" / "libkascade_ref.so"
 
 __all__ = [
-    "compute_stats", "compute_stats_transcribed",
+    "compute_stats", "compute_stats_transcribed", "euler_tour_transcribed",
     "build", "has_ref", "rank_list", "root_forest", "local_pointer_chasing", "pointer_doubling",
     "euler_tour", "rank_via_euler_tour", "is_list", "pack", "unpack", "gen_list", "gen_weights",
     "gen_forest", "ref_gather_rank", "ref_local_pointer_chasing",
@@ -321,3 +321,70 @@ def compute_stats_transcribed(root, rank, level: int) -> tuple[dict, list]:
     out = dict(basic)
     out.update(ext)
     return out, (per_tree if level >= 4 else [])
+
+
+def euler_tour_transcribed(parent) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """compute_euler_tour for one rank, transcribed statement by statement in
+    plain Python (small inputs): the forest as reverse_rooted_tree(...,
+    add_back_edge=true) sends it (lib/kascade/successor_utils.cpp:265-300),
+    the CSR graph as make_graph fills it -- each vertex's adjacency from its
+    end backwards, in arrival order (successor_utils.cpp:236-260) -- and the
+    tour as compute_euler_tour_impl builds it (lib/kascade/eulertour.cpp:
+    33-127): edge ids in CSR order, succ[(u_prev, v)] = (v, u) with u_prev
+    the neighbour before u in v's rotation, the first edge into each root
+    (with neighbours) pointing at that root's dummy element, elements without
+    a message left as self loops.  Returns (succ, weight, is_upward).  An
+    independent check of the C restatement, which derives the same numbering
+    by formulas."""
+    parent = [int(x) for x in np.asarray(parent, dtype=np.uint64)]
+    n = len(parent)
+    # reverse_rooted_tree, one rank: the back edge first, then the edge to
+    # the parent's owner (the same rank), for each non-root i in order
+    recv_edges = []
+    for i in range(n):
+        if parent[i] == i:  # is_root (successor_utils.cpp:65-70)
+            continue
+        recv_edges.append((i, parent[i]))
+        recv_edges.append((parent[i], i))
+    # make_graph
+    xadj = [0] * (n + 1)
+    adjncy = [0] * len(recv_edges)
+    for src, _ in recv_edges:
+        xadj[src] += 1
+    for k in range(1, n + 1):  # std::inclusive_scan
+        xadj[k] += xadj[k - 1]
+    for src, dst in recv_edges:
+        xadj[src] -= 1
+        adjncy[xadj[src]] = dst
+    # compute_euler_tour_impl
+    is_root = {v for v in range(n) if parent[v] == v}
+    num_list_elems = len(adjncy) + len(is_root)
+    weight = [0] * num_list_elems
+    upward = [False] * num_list_elems
+    edge_to_index = {}
+    messages = []
+    next_id = 0
+    root_index = len(adjncy)
+    for v in range(n):
+        neighbors = adjncy[xadj[v]:xadj[v + 1]]
+        degree = len(neighbors)
+        for i in range(degree):
+            u_prev = neighbors[(i + degree - 1) % degree]
+            u = neighbors[i]
+            edge_to_index[(v, u)] = next_id
+            up = parent[v] == u
+            weight[next_id] = 1 if up else -1
+            upward[next_id] = up
+            if v in is_root and i == 0:
+                messages.append((u_prev, v, root_index))
+                weight[root_index] = 0
+                upward[root_index] = False
+                edge_to_index[(v, v)] = root_index
+                root_index += 1
+            else:
+                messages.append((u_prev, v, next_id))
+            next_id += 1
+    succ = list(range(num_list_elems))
+    for u, v, nxt in messages:
+        succ[edge_to_index[(u, v)]] = nxt
+    return np.array(succ, np.uint64), np.array(weight, np.int64), np.array(upward, bool)

@@ -144,3 +144,29 @@ def test_forest_with_rootless_cycle_reports_error(kb, oracle_mod, level0_mode):
     np.testing.assert_array_equal(host_u64(root), root_o)
     np.testing.assert_array_equal(host_u64(depth), depth_o)
     ctx.close()
+
+
+def test_compute_euler_tour_vs_reference_transcription(kb, oracle_mod):
+    """kascade_compute_euler_tour against the statement-by-statement
+    transcription of the reference's tour construction (reverse_rooted_tree,
+    make_graph, compute_euler_tour_impl) on forests with several roots,
+    isolated roots, a star and vertices of high degree."""
+    rng = np.random.default_rng(0xE8)
+    forests = [np.array([0], np.uint64), np.array([0, 1, 2], np.uint64), np.array([0] * 6, np.uint64),
+               np.array([1, 2, 3, 4, 4], np.uint64),
+               np.array([3, 3, 3, 3, 2, 2, 6, 6, 9, 9, 0, 6, 11, 13], np.uint64)]
+    for n in (24, 41, 64, 500):
+        par = np.arange(n, dtype=np.uint64)
+        for v in range(1, n):
+            if rng.random() < 0.85:
+                par[v] = rng.integers(0, v)
+        perm = rng.permutation(n)
+        lab = np.empty(n, np.uint64)
+        lab[perm] = np.arange(n, dtype=np.uint64)
+        p2 = np.empty(n, np.uint64)
+        p2[lab] = lab[par]
+        forests.append(p2)
+    for par in forests:
+        exp, _, _ = oracle_mod.euler_tour_transcribed(par)
+        tour = kb.compute_euler_tour(dev64(par))
+        np.testing.assert_array_equal(host_u64(tour), exp, err_msg=str(par[:16]))

@@ -153,3 +153,43 @@ def test_stats_restatement_equals_transcription(oracle_mod, lo, hi):
         figs, trees = oracle_mod.compute_stats_transcribed(root, rank, 4)
         assert all(t[2] == 0 for t in trees)
         assert figs["avg_rank"] > 1e15
+
+
+def _tour_forests():
+    """Forests of a few dozen vertices: several roots, isolated roots,
+    vertices of degree 3 and more, a star, a path, and random forests."""
+    rng = np.random.default_rng(0xE7)
+    out = [np.array([0], np.uint64),
+           np.array([0, 1, 2], np.uint64),                      # three isolated roots
+           np.array([0, 0, 0, 0, 0, 0], np.uint64),             # a star
+           np.array([1, 2, 3, 4, 4], np.uint64),                # a path ending in root 4
+           np.array([3, 3, 3, 3, 2, 2, 6, 6, 9, 9, 0, 6, 11], np.uint64)]  # two trees, an isolated root, deg >= 3
+    for n in (20, 37, 64):
+        par = np.arange(n, dtype=np.uint64)
+        for v in range(1, n):
+            if rng.random() < 0.85:
+                par[v] = rng.integers(0, v)
+        perm = rng.permutation(n)  # relabel: parents no longer below their children
+        relabel = np.empty(n, np.uint64)
+        relabel[perm] = np.arange(n, dtype=np.uint64)
+        p2 = np.empty(n, np.uint64)
+        p2[relabel] = relabel[par]
+        out.append(p2)
+    return out
+
+
+def test_euler_tour_restatement_equals_transcription(oracle_mod):
+    """The C restatement's reference-numbered tour equals the statement-by-
+    statement transcription of reverse_rooted_tree + make_graph +
+    compute_euler_tour_impl on forests with several roots, isolated roots
+    and high degrees."""
+    forests = _tour_forests()
+    for n in (200, 1000):
+        forests.append(oracle_mod.gen_forest(n, n, 0, 7))
+        forests.append(oracle_mod.gen_forest(n, n + 1, 1, 3, n // 10))
+    for par in forests:
+        ts, tw, _, _, up = oracle_mod.euler_tour(par)
+        t2, w2, up2 = oracle_mod.euler_tour_transcribed(par)
+        np.testing.assert_array_equal(ts, t2, err_msg=str(par[:20]))
+        np.testing.assert_array_equal(tw, w2)
+        np.testing.assert_array_equal(up, up2)
