@@ -103,7 +103,8 @@ __global__ void __launch_bounds__(256) k_link_children(const uint64_t* __restric
   const uint32_t lane = threadIdx.x & 31u;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
-    const uint64_t v = base + threadIdx.x;  // base and blockDim are multiples of 32
+    const uint64_t v = base + threadIdx.x;  // base and blockDim are multiples of 32: lane 0 of a warp
+                                            // handles a multiple of 32
     const bool valid = v < n;
     uint64_t p = valid ? __ldcs(reinterpret_cast<const unsigned long long*>(parent) + v) : v;
     if (valid && p >= n) {
@@ -123,7 +124,8 @@ __global__ void __launch_bounds__(256) k_link_children(const uint64_t* __restric
     old = __shfl_sync(0xffffffffu, old, leader);
     if (valid) {
       const uint32_t after = peers & ~((2u << lane) - 1u);  // higher lanes of my group
-      const uint32_t next = after ? (uint32_t)(base + (uint32_t)(__ffs(after) - 1)) : old;
+      const uint64_t warp_v0 = v - lane;                   // the vertex of this warp's lane 0
+      const uint32_t next = after ? (uint32_t)(warp_v0 + (uint32_t)(__ffs(after) - 1)) : old;
       __stcs(nsib + v, link ? next : NO_CHILD);
     }
   }
