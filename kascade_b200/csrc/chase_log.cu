@@ -190,6 +190,8 @@ __global__ void __launch_bounds__(512) k_chase_log(const Rec* __restrict__ rec, 
       const uint64_t d = acc[c];
       if (act & (1u << c)) {
         if (tag_ruler(rr[c].c)) {
+          // back at its own ruler: a rootless cycle holding one ruler
+          if (tag_id(rr[c].c) == cid[c]) set_error(st, KASCADE_ERR_CYCLE, cid[c]);
           Rec o;
           o.a = acc[c];
           o.b = tag_id(rr[c].c);

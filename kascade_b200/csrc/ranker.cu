@@ -408,6 +408,9 @@ __global__ void __launch_bounds__(512) k_chase(Rec* __restrict__ rec, uint32_t n
           act &= ~(1u << c);
         }
       } else if (tag_ruler(tg)) {
+        // back at its own ruler: a cycle without a root that holds one ruler
+        // (a valid chain only ends at another ruler)
+        if (tag_id(tg) == cid[c]) set_error(st, KASCADE_ERR_CYCLE, cid[c]);
         Rec o;
         o.a = acc[c];
         o.b = tag_id(tg);

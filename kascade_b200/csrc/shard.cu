@@ -138,6 +138,7 @@ __global__ void __launch_bounds__(256) k_shard_chase(Rec* __restrict__ rec, Shar
       const uint64_t x = cur - v.lo;
       const Rec r = ld_rec_cg(rec + x);
       if (tag_ruler(r.c)) {  // the chain ends at the next ruler
+        if (v.gid(tag_id(r.c)) == ruler) set_error(st, KASCADE_ERR_CYCLE, cur);  // back at its own: rootless
         const uint32_t e = atomicAdd(end_count, 1u);
         if (e < end_cap) ends[e] = kascade_shard_end{ruler, v.gid(tag_id(r.c)), dist};
         else set_error(st, KASCADE_ERR_TOO_LARGE, e);
