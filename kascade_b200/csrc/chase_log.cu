@@ -392,7 +392,7 @@ __global__ void __launch_bounds__(FIN_THREADS, 2) k_place(const LogEnt* __restri
                                                             uint32_t* __restrict__ ucount, uint32_t ucap,
                                                             const uint64_t* __restrict__ seg_off,
                                                             const uint32_t* __restrict__ hint, uint32_t nseg,
-                                                            DevStatus* st) {
+                                                            const uint32_t* __restrict__ plus_one, DevStatus* st) {
   const SinkBatch inst{nullptr, nullptr, 0, seg_off, hint, nseg};  // instance offsets of a batch
   extern __shared__ __align__(16) unsigned char smraw[];
   unsigned long long* rank_s = reinterpret_cast<unsigned long long*>(smraw);  // SUB entries
@@ -441,7 +441,8 @@ __global__ void __launch_bounds__(FIN_THREADS, 2) k_place(const LogEnt* __restri
         const unsigned long long ibase = (seg_off && !un) ? inst.base_of(lo + i) : 0ull;
         __stcs(reinterpret_cast<unsigned long long*>(root_out) + lo + i,
                un ? NOT_REACHED : (unsigned long long)r - ibase);
-        __stcs(reinterpret_cast<unsigned long long*>(rank_out) + lo + i, un ? 0ull : rank_s[i]);
+        const unsigned long long add = plus_one ? (__ldg(plus_one + ((lo + i) >> 5)) >> ((lo + i) & 31)) & 1u : 0u;
+        __stcs(reinterpret_cast<unsigned long long*>(rank_out) + lo + i, un ? 0ull : rank_s[i] + add);
       }
       const uint32_t m = __ballot_sync(FULL, un);
       if (m == 0u) continue;
@@ -676,7 +677,7 @@ kascade_status rank_level0_log(kascade_ctx& ctx, const Rec* rec, uint32_t n, uin
     const size_t smem = SUB * (sizeof(unsigned long long) + sizeof(uint32_t));
     k_place<<<(unsigned)std::max<uint64_t>(1, std::min<uint64_t>(items, (uint64_t)ctx.usable_sms() * 2)),
                 FIN_THREADS, smem, s>>>(part2, cursor2, nb, limit, n, beyond, t.heads_are_rulers, t.root, t.rank,
-                                        ulist, ucount, ucap, t.seg_off, t.hint, t.nseg, ctx.d_status);
+                                        ulist, ucount, ucap, t.seg_off, t.hint, t.nseg, t.plus_one, ctx.d_status);
     KS_CHECK_LAUNCH();
   }
   if (!t.heads_are_rulers) {

@@ -4,28 +4,27 @@
 // (lib/kascade/eulertour.cpp:33-127, 235-278, 337-392) with the forest built
 // by reverse_rooted_tree + make_graph (lib/kascade/successor_utils.cpp:236-300).
 //
-// Layout used for ranking a single forest (m = 2n elements): slot v (v < n)
-// is the up edge v -> parent(v), and for a root r the tour's terminal
-// element (weight 0, the reference's dummy root element); slot n + v is the
-// down edge parent(v) -> v, a root's an unused self loop.  The depth of v is
-// the rank of slot v (up edges weigh +1, down edges -1), so the final
-// map-back is a coalesced pass over slots 0..n-1; the tour of a tree starts
-// at the down edge into the root's first child and ends in the root's
-// terminal slot.
+// Ranking needs each vertex's children grouped, in any order (depth and root
+// are unique whatever the rotation), so no sort: one pass links every vertex
+// into its parent's child list with one atomic exchange on the list head.
+// The tour's rotation is the list order, which depends on the order of the
+// exchanges; results do not.
 //
-// A single forest needs no sort: ranking only needs each vertex's children
-// grouped, in any order (depth and root are unique whatever the rotation).
-// One pass links every vertex into its parent's child list (one atomic
-// exchange per warp group of siblings on the parent's list head); a second,
-// purely streaming pass writes both tour records of every vertex at slots
-// indexed by the vertex itself:
-//   slot v      : up edge v -> p, successor the down edge into v's next
-//                 sibling, else p's up slot
-//   slot n + v  : down edge p -> v, successor the down edge into v's first
-//                 child, else v's own up slot
-// The tour's rotation is then the list order, which depends on the order of
-// the atomic exchanges; results do not.  A batch of forests and
-// compute_euler_tour (the reference's numbering) sort the children instead.
+// Layout for ranking a single forest (m = n + d elements): slot v (v < n) is
+// the up edge v -> parent(v), and for a root r the tour's terminal element
+// (weight 0, the reference's dummy root element).  The d non-root vertices
+// with children also have a down edge parent(v) -> v, at slot n + (v's number
+// among them).  A leaf's down edge would be followed at once by its own up
+// edge (weights -1 and +1): the two are one element of weight 0 at slot v, so
+// the tour is ~1.5n long instead of 2n, and a leaf's depth is its element's
+// rank + 1.  Otherwise the depth of v is the rank of slot v, so the map-back
+// is a coalesced pass over slots 0..n-1; the tour of a tree starts at the
+// element entering the root's first child and ends in the root's terminal
+// slot.  A batch of forests keeps both edges of every vertex (slots by
+// vertex, no compaction); compute_euler_tour (the reference's numbering)
+// sorts the children.
+#include <algorithm>
+
 #include "ranker.cuh"
 #include "sort.cuh"
 
@@ -53,22 +52,12 @@ __global__ void __launch_bounds__(256) k_seg_bounds(const uint32_t* __restrict__
 
 constexpr uint32_t NO_CHILD = 0xFFFFFFFFu;
 
-// Where a forest's tour records live, by vertex.  A single forest of n
-// vertices: up edge of v at slot v, down edge into v at slot n + v.  A batch
-// of forests, compacted into one vertex space with per-forest bases fd[j]:
+// Where a batch's forest tour records live, by vertex.  The forests are
+// compacted into one vertex space with per-forest bases fd[j]:
 // the up edge of compact vertex c of forest j at that vertex's position in
 // the caller's concatenated arrays (foff[j] + c - fd[j]), the down edge into
 // c after all input elements (down_base + c).  Ruler sampling thresholds can
 // differ per forest (size classes).
-struct SlotsSingle {
-  uint32_t n;
-  uint32_t th;
-  __device__ __forceinline__ uint32_t seg_of(uint32_t) const { return 0; }
-  __device__ __forceinline__ uint32_t up(uint32_t v, uint32_t) const { return v; }
-  __device__ __forceinline__ uint32_t down(uint32_t v) const { return n + v; }
-  __device__ __forceinline__ uint32_t thresh(uint32_t) const { return th; }
-};
-
 struct SlotsBatch {
   const uint32_t* fd;       // nf + 1 compact starts
   const uint32_t* foff;     // nf concatenated offsets
@@ -91,20 +80,24 @@ struct SlotsBatch {
   __device__ __forceinline__ uint32_t thresh(uint32_t j) const { return __ldg(fthresh + j); }
 };
 
-// Child lists of a single forest: fc[p] = one child of p (NO_CHILD: a leaf),
-// nsib[v] = v's next sibling (NO_CHILD: the last one).  A warp's vertices that
-// share a parent link to each other in lane order and the group's first lane
-// exchanges the list head once.  root_bits gets one bit per vertex (warp
-// ballots over 32 consecutive vertices: no atomics, no clearing).  An
-// out-of-range parent is reported and the vertex treated as a root.
+// Child lists of a forest: fc[p] = one child of p (NO_CHILD: a leaf),
+// nsib[v] = v's next sibling (NO_CHILD: the last one), one atomic exchange on
+// the parent's list head per vertex.  GROUP: a warp's vertices that share a
+// parent first link to each other in lane order and the group's first lane
+// exchanges the head once (a star then costs n/32 exchanges on one word
+// instead of n).  Also writes the root bits (warp ballots over 32 consecutive
+// vertices) and a packed 32-bit copy of the parents; an out-of-range parent
+// is reported and the vertex treated as a root.
+template <bool GROUP>
 __global__ void __launch_bounds__(256) k_link_children(const uint64_t* __restrict__ parent, uint32_t n,
-                                                       uint32_t* __restrict__ fc, uint32_t* __restrict__ nsib,
-                                                       uint32_t* __restrict__ root_bits, DevStatus* st) {
+                                                       uint32_t* __restrict__ p32, uint32_t* __restrict__ fc,
+                                                       uint32_t* __restrict__ nsib, uint32_t* __restrict__ root_bits,
+                                                       DevStatus* st) {
   const uint32_t lane = threadIdx.x & 31u;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
-    const uint64_t v = base + threadIdx.x;  // base and blockDim are multiples of 32: lane 0 of a warp
-                                            // handles a multiple of 32
+    // base and blockDim are multiples of 32: lane 0 of a warp handles a multiple of 32
+    const uint64_t v = base + threadIdx.x;
     const bool valid = v < n;
     uint64_t p = valid ? __ldcs(reinterpret_cast<const unsigned long long*>(parent) + v) : v;
     if (valid && p >= n) {
@@ -113,31 +106,36 @@ __global__ void __launch_bounds__(256) k_link_children(const uint64_t* __restric
     }
     const bool root = valid && p == v;
     const uint32_t rb = __ballot_sync(0xffffffffu, root);
-    if (lane == 0 && (v >> 5) <= ((uint64_t)n - 1) >> 5) root_bits[v >> 5] = rb;
+    if (lane == 0 && valid) root_bits[v >> 5] = rb;
     const bool link = valid && !root;
-    // lanes that do not link get distinct keys
-    const unsigned long long key = link ? p : (0xFFFFFFFF00000000ull | lane);
-    const uint32_t peers = __match_any_sync(0xffffffffu, key);
-    const int leader = __ffs(peers) - 1;
-    uint32_t old = NO_CHILD;
-    if (link && (int)lane == leader) old = atomicExch(fc + p, (uint32_t)v);
-    old = __shfl_sync(0xffffffffu, old, leader);
-    if (valid) {
+    uint32_t next = NO_CHILD;
+    if (GROUP) {
+      // parents are below 2^31: lanes that do not link get distinct keys above
+      const uint32_t key = link ? (uint32_t)p : (0x80000000u | lane);
+      const uint32_t peers = __match_any_sync(0xffffffffu, key);
+      const int leader = __ffs(peers) - 1;
+      uint32_t old = NO_CHILD;
+      if (link && (int)lane == leader) old = atomicExch(fc + p, (uint32_t)v);
+      old = __shfl_sync(0xffffffffu, old, leader);
       const uint32_t after = peers & ~((2u << lane) - 1u);  // higher lanes of my group
-      const uint64_t warp_v0 = v - lane;                   // the vertex of this warp's lane 0
-      const uint32_t next = after ? (uint32_t)(warp_v0 + (uint32_t)(__ffs(after) - 1)) : old;
+      next = after ? (uint32_t)(v - lane + (uint32_t)(__ffs(after) - 1)) : old;
+    } else if (link) {
+      next = atomicExch(fc + p, (uint32_t)v);
+    }
+    if (valid) {
+      __stcg(p32 + v, (uint32_t)p);
       __stcs(nsib + v, link ? next : NO_CHILD);
     }
   }
 }
 
-// Both tour records of every vertex, at slots v and n + v, from the child
+// Both tour records of every vertex, at the slots `slots` gives, from the child
 // lists; rulers sampled among the slots and numbered (one atomic per tile).
 // The down edge into a root's first child is the head of that tree's tour
 // and always a ruler, so no tour element is left unreached; roots' slots are
 // self loops (the terminal, and an unused down slot) and rulers.
 template <class Slots>
-__global__ void __launch_bounds__(256) k_tour_links(const uint64_t* __restrict__ parent, uint32_t n,
+__global__ void __launch_bounds__(256) k_tour_links(const uint32_t* __restrict__ p32, uint32_t n,
                                                     const uint32_t* __restrict__ fc,
                                                     const uint32_t* __restrict__ nsib,
                                                     const uint32_t* __restrict__ root_bits, Rec* __restrict__ rec,
@@ -155,8 +153,8 @@ __global__ void __launch_bounds__(256) k_tour_links(const uint64_t* __restrict__
       const uint64_t v = tile + (uint64_t)i * blockDim.x + threadIdx.x;
       su[i] = sd[i] = 0;
       if (v >= n) continue;
-      uint64_t p = __ldcs(reinterpret_cast<const unsigned long long*>(parent) + v);
-      if (p >= n) p = v;  // reported by k_link_children
+      uint64_t p = __ldcs(p32 + v);  // in range: k_link_children made bad parents roots
+      if (p >= n) p = v;
       const uint32_t sib = __ldcs(nsib + v), first = __ldcs(fc + v);
       const uint32_t j = slots.seg_of((uint32_t)v);  // v and p belong to the same forest
       const uint32_t th = slots.thresh(j);
@@ -304,25 +302,178 @@ kascade_status sort_children(kascade_ctx& ctx, const uint64_t* parent, uint32_t 
   return KASCADE_OK;
 }
 
-// Child lists of the forest (parent[v], n vertices, one vertex space) and
-// both tour records of every vertex at the slots `slots` gives; ruler ids
-// continue `counter`.
+// Leaf contraction of a single forest's tour.  A leaf's down edge is
+// followed by its own up edge (weights -1 and +1), so the two become one
+// element of weight 0 at the leaf's slot v: every other rank is unchanged
+// and the leaf's depth is that element's rank + 1 (leaf_bits tells the
+// output step).  Only non-root vertices with children keep a down edge, at
+// the compacted slot n + (their number among those vertices): ibits marks
+// them (one word per 32 vertices) and ipre counts them before each word, so
+// the element a parent or a sibling continues into is found with two reads of
+// these L2-resident tables.
+__global__ void __launch_bounds__(256) k_internal_words(const uint32_t* __restrict__ p32,
+                                                        const uint32_t* __restrict__ fc, uint32_t n,
+                                                        uint32_t* __restrict__ ibits, uint32_t* __restrict__ icount) {
+  const uint32_t lane = threadIdx.x & 31u;
+  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < n; base += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t v = base + threadIdx.x;
+    const bool internal = v < n && __ldcs(p32 + v) != (uint32_t)v && __ldcs(fc + v) != NO_CHILD;
+    const uint32_t bits = __ballot_sync(0xffffffffu, internal);
+    if (lane == 0 && v < n) {
+      ibits[v >> 5] = bits;
+      icount[v >> 5] = (uint32_t)__popc(bits);
+    }
+  }
+}
+
+// (bits, down edges before the word) of every word of 32 vertices
+__global__ void __launch_bounds__(256) k_internal_pack(const uint32_t* __restrict__ ibits,
+                                                       const uint32_t* __restrict__ ipre, uint32_t words,
+                                                       uint2* __restrict__ iw) {
+  for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < words; w += gridDim.x * blockDim.x)
+    iw[w] = make_uint2(ibits[w], ipre[w]);
+}
+
+struct Entries {
+  const uint2* iw;  // per word of 32 vertices: (down-edge bits, down edges before it)
+  uint32_t n;
+  // the element a walk enters vertex c by: its down edge, or its merged slot
+  // (one 8 B read of an L2-resident table)
+  __device__ __forceinline__ uint32_t of(uint32_t c) const {
+    const uint2 w = __ldg(iw + (c >> 5));
+    const uint32_t below = w.x & ((1u << (c & 31)) - 1u);
+    return ((w.x >> (c & 31)) & 1u) ? n + w.y + (uint32_t)__popc(below) : c;
+  }
+  __device__ __forceinline__ uint32_t down_slot(uint32_t v) const {  // v has a down edge
+    const uint2 w = __ldg(iw + (v >> 5));
+    return n + w.y + (uint32_t)__popc(w.x & ((1u << (v & 31)) - 1u));
+  }
+};
+
+__global__ void __launch_bounds__(256) k_tour_leaves(const uint32_t* __restrict__ p32, uint32_t n,
+                                                     const uint32_t* __restrict__ fc,
+                                                     const uint32_t* __restrict__ nsib,
+                                                     const uint32_t* __restrict__ root_bits, Entries ent,
+                                                     Rec* __restrict__ rec, uint32_t* __restrict__ ruler_elem,
+                                                     uint32_t* __restrict__ counter, uint32_t salt, uint32_t th,
+                                                     uint32_t* __restrict__ leaf_bits, DevStatus* st) {
+  __shared__ uint32_t sm[33];
+  __shared__ uint32_t sbase;
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint64_t tile_sz = (uint64_t)blockDim.x * TB_ITEMS;
+  for (uint64_t tile = (uint64_t)blockIdx.x * tile_sz; tile < n; tile += (uint64_t)gridDim.x * tile_sz) {
+    Rec ru[TB_ITEMS], rd[TB_ITEMS];
+    uint32_t sd[TB_ITEMS];
+    uint32_t rl = 0, cnt = 0, has_down = 0;
+#pragma unroll
+    for (int i = 0; i < TB_ITEMS; ++i) {
+      const uint64_t v = tile + (uint64_t)i * blockDim.x + threadIdx.x;
+      sd[i] = 0;
+      bool leaf = false;
+      if (v < n) {
+        uint64_t p = __ldcs(p32 + v);
+        if (p >= n) p = v;
+        if (p == v) {  // a root: the tour's terminal element (or an isolated vertex)
+          ru[i].a = 0;
+          ru[i].b = (uint32_t)v;
+          rl |= 1u << (2 * i);
+          cnt++;
+        } else {
+          const uint32_t sib = __ldcs(nsib + v), first = __ldcs(fc + v);
+          const uint32_t up_next = (sib != NO_CHILD) ? ent.of(sib) : (uint32_t)p;
+          bool head = false;
+          if ((__ldg(root_bits + (p >> 5)) >> (p & 31)) & 1u) head = __ldg(fc + p) == (uint32_t)v;
+          if (first != NO_CHILD) {
+            sd[i] = ent.down_slot((uint32_t)v);
+            ru[i].a = 1ull;
+            ru[i].b = up_next;
+            rd[i].a = ~0ull;  // -1
+            rd[i].b = ent.of(first);
+            has_down |= 1u << i;
+            if (sampled((uint32_t)v, salt, th)) {
+              rl |= 1u << (2 * i);
+              cnt++;
+            }
+            if (head || sampled(sd[i], salt, th)) {
+              rl |= 2u << (2 * i);
+              cnt++;
+            }
+          } else {
+            leaf = true;
+            ru[i].a = 0;  // down (-1) and up (+1) in one element
+            ru[i].b = up_next;
+            if (head || sampled((uint32_t)v, salt, th)) {
+              rl |= 1u << (2 * i);
+              cnt++;
+            }
+          }
+        }
+      }
+      // a warp's 32 consecutive vertices make one word of leaf bits
+      const uint32_t lb = __ballot_sync(0xffffffffu, leaf);
+      if (lane == 0 && v < n) leaf_bits[v >> 5] = lb;
+    }
+    uint32_t total;
+    uint32_t pre = block_exclusive_scan(cnt, sm, &total);
+    if (threadIdx.x == 0) {
+      uint32_t b = total ? atomicAdd(counter, total) : 0u;
+      if ((uint64_t)b + total > MAX_RULERS) set_error(st, KASCADE_ERR_TOO_LARGE, b);
+      sbase = b;
+    }
+    __syncthreads();
+    uint32_t id = sbase + pre;
+#pragma unroll
+    for (int i = 0; i < TB_ITEMS; ++i) {
+      const uint64_t v = tile + (uint64_t)i * blockDim.x + threadIdx.x;
+      if (v >= n) continue;
+      ru[i].c = TAG_UNREACHED;
+      rd[i].c = TAG_UNREACHED;
+      if ((rl >> (2 * i)) & 1u) {
+        if (id < MAX_RULERS) {
+          ru[i].c = TAG_RULER | id;
+          ruler_elem[id] = (uint32_t)v;
+        }
+        id++;
+      }
+      if ((rl >> (2 * i)) & 2u) {
+        if (id < MAX_RULERS) {
+          rd[i].c = TAG_RULER | id;
+          ruler_elem[id] = sd[i];
+        }
+        id++;
+      }
+      st_rec_cs(rec + v, ru[i]);
+      if ((has_down >> i) & 1u) st_rec_cs(rec + sd[i], rd[i]);
+    }
+    __syncthreads();
+  }
+}
+
+// Child lists of the forest (parent[v], n vertices, one vertex space), the
+// packed parents and the root bits.
+kascade_status link_children(kascade_ctx& ctx, const uint64_t* parent, uint32_t n, uint32_t* fc, uint32_t* nsib,
+                             uint32_t* p32, uint32_t* root_bits, cudaStream_t s) {
+  ProfScope ps(ctx, "link_children", s);
+  KS_CUDA(cudaMemsetAsync(fc, 0xFF, sizeof(uint32_t) * (size_t)n, s));
+  k_link_children<true><<<grid_for(ctx, n, 256, 8), 256, 0, s>>>(parent, n, p32, fc, nsib, root_bits, ctx.d_status);
+  KS_CHECK_LAUNCH();
+  return KASCADE_OK;
+}
+
+// Child lists and both tour records of every vertex at the slots `slots`
+// gives (a batch's forests); ruler ids continue `counter`.
 template <class Slots>
 kascade_status build_tour(kascade_ctx& ctx, const uint64_t* parent, uint32_t n, const Slots& slots, Rec* rec,
                           uint32_t* ruler_elem, uint32_t* counter, uint32_t salt, cudaStream_t s) {
   uint32_t* fc = alloc<uint32_t>(ctx, n);
   uint32_t* nsib = alloc<uint32_t>(ctx, n);
+  uint32_t* p32 = alloc<uint32_t>(ctx, n);
   uint32_t* root_bits = alloc<uint32_t>(ctx, ((uint64_t)n + 31) / 32);
-  if (!fc || !nsib || !root_bits) return KASCADE_ERR_OOM;
-  {
-    ProfScope ps(ctx, "link_children", s);
-    KS_CUDA(cudaMemsetAsync(fc, 0xFF, sizeof(uint32_t) * (size_t)n, s));
-    k_link_children<<<grid_for(ctx, n, 256, 8), 256, 0, s>>>(parent, n, fc, nsib, root_bits, ctx.d_status);
-    KS_CHECK_LAUNCH();
-  }
+  if (!fc || !nsib || !p32 || !root_bits) return KASCADE_ERR_OOM;
+  KS_TRY(link_children(ctx, parent, n, fc, nsib, p32, root_bits, s));
   ProfScope ps(ctx, "tour_build", s);
   const unsigned grid = grid_for(ctx, ((uint64_t)n + 256 * TB_ITEMS - 1) / (256 * TB_ITEMS) * 256, 256, 8);
-  k_tour_links<Slots><<<grid, 256, 0, s>>>(parent, n, fc, nsib, root_bits, rec, ruler_elem, counter, salt, slots,
+  k_tour_links<Slots><<<grid, 256, 0, s>>>(p32, n, fc, nsib, root_bits, rec, ruler_elem, counter, salt, slots,
                                            ctx.d_status);
   KS_CHECK_LAUNCH();
   return KASCADE_OK;
@@ -334,15 +485,46 @@ kascade_status root_forest_impl(kascade_ctx& ctx, const uint64_t* parent, uint32
                                 uint64_t* depth_out, int keep_roots, const Params& p, cudaStream_t s,
                                 bool device_levels) {
   if (n == 0) return KASCADE_OK;
-  const uint32_t m = 2 * n;
-  Rec* rec = alloc<Rec>(ctx, m);
-  uint32_t* ruler_elem = alloc<uint32_t>(ctx, m);
-  uint32_t* ctr = alloc<uint32_t>(ctx, 1);
-  if (!rec || !ruler_elem || !ctr) return KASCADE_ERR_OOM;
-  KS_CUDA(cudaMemsetAsync(ctr, 0, sizeof(uint32_t), s));
-  const SlotsSingle slots{n, (uint32_t)(4294967296.0 / (double)(p.spacing0 < 2 ? 2 : p.spacing0))};
-  KS_TRY(build_tour(ctx, parent, n, slots, rec, ruler_elem, ctr, mix32(p.seed ^ 0x70757254u), s));
-  SinkTour sink{root_out, depth_out, n, keep_roots};
+  const uint32_t words = (uint32_t)(((uint64_t)n + 31) / 32);
+  Rec* rec = alloc<Rec>(ctx, 2ull * n);
+  uint32_t* ruler_elem = alloc<uint32_t>(ctx, 2ull * n);
+  uint32_t* ctr = alloc<uint32_t>(ctx, 2);  // ruler count, down-edge count
+  uint32_t* fc = alloc<uint32_t>(ctx, n);
+  uint32_t* nsib = alloc<uint32_t>(ctx, n);
+  uint32_t* p32 = alloc<uint32_t>(ctx, n);
+  uint32_t* root_bits = alloc<uint32_t>(ctx, words);
+  uint32_t* ibits = alloc<uint32_t>(ctx, words);
+  uint32_t* icount = alloc<uint32_t>(ctx, words);
+  uint32_t* ipre = alloc<uint32_t>(ctx, words);
+  uint32_t* leaf_bits = alloc<uint32_t>(ctx, words);
+  uint2* iw = alloc<uint2>(ctx, words);
+  if (!rec || !ruler_elem || !ctr || !fc || !nsib || !p32 || !root_bits || !ibits || !icount || !ipre || !leaf_bits ||
+      !iw)
+    return KASCADE_ERR_OOM;
+  KS_CUDA(cudaMemsetAsync(ctr, 0, 2 * sizeof(uint32_t), s));
+  KS_TRY(link_children(ctx, parent, n, fc, nsib, p32, root_bits, s));
+  uint32_t downs = 0;
+  {
+    ProfScope ps(ctx, "tour_build", s);
+    k_internal_words<<<grid_for(ctx, n, 256, 8), 256, 0, s>>>(p32, fc, n, ibits, icount);
+    KS_CHECK_LAUNCH();
+    KS_TRY(exclusive_scan_u32(ctx, icount, ipre, words, ctr + 1, s));
+    k_internal_pack<<<grid_for(ctx, words, 256, 8), 256, 0, s>>>(ibits, ipre, words, iw);
+    KS_CHECK_LAUNCH();
+  }
+  // the tour's length: one element per vertex, and a down edge per non-root
+  // vertex with children (one host read)
+  KS_TRY(read_u32(ctx, ctr + 1, &downs, s));
+  const uint32_t m = n + downs;
+  {
+    ProfScope ps(ctx, "tour_build", s);
+    const unsigned grid = grid_for(ctx, ((uint64_t)n + 256 * TB_ITEMS - 1) / (256 * TB_ITEMS) * 256, 256, 8);
+    const uint32_t th = (uint32_t)(4294967296.0 / (double)(p.spacing0 < 2 ? 2 : p.spacing0));
+    k_tour_leaves<<<grid, 256, 0, s>>>(p32, n, fc, nsib, root_bits, Entries{iw, n}, rec, ruler_elem, ctr,
+                                       mix32(p.seed ^ 0x70757254u), th, leaf_bits, ctx.d_status);
+    KS_CHECK_LAUNCH();
+  }
+  SinkTour sink{root_out, depth_out, n, keep_roots, leaf_bits};
   if (device_levels && m > p.base_max && p.max_levels > 0) {
     if (m < p.level0_log_min)
       return rank_records_dev(ctx, rec, m, ctr, dev_cap_next(m, p.spacing0), ruler_elem, sink, p, s);

@@ -54,6 +54,9 @@ struct LogTarget {
   const uint64_t* seg_off = nullptr;
   const uint32_t* hint = nullptr;
   uint32_t nseg = 0;
+  // bit x set: element x's rank output is one more than its rank in the list
+  // (a tree rooting's leaves, whose down and up edge share one element)
+  const uint32_t* plus_one = nullptr;
 };
 
 // Plain arrays. keep_roots: leave root entries untouched (the reference's
@@ -81,15 +84,22 @@ struct SinkPlain {
 
 // Euler tour: elements 0..nv-1 are the vertices' up edges (roots: the tour's
 // terminal element), so only those produce output.
+// leaf_bits (optional): bit v set for a leaf whose down and up edge are one
+// element of weight 0, whose rank is then one less than the leaf's depth.
 struct SinkTour {
   static constexpr bool kWriteFree = true;
   uint64_t* root;
   uint64_t* depth;
   uint32_t nv;
   int keep_roots;
+  const uint32_t* leaf_bits = nullptr;
   uint32_t limit(uint32_t n) const { return n < nv ? n : nv; }
   // the tour build makes every tour head a ruler
-  LogTarget log_target(uint32_t n) const { return LogTarget{root, depth, limit(n), keep_roots, 1}; }
+  LogTarget log_target(uint32_t n) const {
+    LogTarget t{root, depth, limit(n), keep_roots, 1};
+    t.plus_one = leaf_bits;
+    return t;
+  }
   __device__ __forceinline__ void put(uint32_t x, uint64_t rk, uint32_t rt, bool is_root) const {
     if (x >= nv) return;
     if (is_root) {
@@ -99,6 +109,7 @@ struct SinkTour {
       }
       return;
     }
+    if (leaf_bits) rk += (__ldg(leaf_bits + (x >> 5)) >> (x & 31)) & 1u;
     __stcs(root + x, (unsigned long long)rt);
     __stcs(depth + x, (unsigned long long)rk);
   }
