@@ -366,7 +366,7 @@ typedef struct kascade_server_config {
   uint64_t hbm_budget_bytes;     /* admission budget (default 40 GiB)             */
   uint32_t max_batch_requests;   /* requests per batch (default 4096)             */
   uint32_t reserved;
-  uint64_t max_batch_elements;   /* elements per batch, large lane (default 2^26) */
+  uint64_t max_batch_elements;   /* elements per batch, large lane (default 2^27) */
   uint64_t small_max;            /* latency lane: requests up to this many
                                     elements (default 2^20)                       */
   uint64_t small_batch_elements; /* elements per batch, latency lane (2^23)       */

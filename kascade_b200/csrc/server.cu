@@ -629,7 +629,7 @@ KASCADE_API void kascade_server_config_init(kascade_server_config* c) {
   c->device = 0;
   c->hbm_budget_bytes = 40ull << 30;
   c->max_batch_requests = 4096;
-  c->max_batch_elements = 1ull << 26;
+  c->max_batch_elements = 1ull << 27;
   c->small_max = 1ull << 20;
   c->small_batch_elements = 1ull << 23;
   c->latency_sms = 80;
@@ -645,7 +645,7 @@ KASCADE_API kascade_status kascade_server_create(const kascade_server_config* cf
   kascade_server_config_init(&s->cfg);
   if (cfg) s->cfg = *cfg;
   if (s->cfg.max_batch_requests == 0) s->cfg.max_batch_requests = 4096;
-  if (s->cfg.max_batch_elements == 0) s->cfg.max_batch_elements = 1ull << 26;
+  if (s->cfg.max_batch_elements == 0) s->cfg.max_batch_elements = 1ull << 27;
   if (s->cfg.hbm_budget_bytes == 0) s->cfg.hbm_budget_bytes = 40ull << 30;
   if (s->cfg.small_batch_elements == 0) s->cfg.small_batch_elements = 1ull << 23;
   if (cudaSetDevice(s->cfg.device) != cudaSuccess ||
