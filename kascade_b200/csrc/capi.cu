@@ -229,9 +229,10 @@ KASCADE_API uint64_t kascade_scratch_bytes_rank_list(uint64_t n) {
 }
 
 KASCADE_API uint64_t kascade_scratch_bytes_root_forest(uint64_t n) {
-  // sort buffers (16n) + histogram + segments (8n) + tour records (32n)
-  // + ruler list (8n) + write-free path on 2n tour slots: log (32n),
-  // partitioned results (16n) + deeper levels
+  // tour records on 2n slots (32n) + ruler list (8n) + child lists, packed
+  // parents and bit tables (~13n) + write-free level 0 over the <= 2n tour
+  // elements: log (32n), first-pass windows (16n) + deeper levels, with
+  // headroom
   return 16 * n + 8 * n + 32 * n + 8 * n + 32 * n + 16 * n + (80 * n) / 16 + (192ull << 20);
 }
 

@@ -33,6 +33,7 @@ namespace ks {
 namespace {
 
 constexpr int TB_ITEMS = 4;
+constexpr int LINK_ITEMS = 4;  // vertices per thread in one linking round
 
 inline int bits_for(uint64_t n) {
   int b = 1;
@@ -80,6 +81,15 @@ struct SlotsBatch {
   __device__ __forceinline__ uint32_t thresh(uint32_t j) const { return __ldg(fthresh + j); }
 };
 
+// Exchange on a child-list head with an L2 evict-last hint: the head array is
+// the one array linking reads at random, so its lines keep L2 ahead of the
+// streamed parents and sibling links (2.47 -> 2.38 ms at 2^26 vertices).
+__device__ __forceinline__ uint32_t exch_head(uint32_t* p, uint32_t v, uint64_t pol) {
+  uint32_t old;
+  asm volatile("atom.global.exch.L2::cache_hint.b32 %0, [%1], %2, %3;" : "=r"(old) : "l"(p), "r"(v), "l"(pol) : "memory");
+  return old;
+}
+
 // Child lists of a forest: fc[p] = one child of p (NO_CHILD: a leaf),
 // nsib[v] = v's next sibling (NO_CHILD: the last one), one atomic exchange on
 // the parent's list head per vertex.  GROUP: a warp's vertices that share a
@@ -94,37 +104,56 @@ __global__ void __launch_bounds__(256) k_link_children(const uint64_t* __restric
                                                        uint32_t* __restrict__ nsib, uint32_t* __restrict__ root_bits,
                                                        DevStatus* st) {
   const uint32_t lane = threadIdx.x & 31u;
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
-    // base and blockDim are multiples of 32: lane 0 of a warp handles a multiple of 32
-    const uint64_t v = base + threadIdx.x;
-    const bool valid = v < n;
-    uint64_t p = valid ? __ldcs(reinterpret_cast<const unsigned long long*>(parent) + v) : v;
-    if (valid && p >= n) {
-      set_error(st, KASCADE_ERR_OUT_OF_RANGE, v);
-      p = v;
+  const uint64_t pol = l2_keep_policy();
+  const uint64_t tile_sz = (uint64_t)blockDim.x * LINK_ITEMS;
+  for (uint64_t tile = (uint64_t)blockIdx.x * tile_sz; tile < n; tile += (uint64_t)gridDim.x * tile_sz) {
+    // tile and blockDim are multiples of 32: lane 0 of a warp handles a multiple of 32
+    uint64_t p[LINK_ITEMS];
+#pragma unroll
+    for (int i = 0; i < LINK_ITEMS; ++i) {
+      const uint64_t v = tile + (uint64_t)i * blockDim.x + threadIdx.x;
+      p[i] = v < n ? __ldcs(reinterpret_cast<const unsigned long long*>(parent) + v) : v;
     }
-    const bool root = valid && p == v;
-    const uint32_t rb = __ballot_sync(0xffffffffu, root);
-    if (lane == 0 && valid) root_bits[v >> 5] = rb;
-    const bool link = valid && !root;
-    uint32_t next = NO_CHILD;
-    if (GROUP) {
-      // parents are below 2^31: lanes that do not link get distinct keys above
-      const uint32_t key = link ? (uint32_t)p : (0x80000000u | lane);
-      const uint32_t peers = __match_any_sync(0xffffffffu, key);
-      const int leader = __ffs(peers) - 1;
-      uint32_t old = NO_CHILD;
-      if (link && (int)lane == leader) old = atomicExch(fc + p, (uint32_t)v);
-      old = __shfl_sync(0xffffffffu, old, leader);
-      const uint32_t after = peers & ~((2u << lane) - 1u);  // higher lanes of my group
-      next = after ? (uint32_t)(v - lane + (uint32_t)(__ffs(after) - 1)) : old;
-    } else if (link) {
-      next = atomicExch(fc + p, (uint32_t)v);
+    // every item's exchange is issued before any result is used
+    uint32_t old[LINK_ITEMS], peers[LINK_ITEMS];
+#pragma unroll
+    for (int i = 0; i < LINK_ITEMS; ++i) {
+      const uint64_t v = tile + (uint64_t)i * blockDim.x + threadIdx.x;
+      const bool valid = v < n;
+      if (valid && p[i] >= n) {
+        set_error(st, KASCADE_ERR_OUT_OF_RANGE, v);
+        p[i] = v;
+      }
+      const bool root = valid && p[i] == v;
+      const uint32_t rb = __ballot_sync(0xffffffffu, root);
+      if (lane == 0 && valid) root_bits[v >> 5] = rb;
+      const bool link = valid && !root;
+      old[i] = NO_CHILD;
+      peers[i] = 1u << lane;
+      if (GROUP) {
+        // parents are below 2^31: lanes that do not link get distinct keys above
+        const uint32_t key = link ? (uint32_t)p[i] : (0x80000000u | lane);
+        peers[i] = __match_any_sync(0xffffffffu, key);
+        if (link && (int)lane == __ffs(peers[i]) - 1) old[i] = exch_head(fc + p[i], (uint32_t)v, pol);
+      } else if (link) {
+        old[i] = exch_head(fc + p[i], (uint32_t)v, pol);
+      }
     }
-    if (valid) {
-      __stcg(p32 + v, (uint32_t)p);
-      __stcs(nsib + v, link ? next : NO_CHILD);
+#pragma unroll
+    for (int i = 0; i < LINK_ITEMS; ++i) {
+      const uint64_t v = tile + (uint64_t)i * blockDim.x + threadIdx.x;
+      const bool valid = v < n;
+      const bool link = valid && p[i] != v;
+      uint32_t next = old[i];
+      if (GROUP) {
+        next = __shfl_sync(0xffffffffu, old[i], __ffs(peers[i]) - 1);
+        const uint32_t after = peers[i] & ~((2u << lane) - 1u);  // higher lanes of my group
+        if (after) next = (uint32_t)(v - lane + (uint32_t)(__ffs(after) - 1));
+      }
+      if (valid) {
+        __stcs(p32 + v, (uint32_t)p[i]);  // streamed past L2: the list heads keep it
+        __stcs(nsib + v, link ? next : NO_CHILD);
+      }
     }
   }
 }
@@ -309,19 +338,35 @@ kascade_status sort_children(kascade_ctx& ctx, const uint64_t* parent, uint32_t 
 // output step).  Only non-root vertices with children keep a down edge, at
 // the compacted slot n + (their number among those vertices): ibits marks
 // them (one word per 32 vertices) and ipre counts them before each word, so
-// the element a parent or a sibling continues into is found with two reads of
-// these L2-resident tables.
+// the element a parent or a sibling continues into is found with one read of
+// these L2-resident tables.  head_bits marks the first child of every root
+// (the vertex the tree's tour enters first), so the tour build reads its own
+// word instead of its parent's root bit and list head.
 __global__ void __launch_bounds__(256) k_internal_words(const uint32_t* __restrict__ p32,
                                                         const uint32_t* __restrict__ fc, uint32_t n,
-                                                        uint32_t* __restrict__ ibits, uint32_t* __restrict__ icount) {
+                                                        uint32_t* __restrict__ ibits, uint32_t* __restrict__ icount,
+                                                        uint32_t* __restrict__ head_bits) {
   const uint32_t lane = threadIdx.x & 31u;
-  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < n; base += (uint64_t)gridDim.x * blockDim.x) {
-    const uint64_t v = base + threadIdx.x;
-    const bool internal = v < n && __ldcs(p32 + v) != (uint32_t)v && __ldcs(fc + v) != NO_CHILD;
-    const uint32_t bits = __ballot_sync(0xffffffffu, internal);
-    if (lane == 0 && v < n) {
-      ibits[v >> 5] = bits;
-      icount[v >> 5] = (uint32_t)__popc(bits);
+  const uint64_t tile_sz = (uint64_t)blockDim.x * TB_ITEMS;
+  for (uint64_t tile = (uint64_t)blockIdx.x * tile_sz; tile < n; tile += (uint64_t)gridDim.x * tile_sz) {
+    // both words of every item are loaded before any is used: 2 x TB_ITEMS loads in flight
+    uint32_t pv[TB_ITEMS], fv[TB_ITEMS];
+#pragma unroll
+    for (int i = 0; i < TB_ITEMS; ++i) {
+      const uint64_t v = tile + (uint64_t)i * blockDim.x + threadIdx.x;
+      pv[i] = v < n ? __ldcs(p32 + v) : (uint32_t)v;
+      fv[i] = v < n ? __ldcs(fc + v) : NO_CHILD;
+    }
+#pragma unroll
+    for (int i = 0; i < TB_ITEMS; ++i) {
+      const uint64_t v = tile + (uint64_t)i * blockDim.x + threadIdx.x;
+      const uint32_t bits = __ballot_sync(0xffffffffu, v < n && pv[i] != (uint32_t)v && fv[i] != NO_CHILD);
+      // a root's list head enters its tree first: the head of that tree's tour
+      if (v < n && pv[i] == (uint32_t)v && fv[i] != NO_CHILD) atomicOr(head_bits + (fv[i] >> 5), 1u << (fv[i] & 31));
+      if (lane == 0 && v < n) {
+        ibits[v >> 5] = bits;
+        icount[v >> 5] = (uint32_t)__popc(bits);
+      }
     }
   }
 }
@@ -337,23 +382,26 @@ __global__ void __launch_bounds__(256) k_internal_pack(const uint32_t* __restric
 struct Entries {
   const uint2* iw;  // per word of 32 vertices: (down-edge bits, down edges before it)
   uint32_t n;
-  // the element a walk enters vertex c by: its down edge, or its merged slot
-  // (one 8 B read of an L2-resident table)
-  __device__ __forceinline__ uint32_t of(uint32_t c) const {
-    const uint2 w = __ldg(iw + (c >> 5));
+  __device__ __forceinline__ uint2 word(uint32_t c) const { return __ldg(iw + (c >> 5)); }
+  // the element a walk enters vertex c by, from c's word: its down edge, or
+  // its merged slot
+  __device__ __forceinline__ uint32_t of(uint32_t c, uint2 w) const {
     const uint32_t below = w.x & ((1u << (c & 31)) - 1u);
     return ((w.x >> (c & 31)) & 1u) ? n + w.y + (uint32_t)__popc(below) : c;
   }
-  __device__ __forceinline__ uint32_t down_slot(uint32_t v) const {  // v has a down edge
-    const uint2 w = __ldg(iw + (v >> 5));
+  __device__ __forceinline__ uint32_t down_slot(uint32_t v, uint2 w) const {  // v has a down edge
     return n + w.y + (uint32_t)__popc(w.x & ((1u << (v & 31)) - 1u));
   }
 };
 
+// One tile of TB_ITEMS vertices per thread in two rounds of independent loads
+// (the vertex's own words; the table words of its sibling, its first child
+// and itself), so a tile waits for two memory latencies rather than a chain
+// of them per vertex.
 __global__ void __launch_bounds__(256) k_tour_leaves(const uint32_t* __restrict__ p32, uint32_t n,
                                                      const uint32_t* __restrict__ fc,
                                                      const uint32_t* __restrict__ nsib,
-                                                     const uint32_t* __restrict__ root_bits, Entries ent,
+                                                     const uint32_t* __restrict__ head_bits, Entries ent,
                                                      Rec* __restrict__ rec, uint32_t* __restrict__ ruler_elem,
                                                      uint32_t* __restrict__ counter, uint32_t salt, uint32_t th,
                                                      uint32_t* __restrict__ leaf_bits, DevStatus* st) {
@@ -362,35 +410,61 @@ __global__ void __launch_bounds__(256) k_tour_leaves(const uint32_t* __restrict_
   const uint32_t lane = threadIdx.x & 31u;
   const uint64_t tile_sz = (uint64_t)blockDim.x * TB_ITEMS;
   for (uint64_t tile = (uint64_t)blockIdx.x * tile_sz; tile < n; tile += (uint64_t)gridDim.x * tile_sz) {
+    uint32_t pv[TB_ITEMS], sib[TB_ITEMS], first[TB_ITEMS], hw[TB_ITEMS];
+#pragma unroll
+    for (int i = 0; i < TB_ITEMS; ++i) {
+      const uint64_t v = tile + (uint64_t)i * blockDim.x + threadIdx.x;
+      pv[i] = (uint32_t)v;
+      sib[i] = first[i] = NO_CHILD;
+      hw[i] = 0;
+      if (v < n) {
+        pv[i] = __ldcs(p32 + v);
+        sib[i] = __ldcs(nsib + v);
+        first[i] = __ldcs(fc + v);
+        hw[i] = __ldg(head_bits + (v >> 5));
+      }
+    }
+    uint2 wsib[TB_ITEMS], wfirst[TB_ITEMS], wown[TB_ITEMS];
+#pragma unroll
+    for (int i = 0; i < TB_ITEMS; ++i) {
+      const uint32_t v = (uint32_t)(tile + (uint64_t)i * blockDim.x + threadIdx.x);
+      if (pv[i] >= n) pv[i] = v;  // k_link_children made bad parents roots; keeps every read in range
+      const bool child = v < n && pv[i] != v;
+      wsib[i] = wfirst[i] = wown[i] = make_uint2(0, 0);
+      if (child) {
+        if (sib[i] != NO_CHILD) wsib[i] = ent.word(sib[i]);
+        if (first[i] != NO_CHILD) {
+          wfirst[i] = ent.word(first[i]);
+          wown[i] = ent.word(v);
+        }
+      }
+    }
     Rec ru[TB_ITEMS], rd[TB_ITEMS];
     uint32_t sd[TB_ITEMS];
     uint32_t rl = 0, cnt = 0, has_down = 0;
 #pragma unroll
     for (int i = 0; i < TB_ITEMS; ++i) {
-      const uint64_t v = tile + (uint64_t)i * blockDim.x + threadIdx.x;
+      const uint32_t v = (uint32_t)(tile + (uint64_t)i * blockDim.x + threadIdx.x);
       sd[i] = 0;
       bool leaf = false;
       if (v < n) {
-        uint64_t p = __ldcs(p32 + v);
-        if (p >= n) p = v;
+        const uint32_t p = pv[i];
         if (p == v) {  // a root: the tour's terminal element (or an isolated vertex)
           ru[i].a = 0;
-          ru[i].b = (uint32_t)v;
+          ru[i].b = v;
           rl |= 1u << (2 * i);
           cnt++;
         } else {
-          const uint32_t sib = __ldcs(nsib + v), first = __ldcs(fc + v);
-          const uint32_t up_next = (sib != NO_CHILD) ? ent.of(sib) : (uint32_t)p;
-          bool head = false;
-          if ((__ldg(root_bits + (p >> 5)) >> (p & 31)) & 1u) head = __ldg(fc + p) == (uint32_t)v;
-          if (first != NO_CHILD) {
-            sd[i] = ent.down_slot((uint32_t)v);
+          const uint32_t up_next = (sib[i] != NO_CHILD) ? ent.of(sib[i], wsib[i]) : p;
+          const bool head = (hw[i] >> (v & 31)) & 1u;  // the down edge (or merged element) heading a tour
+          if (first[i] != NO_CHILD) {
+            sd[i] = ent.down_slot(v, wown[i]);
             ru[i].a = 1ull;
             ru[i].b = up_next;
             rd[i].a = ~0ull;  // -1
-            rd[i].b = ent.of(first);
+            rd[i].b = ent.of(first[i], wfirst[i]);
             has_down |= 1u << i;
-            if (sampled((uint32_t)v, salt, th)) {
+            if (sampled(v, salt, th)) {
               rl |= 1u << (2 * i);
               cnt++;
             }
@@ -402,7 +476,7 @@ __global__ void __launch_bounds__(256) k_tour_leaves(const uint32_t* __restrict_
             leaf = true;
             ru[i].a = 0;  // down (-1) and up (+1) in one element
             ru[i].b = up_next;
-            if (head || sampled((uint32_t)v, salt, th)) {
+            if (head || sampled(v, salt, th)) {
               rl |= 1u << (2 * i);
               cnt++;
             }
@@ -497,16 +571,18 @@ kascade_status root_forest_impl(kascade_ctx& ctx, const uint64_t* parent, uint32
   uint32_t* icount = alloc<uint32_t>(ctx, words);
   uint32_t* ipre = alloc<uint32_t>(ctx, words);
   uint32_t* leaf_bits = alloc<uint32_t>(ctx, words);
+  uint32_t* head_bits = alloc<uint32_t>(ctx, words);
   uint2* iw = alloc<uint2>(ctx, words);
   if (!rec || !ruler_elem || !ctr || !fc || !nsib || !p32 || !root_bits || !ibits || !icount || !ipre || !leaf_bits ||
-      !iw)
+      !head_bits || !iw)
     return KASCADE_ERR_OOM;
   KS_CUDA(cudaMemsetAsync(ctr, 0, 2 * sizeof(uint32_t), s));
+  KS_CUDA(cudaMemsetAsync(head_bits, 0, sizeof(uint32_t) * (size_t)words, s));
   KS_TRY(link_children(ctx, parent, n, fc, nsib, p32, root_bits, s));
   uint32_t downs = 0;
   {
     ProfScope ps(ctx, "tour_build", s);
-    k_internal_words<<<grid_for(ctx, n, 256, 8), 256, 0, s>>>(p32, fc, n, ibits, icount);
+    k_internal_words<<<grid_for(ctx, n, 256, 8), 256, 0, s>>>(p32, fc, n, ibits, icount, head_bits);
     KS_CHECK_LAUNCH();
     KS_TRY(exclusive_scan_u32(ctx, icount, ipre, words, ctr + 1, s));
     k_internal_pack<<<grid_for(ctx, words, 256, 8), 256, 0, s>>>(ibits, ipre, words, iw);
@@ -520,7 +596,7 @@ kascade_status root_forest_impl(kascade_ctx& ctx, const uint64_t* parent, uint32
     ProfScope ps(ctx, "tour_build", s);
     const unsigned grid = grid_for(ctx, ((uint64_t)n + 256 * TB_ITEMS - 1) / (256 * TB_ITEMS) * 256, 256, 8);
     const uint32_t th = (uint32_t)(4294967296.0 / (double)(p.spacing0 < 2 ? 2 : p.spacing0));
-    k_tour_leaves<<<grid, 256, 0, s>>>(p32, n, fc, nsib, root_bits, Entries{iw, n}, rec, ruler_elem, ctr,
+    k_tour_leaves<<<grid, 256, 0, s>>>(p32, n, fc, nsib, head_bits, Entries{iw, n}, rec, ruler_elem, ctr,
                                        mix32(p.seed ^ 0x70757254u), th, leaf_bits, ctx.d_status);
     KS_CHECK_LAUNCH();
   }
