@@ -6,8 +6,10 @@
 // -- one persistent launch with one device work queue -- serves every
 // instance:
 //   list element g (concatenated position)  -> record g
-//   forest vertex g                         -> record g (its up edge / tour end)
+//   forest vertex g                         -> record g (its up edge / tour end;
+//                                              a leaf's down and up edge in one)
 //   down edges of all forests (F of them)   -> records total_n .. total_n+F-1
+//                                              (a leaf's or a root's: a dead self loop)
 // Each instance's ruler spacing comes from its size class (the context's
 // size-class table, filled by the autotuner).  Roots are reported relative to
 // their own instance.
@@ -21,8 +23,9 @@
 namespace ks {
 
 kascade_status batch_tours(kascade_ctx& ctx, const uint64_t* fpar, uint32_t F, const uint32_t* fd, const uint32_t* foff,
-                           const uint32_t* fthresh, uint32_t nf, uint32_t down_base, Rec* rec, uint32_t* ruler_elem,
-                           uint32_t* counter, uint32_t salt, cudaStream_t s);
+                           const uint32_t* fthresh, const uint32_t* fhint, uint32_t nf, uint32_t down_base, Rec* rec,
+                           uint32_t* ruler_elem, uint32_t* counter, uint32_t* leaf_out, uint32_t salt,
+                           cudaStream_t s);
 
 namespace {
 
@@ -178,7 +181,7 @@ uint32_t spacing_for(const kascade_ctx& ctx, uint64_t n) {
 struct BatchTables {
   std::vector<DSeg> dsegs;
   std::vector<Item> items;
-  std::vector<uint32_t> fd, foff, fth, hint;
+  std::vector<uint32_t> fd, foff, fth, hint, fhint;
   std::vector<unsigned long long> seg_off;
   uint64_t total = 0, F = 0;
   uint32_t nseg = 0, nf = 0, M = 0, spacing_min = 0xFFFFFFFFu, spacing_max = 0;
@@ -186,7 +189,7 @@ struct BatchTables {
   // device copies
   DSeg* d_segs = nullptr;
   Item* d_items = nullptr;
-  uint32_t *d_fd = nullptr, *d_foff = nullptr, *d_fth = nullptr, *d_hint = nullptr;
+  uint32_t *d_fd = nullptr, *d_foff = nullptr, *d_fth = nullptr, *d_hint = nullptr, *d_fhint = nullptr;
   unsigned long long* d_off = nullptr;
 };
 
@@ -252,6 +255,17 @@ kascade_status batch_build_tables(const kascade_ctx& ctx, const kascade_segment*
       t.hint[k] = j;
     }
   }
+  // per 4096 compact forest vertices: the forest holding the first (and one
+  // entry past the last block, so a block's search range is [fhint[k], fhint[k+1]])
+  t.fhint.resize((size_t)((t.F + 4095) / 4096) + 1);
+  {
+    uint32_t j = 0;
+    for (size_t k = 0; k < t.fhint.size(); ++k) {
+      const uint64_t c = (uint64_t)k * 4096;
+      while (j + 1 < t.nf && t.fd[j + 1] <= c) ++j;
+      t.fhint[k] = j;
+    }
+  }
   t.M = (uint32_t)(total + t.F);
   t.dom_class = std::max_element(class_elems.begin(), class_elems.end()) - class_elems.begin();
   return KASCADE_OK;
@@ -265,7 +279,9 @@ kascade_status batch_upload_tables(kascade_ctx& ctx, BatchTables& t, cudaStream_
   t.d_fth = alloc<uint32_t>(ctx, t.fth.size() + 1);
   t.d_off = alloc<unsigned long long>(ctx, t.nseg);
   t.d_hint = alloc<uint32_t>(ctx, t.hint.size());
-  if (!t.d_segs || !t.d_items || !t.d_fd || !t.d_foff || !t.d_fth || !t.d_off || !t.d_hint) return KASCADE_ERR_OOM;
+  t.d_fhint = alloc<uint32_t>(ctx, t.fhint.size());
+  if (!t.d_segs || !t.d_items || !t.d_fd || !t.d_foff || !t.d_fth || !t.d_off || !t.d_hint || !t.d_fhint)
+    return KASCADE_ERR_OOM;
   KS_CUDA(cudaMemcpyAsync(t.d_segs, t.dsegs.data(), sizeof(DSeg) * t.nseg, cudaMemcpyHostToDevice, s));
   KS_CUDA(cudaMemcpyAsync(t.d_items, t.items.data(), sizeof(Item) * t.items.size(), cudaMemcpyHostToDevice, s));
   KS_CUDA(cudaMemcpyAsync(t.d_fd, t.fd.data(), sizeof(uint32_t) * t.fd.size(), cudaMemcpyHostToDevice, s));
@@ -275,6 +291,7 @@ kascade_status batch_upload_tables(kascade_ctx& ctx, BatchTables& t, cudaStream_
   }
   KS_CUDA(cudaMemcpyAsync(t.d_off, t.seg_off.data(), sizeof(unsigned long long) * t.nseg, cudaMemcpyHostToDevice, s));
   KS_CUDA(cudaMemcpyAsync(t.d_hint, t.hint.data(), sizeof(uint32_t) * t.hint.size(), cudaMemcpyHostToDevice, s));
+  KS_CUDA(cudaMemcpyAsync(t.d_fhint, t.fhint.data(), sizeof(uint32_t) * t.fhint.size(), cudaMemcpyHostToDevice, s));
   return KASCADE_OK;
 }
 
@@ -289,8 +306,12 @@ kascade_status batch_enqueue(kascade_ctx& ctx, const BatchTables& t, const uint6
   uint32_t* ruler_elem = alloc<uint32_t>(ctx, M);
   uint64_t* fpar = alloc<uint64_t>(ctx, t.F + 1);
   uint32_t* ctr = alloc<uint32_t>(ctx, 1);
-  if (!rec || !ruler_elem || !fpar || !ctr) return KASCADE_ERR_OOM;
+  // forest leaves by output position: their rank is one less than their depth
+  const uint64_t leaf_words = t.F ? (t.total + 31) / 32 : 0;
+  uint32_t* leaf_out = leaf_words ? alloc<uint32_t>(ctx, leaf_words) : nullptr;
+  if (!rec || !ruler_elem || !fpar || !ctr || (leaf_words && !leaf_out)) return KASCADE_ERR_OOM;
   KS_CUDA(cudaMemsetAsync(ctr, 0, sizeof(uint32_t), s));
+  if (leaf_out) KS_CUDA(cudaMemsetAsync(leaf_out, 0, sizeof(uint32_t) * leaf_words, s));
   Params p = make_params(ctx, opts, M);
   {
     // one chase launch serves every instance: its chains and block size come
@@ -313,9 +334,10 @@ kascade_status batch_enqueue(kascade_ctx& ctx, const BatchTables& t, const uint6
                                                           BWUnit{}, rec, fpar, ruler_elem, ctr, salt, ctx.d_status);
     KS_CHECK_LAUNCH();
   }
-  KS_TRY(batch_tours(ctx, fpar, (uint32_t)t.F, t.d_fd, t.d_foff, t.d_fth, t.nf, (uint32_t)t.total, rec, ruler_elem,
-                     ctr, mix32(p.seed ^ 0x70757254u), s));
-  SinkBatch sink{root_out, rank_out, (uint32_t)t.total, reinterpret_cast<const uint64_t*>(t.d_off), t.d_hint, t.nseg};
+  KS_TRY(batch_tours(ctx, fpar, (uint32_t)t.F, t.d_fd, t.d_foff, t.d_fth, t.d_fhint, t.nf, (uint32_t)t.total, rec,
+                     ruler_elem, ctr, leaf_out, mix32(p.seed ^ 0x70757254u), s));
+  SinkBatch sink{root_out, rank_out, (uint32_t)t.total, reinterpret_cast<const uint64_t*>(t.d_off), t.d_hint, t.nseg,
+                 leaf_out};
   p.algorithm = KASCADE_ALGO_SPARSE_RULING_SET;
   // the write-free chase's hop cap follows the sparsest instance's spacing
   if (!(opts && opts->max_chain)) p.max_chain = 64u * std::max(t.spacing_max, p.spacing0) + 1024u;

@@ -393,10 +393,10 @@ __global__ void __launch_bounds__(FIN_THREADS, 2) k_place(const LogEnt* __restri
                                                             const uint64_t* __restrict__ seg_off,
                                                             const uint32_t* __restrict__ hint, uint32_t nseg,
                                                             const uint32_t* __restrict__ plus_one, DevStatus* st) {
-  const SinkBatch inst{nullptr, nullptr, 0, seg_off, hint, nseg};  // instance offsets of a batch
   extern __shared__ __align__(16) unsigned char smraw[];
   unsigned long long* rank_s = reinterpret_cast<unsigned long long*>(smraw);  // SUB entries
   uint32_t* root_s = reinterpret_cast<uint32_t*>(rank_s + SUB);               // SUB entries
+  __shared__ uint32_t plus_s[SUB / 32];                                       // the sub-window's plus_one words
   const uint32_t lane = threadIdx.x & 31u;
   if (blockIdx.x == 0 && threadIdx.x == 0 && heads_are_rulers) {
     const uint32_t want = n - limit;
@@ -410,6 +410,9 @@ __global__ void __launch_bounds__(FIN_THREADS, 2) k_place(const LogEnt* __restri
     const uint32_t len = min(SUB, limit - lo);
     const uint32_t cnt = min(__ldcg(cursor2 + (uint64_t)it * CURSOR_STRIDE), SUB);
     for (uint32_t i = threadIdx.x; i < SUB; i += FIN_THREADS) root_s[i] = NO_ROOT;
+    // lo is a multiple of SUB: the sub-window's bits are whole words
+    if (plus_one)
+      for (uint32_t i = threadIdx.x; i < (len + 31) / 32; i += FIN_THREADS) plus_s[i] = __ldg(plus_one + (lo >> 5) + i);
     __syncthreads();
     const LogEnt* src = part2 + (uint64_t)it * SUB;
     for (uint32_t g = 0; g < SUB / FIN_THREADS; g += FIN_GROUP) {
@@ -432,16 +435,34 @@ __global__ void __launch_bounds__(FIN_THREADS, 2) k_place(const LogEnt* __restri
       }
     }
     __syncthreads();
+    // a batch: the instance holding this thread's first element, its offset
+    // and the next instance's; a thread's elements only move forward
+    uint32_t jseg = 0;
+    unsigned long long cur_off = 0, next_off = ~0ull;
+    if (seg_off) {
+      const uint32_t x0 = lo + threadIdx.x;
+      jseg = __ldg(hint + (x0 >> 12));
+      while (jseg + 1 < nseg && __ldg(seg_off + jseg + 1) <= x0) ++jseg;
+      cur_off = __ldg(seg_off + jseg);
+      next_off = jseg + 1 < nseg ? __ldg(seg_off + jseg + 1) : ~0ull;
+    }
     for (uint32_t i0 = 0; i0 < len; i0 += FIN_THREADS) {
       const uint32_t i = i0 + threadIdx.x;
       bool un = false;
       if (i < len) {
         const uint32_t r = root_s[i];
         un = r == NO_ROOT;
-        const unsigned long long ibase = (seg_off && !un) ? inst.base_of(lo + i) : 0ull;
+        if (seg_off) {
+          while (lo + i >= next_off) {
+            ++jseg;
+            cur_off = next_off;
+            next_off = jseg + 1 < nseg ? __ldg(seg_off + jseg + 1) : ~0ull;
+          }
+        }
+        const unsigned long long ibase = un ? 0ull : cur_off;
         __stcs(reinterpret_cast<unsigned long long*>(root_out) + lo + i,
                un ? NOT_REACHED : (unsigned long long)r - ibase);
-        const unsigned long long add = plus_one ? (__ldg(plus_one + ((lo + i) >> 5)) >> ((lo + i) & 31)) & 1u : 0u;
+        const unsigned long long add = plus_one ? (plus_s[i >> 5] >> (i & 31)) & 1u : 0u;
         __stcs(reinterpret_cast<unsigned long long*>(rank_out) + lo + i, un ? 0ull : rank_s[i] + add);
       }
       const uint32_t m = __ballot_sync(FULL, un);

@@ -20,9 +20,11 @@
 // rank + 1.  Otherwise the depth of v is the rank of slot v, so the map-back
 // is a coalesced pass over slots 0..n-1; the tour of a tree starts at the
 // element entering the root's first child and ends in the root's terminal
-// slot.  A batch of forests keeps both edges of every vertex (slots by
-// vertex, no compaction); compute_euler_tour (the reference's numbering)
-// sorts the children.
+// slot.  A batch of forests keeps one up and one down slot per vertex (slots
+// by vertex, no compaction, so its record count does not depend on the
+// forests' shapes) and contracts leaves the same way: a leaf's down slot,
+// like a root's, is a dead self loop no element points to.
+// compute_euler_tour (the reference's numbering) sorts the children.
 #include <algorithm>
 
 #include "ranker.cuh"
@@ -63,10 +65,13 @@ struct SlotsBatch {
   const uint32_t* fd;       // nf + 1 compact starts
   const uint32_t* foff;     // nf concatenated offsets
   const uint32_t* fthresh;  // nf sampling thresholds
+  const uint32_t* fhint;    // per 4096 compact vertices: the forest holding the first
   uint32_t nf;
   uint32_t down_base;
   __device__ __forceinline__ uint32_t seg_of(uint32_t c) const {
-    uint32_t lo = 0, hi = nf;  // last j with fd[j] <= c
+    // last j with fd[j] <= c, between the forests holding this block's first
+    // vertex and the next block's
+    uint32_t lo = __ldg(fhint + (c >> 12)), hi = min(__ldg(fhint + (c >> 12) + 1) + 1, nf);
     while (hi - lo > 1) {
       const uint32_t mid = (lo + hi) >> 1;
       if (__ldg(fd + mid) <= c)
@@ -158,61 +163,124 @@ __global__ void __launch_bounds__(256) k_link_children(const uint64_t* __restric
   }
 }
 
-// Both tour records of every vertex, at the slots `slots` gives, from the child
-// lists; rulers sampled among the slots and numbered (one atomic per tile).
-// The down edge into a root's first child is the head of that tree's tour
-// and always a ruler, so no tour element is left unreached; roots' slots are
-// self loops (the terminal, and an unused down slot) and rulers.
+// Sets bit g of `bits` for every lane with `set`: one atomic per distinct word
+// the warp touches.  Called by all lanes of the warp.
+__device__ __forceinline__ void warp_set_bits(uint32_t* __restrict__ bits, bool set, uint32_t g, uint32_t lane) {
+  uint32_t pending = __ballot_sync(0xffffffffu, set);
+  while (pending != 0u) {
+    const int l = __ffs(pending) - 1;
+    const uint32_t w = __shfl_sync(0xffffffffu, g >> 5, l);
+    const bool in = set && (g >> 5) == w;
+    const uint32_t word = __reduce_or_sync(0xffffffffu, in ? 1u << (g & 31) : 0u);
+    if ((int)lane == l) atomicOr(bits + w, word);
+    pending &= ~__ballot_sync(0xffffffffu, in);
+  }
+}
+
+// The tour records of a batch's forests at the slots `slots` gives, from the
+// child lists, with leaf contraction as for single forests: a leaf's down and
+// up edge are one element of weight 0 at its up slot (its output position),
+// whose rank is one less than the leaf's depth (bit set in leaf_out, indexed
+// by output position).  The down slot of a leaf or a root holds a dead self
+// loop of weight 0 that no element points to: the slots keep one place per
+// vertex, so the batch's record count stays fixed (a plan's shapes do not
+// depend on its forests' shapes) while the chase visits ~1.5 elements per
+// vertex instead of 2.  A tree's tour starts at the element entering its
+// root's list head (head_bits), which is always a ruler; ibits (vertices with
+// a down edge) tells which element a sibling or first child is entered by.
+// A tile's loads are issued in two independent rounds; rulers are sampled
+// among the slots and numbered with one atomic per tile.
 template <class Slots>
 __global__ void __launch_bounds__(256) k_tour_links(const uint32_t* __restrict__ p32, uint32_t n,
                                                     const uint32_t* __restrict__ fc,
                                                     const uint32_t* __restrict__ nsib,
-                                                    const uint32_t* __restrict__ root_bits, Rec* __restrict__ rec,
+                                                    const uint32_t* __restrict__ ibits,
+                                                    const uint32_t* __restrict__ head_bits, Rec* __restrict__ rec,
                                                     uint32_t* __restrict__ ruler_elem, uint32_t* __restrict__ counter,
-                                                    uint32_t salt, Slots slots, DevStatus* st) {
+                                                    uint32_t* __restrict__ leaf_out, uint32_t salt, Slots slots,
+                                                    DevStatus* st) {
   __shared__ uint32_t sm[33];
   __shared__ uint32_t sbase;
+  const uint32_t lane = threadIdx.x & 31u;
   const uint64_t tile_sz = (uint64_t)blockDim.x * TB_ITEMS;
   for (uint64_t tile = (uint64_t)blockIdx.x * tile_sz; tile < n; tile += (uint64_t)gridDim.x * tile_sz) {
+    uint32_t pv[TB_ITEMS], sib[TB_ITEMS], first[TB_ITEMS], hw[TB_ITEMS], jv[TB_ITEMS];
+#pragma unroll
+    for (int i = 0; i < TB_ITEMS; ++i) {
+      const uint64_t v = tile + (uint64_t)i * blockDim.x + threadIdx.x;
+      pv[i] = (uint32_t)v;
+      sib[i] = first[i] = NO_CHILD;
+      hw[i] = jv[i] = 0;
+      if (v < n) {
+        pv[i] = __ldcs(p32 + v);  // in range: k_link_children made bad parents roots
+        sib[i] = __ldcs(nsib + v);
+        first[i] = __ldcs(fc + v);
+        hw[i] = __ldg(head_bits + (v >> 5));
+        jv[i] = slots.seg_of((uint32_t)v);  // v, its parent and its children belong to the same forest
+      }
+    }
+    uint32_t wsib[TB_ITEMS], wfirst[TB_ITEMS];
+#pragma unroll
+    for (int i = 0; i < TB_ITEMS; ++i) {
+      const uint32_t v = (uint32_t)(tile + (uint64_t)i * blockDim.x + threadIdx.x);
+      if (pv[i] >= n) pv[i] = v;
+      wsib[i] = wfirst[i] = 0;
+      if (v < n && pv[i] != v) {
+        if (sib[i] != NO_CHILD) wsib[i] = __ldg(ibits + (sib[i] >> 5));
+        if (first[i] != NO_CHILD) wfirst[i] = __ldg(ibits + (first[i] >> 5));
+      }
+    }
     Rec ru[TB_ITEMS], rd[TB_ITEMS];
     uint32_t su[TB_ITEMS], sd[TB_ITEMS];
     uint32_t rl = 0, cnt = 0;
 #pragma unroll
     for (int i = 0; i < TB_ITEMS; ++i) {
-      const uint64_t v = tile + (uint64_t)i * blockDim.x + threadIdx.x;
+      const uint32_t v = (uint32_t)(tile + (uint64_t)i * blockDim.x + threadIdx.x);
       su[i] = sd[i] = 0;
-      if (v >= n) continue;
-      uint64_t p = __ldcs(p32 + v);  // in range: k_link_children made bad parents roots
-      if (p >= n) p = v;
-      const uint32_t sib = __ldcs(nsib + v), first = __ldcs(fc + v);
-      const uint32_t j = slots.seg_of((uint32_t)v);  // v and p belong to the same forest
-      const uint32_t th = slots.thresh(j);
-      const uint32_t up = slots.up((uint32_t)v, j), down = slots.down((uint32_t)v);
-      su[i] = up;
-      sd[i] = down;
-      if (p == v) {
-        ru[i].a = 0;
-        ru[i].b = up;
-        rd[i].a = 0;
+      bool leaf = false;
+      if (v < n) {
+        const uint32_t j = jv[i], p = pv[i];
+        const uint32_t th = slots.thresh(j);
+        const uint32_t up = slots.up(v, j), down = slots.down(v);
+        su[i] = up;
+        sd[i] = down;
+        rd[i].a = 0;  // a dead self loop unless v keeps a down edge
         rd[i].b = down;
-        rl |= 3u << (2 * i);
-        cnt += 2;
-        continue;
+        if (p == v) {  // a root: the tour's terminal element (or an isolated vertex)
+          ru[i].a = 0;
+          ru[i].b = up;
+          rl |= 1u << (2 * i);
+          cnt++;
+        } else {
+          // the element a walk enters child c by: its down edge, or its merged slot
+          const uint32_t up_next = (sib[i] != NO_CHILD)
+                                       ? (((wsib[i] >> (sib[i] & 31)) & 1u) ? slots.down(sib[i]) : slots.up(sib[i], j))
+                                       : slots.up(p, j);
+          const bool head = (hw[i] >> (v & 31)) & 1u;
+          ru[i].b = up_next;
+          if (first[i] != NO_CHILD) {
+            ru[i].a = 1ull;
+            rd[i].a = ~0ull;  // -1
+            rd[i].b = ((wfirst[i] >> (first[i] & 31)) & 1u) ? slots.down(first[i]) : slots.up(first[i], j);
+            if (sampled(up, salt, th)) {
+              rl |= 1u << (2 * i);
+              cnt++;
+            }
+            if (head || sampled(down, salt, th)) {
+              rl |= 2u << (2 * i);
+              cnt++;
+            }
+          } else {
+            leaf = true;
+            ru[i].a = 0;  // down (-1) and up (+1) in one element
+            if (head || sampled(up, salt, th)) {
+              rl |= 1u << (2 * i);
+              cnt++;
+            }
+          }
+        }
       }
-      ru[i].a = 1ull;
-      ru[i].b = (sib != NO_CHILD) ? slots.down(sib) : slots.up((uint32_t)p, j);
-      rd[i].a = ~0ull;  // -1
-      rd[i].b = (first != NO_CHILD) ? slots.down(first) : up;
-      bool head = false;
-      if ((__ldg(root_bits + (p >> 5)) >> (p & 31)) & 1u) head = __ldg(fc + p) == (uint32_t)v;
-      if (sampled(up, salt, th)) {
-        rl |= 1u << (2 * i);
-        cnt++;
-      }
-      if (head || sampled(down, salt, th)) {
-        rl |= 2u << (2 * i);
-        cnt++;
-      }
+      warp_set_bits(leaf_out, leaf, su[i], lane);
     }
     uint32_t total;
     uint32_t pre = block_exclusive_scan(cnt, sm, &total);
@@ -244,7 +312,7 @@ __global__ void __launch_bounds__(256) k_tour_links(const uint32_t* __restrict__
         id++;
       }
       st_rec_cs(rec + su[i], ru[i]);
-      st_rec_cs(rec + sd[i], rd[i]);
+      st_rec_cs(rec + sd[i], rd[i]);  // every down slot, dead or not: the stores stay coalesced
     }
     __syncthreads();
   }
@@ -534,21 +602,29 @@ kascade_status link_children(kascade_ctx& ctx, const uint64_t* parent, uint32_t 
   return KASCADE_OK;
 }
 
-// Child lists and both tour records of every vertex at the slots `slots`
-// gives (a batch's forests); ruler ids continue `counter`.
+// Child lists and the leaf-contracted tour records of every vertex at the
+// slots `slots` gives (a batch's forests); ruler ids continue `counter`,
+// leaves are marked in leaf_out (by output position, zeroed by the caller).
 template <class Slots>
 kascade_status build_tour(kascade_ctx& ctx, const uint64_t* parent, uint32_t n, const Slots& slots, Rec* rec,
-                          uint32_t* ruler_elem, uint32_t* counter, uint32_t salt, cudaStream_t s) {
+                          uint32_t* ruler_elem, uint32_t* counter, uint32_t* leaf_out, uint32_t salt, cudaStream_t s) {
+  const uint64_t words = ((uint64_t)n + 31) / 32;
   uint32_t* fc = alloc<uint32_t>(ctx, n);
   uint32_t* nsib = alloc<uint32_t>(ctx, n);
   uint32_t* p32 = alloc<uint32_t>(ctx, n);
-  uint32_t* root_bits = alloc<uint32_t>(ctx, ((uint64_t)n + 31) / 32);
-  if (!fc || !nsib || !p32 || !root_bits) return KASCADE_ERR_OOM;
+  uint32_t* root_bits = alloc<uint32_t>(ctx, words);
+  uint32_t* ibits = alloc<uint32_t>(ctx, words);
+  uint32_t* icount = alloc<uint32_t>(ctx, words);
+  uint32_t* head_bits = alloc<uint32_t>(ctx, words);
+  if (!fc || !nsib || !p32 || !root_bits || !ibits || !icount || !head_bits) return KASCADE_ERR_OOM;
+  KS_CUDA(cudaMemsetAsync(head_bits, 0, sizeof(uint32_t) * words, s));
   KS_TRY(link_children(ctx, parent, n, fc, nsib, p32, root_bits, s));
   ProfScope ps(ctx, "tour_build", s);
+  k_internal_words<<<grid_for(ctx, n, 256, 8), 256, 0, s>>>(p32, fc, n, ibits, icount, head_bits);
+  KS_CHECK_LAUNCH();
   const unsigned grid = grid_for(ctx, ((uint64_t)n + 256 * TB_ITEMS - 1) / (256 * TB_ITEMS) * 256, 256, 8);
-  k_tour_links<Slots><<<grid, 256, 0, s>>>(p32, n, fc, nsib, root_bits, rec, ruler_elem, counter, salt, slots,
-                                           ctx.d_status);
+  k_tour_links<Slots><<<grid, 256, 0, s>>>(p32, n, fc, nsib, ibits, head_bits, rec, ruler_elem, counter, leaf_out,
+                                           salt, slots, ctx.d_status);
   KS_CHECK_LAUNCH();
   return KASCADE_OK;
 }
@@ -616,11 +692,12 @@ kascade_status root_forest_impl(kascade_ctx& ctx, const uint64_t* parent, uint32
 // space (fpar[c] = compact parent of compact vertex c); records go to the
 // slots described by SlotsBatch, ruler ids continue `counter`.
 kascade_status batch_tours(kascade_ctx& ctx, const uint64_t* fpar, uint32_t F, const uint32_t* fd, const uint32_t* foff,
-                           const uint32_t* fthresh, uint32_t nf, uint32_t down_base, Rec* rec, uint32_t* ruler_elem,
-                           uint32_t* counter, uint32_t salt, cudaStream_t s) {
+                           const uint32_t* fthresh, const uint32_t* fhint, uint32_t nf, uint32_t down_base, Rec* rec,
+                           uint32_t* ruler_elem, uint32_t* counter, uint32_t* leaf_out, uint32_t salt,
+                           cudaStream_t s) {
   if (F == 0) return KASCADE_OK;
-  const SlotsBatch slots{fd, foff, fthresh, nf, down_base};
-  return build_tour(ctx, fpar, F, slots, rec, ruler_elem, counter, salt, s);
+  const SlotsBatch slots{fd, foff, fthresh, fhint, nf, down_base};
+  return build_tour(ctx, fpar, F, slots, rec, ruler_elem, counter, leaf_out, salt, s);
 }
 
 kascade_status compute_euler_tour_impl(kascade_ctx& ctx, const uint64_t* parent, uint32_t n, uint64_t* tour,

@@ -119,6 +119,8 @@ struct SinkTour {
 // roots are reported relative to their instance.  seg_off holds the nseg
 // instance offsets (non-decreasing), hint[k] the instance containing element
 // k * 4096.  Elements at or beyond `total` (tour down edges) give no output.
+// plus_one (optional): bit x set for a forest leaf whose down and up edge are
+// one element, whose rank is then one less than the leaf's depth.
 struct SinkBatch {
   static constexpr bool kWriteFree = true;
   uint64_t* root;
@@ -127,8 +129,13 @@ struct SinkBatch {
   const uint64_t* seg_off;
   const uint32_t* hint;
   uint32_t nseg;
+  const uint32_t* plus_one = nullptr;
   uint32_t limit(uint32_t n) const { return n < total ? n : total; }
-  LogTarget log_target(uint32_t n) const { return LogTarget{root, rank, limit(n), 0, 0, seg_off, hint, nseg}; }
+  LogTarget log_target(uint32_t n) const {
+    LogTarget t{root, rank, limit(n), 0, 0, seg_off, hint, nseg};
+    t.plus_one = plus_one;
+    return t;
+  }
   __device__ __forceinline__ uint64_t base_of(uint32_t x) const {
     uint32_t j = __ldg(hint + (x >> 12));
     while (j + 1 < nseg && __ldg(seg_off + j + 1) <= x) ++j;
@@ -142,6 +149,7 @@ struct SinkBatch {
       __stcs(rank + x, 0ull);
       return;
     }
+    if (plus_one) rk += (__ldg(plus_one + (x >> 5)) >> (x & 31)) & 1u;
     __stcs(root + x, (unsigned long long)(rt - b));
     __stcs(rank + x, (unsigned long long)rk);
   }

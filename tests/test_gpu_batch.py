@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 import torch
 
-from gpu_util import DEEP, host_i64, host_u64
+from gpu_util import DEEP, dev64, host_i64, host_u64
 
 pytestmark = pytest.mark.gpu
 
@@ -277,3 +277,55 @@ def test_batch_4096_instances_full_size_against_reference_chase(kb, oracle_mod):
     exp_rank = torch.from_numpy(r_h).to(dev)
     bad = (exp_root != root) | (exp_rank != rank)
     assert not bool(bad.any()), f"{int(bad.sum())} elements differ, first at {int(bad.nonzero()[0])}"
+
+
+def _shaped_forests(rng):
+    """Forests that exercise every element of a batch's leaf-contracted tour:
+    isolated roots, stars (a root whose every child is a leaf), paths (no
+    leaf but the last vertex), caterpillars, two-vertex trees, several trees
+    in one forest, and random trees with vertices relabelled so that parents
+    are not below their children."""
+    out = [np.array([0], np.uint64), np.array([0, 1, 2, 3], np.uint64), np.zeros(50, np.uint64),
+           np.array([1, 1], np.uint64), np.array([0, 0, 2, 2, 4, 4], np.uint64)]
+    path = np.arange(1, 801, dtype=np.uint64)
+    path[-1] = 799
+    out.append(path)
+    spine = 300
+    cat = np.empty(spine * 3, np.uint64)
+    cat[:spine] = np.arange(-1, spine - 1) % spine
+    cat[0] = 0
+    cat[spine:] = rng.integers(0, spine, 2 * spine)
+    out.append(cat)
+    for n in (33, 257, 4000):
+        par = np.arange(n, dtype=np.uint64)
+        for v in range(1, n):
+            if rng.random() < 0.97:
+                par[v] = rng.integers(0, v)
+        perm = rng.permutation(n)
+        relabel = np.empty(n, np.uint64)
+        relabel[perm] = np.arange(n, dtype=np.uint64)
+        p2 = np.empty(n, np.uint64)
+        p2[relabel] = relabel[par]
+        out.append(p2)
+    return out
+
+
+@pytest.mark.parametrize("tuning", [{}, DEEP, dict(level0_mode=1), dict(level0_mode=2), dict(DEEP, level0_mode=2),
+                                    dict(ruler_spacing=3, level0_mode=2), dict(base_case_size=1 << 16)])
+def test_batch_forest_shapes(kb, oracle_mod, tuning):
+    """Hand-shaped forests between lists in one batch, every tuning path
+    (single-CTA base case, stamping and write-free level 0, deep recursion):
+    depths and roots equal the oracle's, leaves included."""
+    rng = np.random.default_rng(0xF0)
+    parts, kinds = [], []
+    for f in _shaped_forests(rng):
+        lst = oracle_mod.gen_list(int(rng.integers(1, 500)), int(rng.integers(1 << 30)), 0)
+        parts += [lst, f]
+        kinds += [kb.SEG_LIST, kb.SEG_FOREST]
+    sizes = np.array([p.size for p in parts], np.int64)
+    kinds = np.array(kinds)
+    inputs = dev64(np.concatenate(parts))
+    segs = kb.make_segments(sizes, kinds)
+    for _ in range(2):  # a second call on the same context reuses its scratch
+        root, rank = kb.rank_batch(inputs, segs, None, tuning=kb.GpuTuning(**tuning))
+        _check(kb, oracle_mod, inputs, None, sizes, kinds, root, rank)
