@@ -109,7 +109,8 @@ __global__ void __launch_bounds__(512) k_chase_log(const Rec* __restrict__ rec, 
                                                    Rec* __restrict__ rec_next, uint32_t* __restrict__ work,
                                                    LogEnt* __restrict__ log, uint32_t* __restrict__ chunk_fill,
                                                    uint32_t* __restrict__ chunk_cursor, uint32_t nchunks,
-                                                   uint32_t max_hops, DevStatus* st) {
+                                                   uint32_t max_hops, uint32_t* __restrict__ has_pred,
+                                                   DevStatus* st) {
   constexpr uint32_t BATCH = 32u * C;
   if (r_dev) r = min(r, *r_dev);  // the ruler count on the device, r its capacity
   const uint32_t lane = threadIdx.x & 31u;
@@ -191,7 +192,10 @@ __global__ void __launch_bounds__(512) k_chase_log(const Rec* __restrict__ rec, 
       if (act & (1u << c)) {
         if (tag_ruler(rr[c].c)) {
           // back at its own ruler: a rootless cycle holding one ruler
-          if (tag_id(rr[c].c) == cid[c]) set_error(st, KASCADE_ERR_CYCLE, cid[c]);
+          if (tag_id(rr[c].c) == cid[c])
+            set_error(st, KASCADE_ERR_CYCLE, cid[c]);
+          else if (has_pred)  // that ruler has a predecessor in the ruler sub-list
+            atomicOr(has_pred + (tag_id(rr[c].c) >> 5), 1u << (tag_id(rr[c].c) & 31));
           Rec o;
           o.a = acc[c];
           o.b = tag_id(rr[c].c);
@@ -571,10 +575,10 @@ template <int C>
 kascade_status launch_chase_log_c(kascade_ctx& ctx, const Rec* rec, uint32_t n, const uint32_t* ruler_elem, uint32_t r,
                                   const uint32_t* r_dev, Rec* rec_next, uint32_t* work, LogEnt* log,
                                   uint32_t* chunk_fill, uint32_t* chunk_cursor, uint32_t nchunks, uint32_t max_hops,
-                                  unsigned grid, uint32_t block, cudaStream_t s) {
+                                  uint32_t* has_pred, unsigned grid, uint32_t block, cudaStream_t s) {
   ProfScope ps(ctx, "chase", s);
   k_chase_log<C><<<grid, block, 0, s>>>(rec, n, ruler_elem, r, r_dev, rec_next, work, log, chunk_fill, chunk_cursor,
-                                      nchunks, max_hops, ctx.d_status);
+                                      nchunks, max_hops, has_pred, ctx.d_status);
   KS_CHECK_LAUNCH();
   return KASCADE_OK;
 }
@@ -616,11 +620,15 @@ kascade_status rank_level0_log(kascade_ctx& ctx, const Rec* rec, uint32_t n, uin
   Rec* rec1 = alloc<Rec>(ctx, r0);
   Out* out1 = alloc<Out>(ctx, r0);
   uint32_t* lv = r0_dev ? alloc<uint32_t>(ctx, MAX_DEV_LEVELS + 2) : nullptr;  // level sizes (device)
-  if (!log || !chunk_fill || !counters || !rec1 || !out1 || (r0_dev && !lv)) return KASCADE_ERR_OOM;
+  // device-driven levels: the rulers a chain ended at (level-1 list heads are the others)
+  const uint64_t pwords = ((uint64_t)r0 + 31) / 32;
+  uint32_t* pred1 = r0_dev ? alloc<uint32_t>(ctx, pwords) : nullptr;
+  if (!log || !chunk_fill || !counters || !rec1 || !out1 || (r0_dev && (!lv || !pred1))) return KASCADE_ERR_OOM;
   KS_CUDA(cudaMemsetAsync(chunk_fill, 0, sizeof(uint32_t) * nchunks, s));
   KS_CUDA(cudaMemsetAsync(counters, 0, sizeof(uint32_t) * 8, s));
   if (r0_dev) {
     KS_CUDA(cudaMemsetAsync(lv, 0, sizeof(uint32_t) * (MAX_DEV_LEVELS + 2), s));
+    KS_CUDA(cudaMemsetAsync(pred1, 0, sizeof(uint32_t) * pwords, s));
     KS_TRY(launch_check_count(ctx, r0_dev, r0, lv + 1, s));
   }
   const uint32_t* r_dev = r0_dev ? lv + 1 : nullptr;
@@ -633,22 +641,22 @@ kascade_status rank_level0_log(kascade_ctx& ctx, const Rec* rec, uint32_t n, uin
   switch (C) {
     case 1:
       KS_TRY(launch_chase_log_c<1>(ctx, rec, n, ruler_elem0, r0, r_dev, rec1, chase_work, log, chunk_fill,
-                                   chunk_cursor, nchunks, max_hops, grid, block, s));
+                                   chunk_cursor, nchunks, max_hops, pred1, grid, block, s));
       break;
     case 4:
       KS_TRY(launch_chase_log_c<4>(ctx, rec, n, ruler_elem0, r0, r_dev, rec1, chase_work, log, chunk_fill,
-                                   chunk_cursor, nchunks, max_hops, grid, block, s));
+                                   chunk_cursor, nchunks, max_hops, pred1, grid, block, s));
       break;
     default:
       KS_TRY(launch_chase_log_c<2>(ctx, rec, n, ruler_elem0, r0, r_dev, rec1, chase_work, log, chunk_fill,
-                                   chunk_cursor, nchunks, max_hops, grid, block, s));
+                                   chunk_cursor, nchunks, max_hops, pred1, grid, block, s));
   }
   // level-1 elements are level-0 rulers: their level-0 index is ruler_elem0
   int levels = 0;
   if (r0_dev) {
     k_hop_cap_status<<<1, 1, 0, s>>>(ctx.d_status);
     KS_CHECK_LAUNCH();
-    KS_TRY(rank_deep_dev(ctx, rec1, out1, r0, lv, ruler_elem0, p, s, &levels));
+    KS_TRY(rank_deep_dev(ctx, rec1, out1, r0, lv, ruler_elem0, pred1, p, s, &levels));
   } else {
     // a chain hit the hop cap: let the caller rerun level 0 on the stamping path
     uint32_t over = 0;

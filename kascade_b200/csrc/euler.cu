@@ -34,8 +34,8 @@ namespace ks {
 
 namespace {
 
-constexpr int TB_ITEMS = 4;
-constexpr int LINK_ITEMS = 4;  // vertices per thread in one linking round
+constexpr int TB_ITEMS = 2;  // vertices per thread in the tour kernels (fewer registers, more resident warps)
+constexpr int LINK_ITEMS = 8;  // vertices per thread in one linking round
 
 inline int bits_for(uint64_t n) {
   int b = 1;

@@ -239,13 +239,19 @@ __global__ void __launch_bounds__(256) k_prepare_tma(const uint64_t* __restrict_
 // n_dev (device-driven recursion): the level's size is read from device
 // memory, n is then its capacity; rulers beyond cap_next are reported as an
 // overflow (KASCADE_ERR_TIMEOUT, the caller reruns on the host-driven path).
+// has_pred (optional): bit x set when a chain of the level above ended at x;
+// an element without it heads its list at this level and becomes a ruler, so
+// no element of this level is left for propagation to walk to its first
+// ruler (a batch's level holds one list per instance, and the longest of
+// those walks would set the propagation's duration).
 __global__ void __launch_bounds__(256) k_prepare_level(Rec* __restrict__ rec, uint32_t n,
                                                        const uint32_t* __restrict__ n_dev, uint32_t cap_next,
                                                        const uint32_t* __restrict__ elem0,
                                                        uint32_t* __restrict__ ruler_elem,
                                                        uint32_t* __restrict__ elem0_next,
                                                        uint32_t* __restrict__ counter, uint32_t salt,
-                                                       uint32_t thresh, DevStatus* st) {
+                                                       uint32_t thresh, const uint32_t* __restrict__ has_pred,
+                                                       DevStatus* st) {
   __shared__ uint32_t sm[33];
   __shared__ uint32_t sbase;
   if (n_dev) n = min(*n_dev, n);
@@ -262,7 +268,8 @@ __global__ void __launch_bounds__(256) k_prepare_level(Rec* __restrict__ rec, ui
           set_error(st, KASCADE_ERR_OUT_OF_RANGE, x);
           rv[i].b = (uint32_t)x;
         }
-        if (rv[i].b == (uint32_t)x || sampled((uint32_t)x, salt, thresh)) {
+        const bool head = has_pred && !((__ldg(has_pred + (x >> 5)) >> (x & 31)) & 1u);
+        if (rv[i].b == (uint32_t)x || head || sampled((uint32_t)x, salt, thresh)) {
           rl |= 1u << i;
           cnt++;
         }
@@ -318,7 +325,8 @@ template <int C>
 __global__ void __launch_bounds__(512) k_chase(Rec* __restrict__ rec, uint32_t n, const uint32_t* __restrict__ n_dev,
                                                const uint32_t* __restrict__ ruler_elem, uint32_t r,
                                                const uint32_t* __restrict__ r_dev, Rec* __restrict__ rec_next,
-                                               uint32_t* __restrict__ work, DevStatus* st) {
+                                               uint32_t* __restrict__ work, uint32_t* __restrict__ has_pred,
+                                               DevStatus* st) {
   // device-driven recursion: sizes from device memory, n and r capacities
   if (n_dev) n = min(*n_dev, n);
   if (r_dev) r = min(*r_dev, r);
@@ -410,7 +418,10 @@ __global__ void __launch_bounds__(512) k_chase(Rec* __restrict__ rec, uint32_t n
       } else if (tag_ruler(tg)) {
         // back at its own ruler: a cycle without a root that holds one ruler
         // (a valid chain only ends at another ruler)
-        if (tag_id(tg) == cid[c]) set_error(st, KASCADE_ERR_CYCLE, cid[c]);
+        if (tag_id(tg) == cid[c])
+          set_error(st, KASCADE_ERR_CYCLE, cid[c]);
+        else if (has_pred)
+          atomicOr(has_pred + (tag_id(tg) >> 5), 1u << (tag_id(tg) & 31));  // that ruler has a predecessor
         Rec o;
         o.a = acc[c];
         o.b = tag_id(tg);
@@ -701,7 +712,7 @@ kascade_status launch_chase_c(kascade_ctx& ctx, Rec* rec, uint32_t n, const uint
   uint64_t need_blocks = (need + warps_per_block - 1) / warps_per_block;
   if (need_blocks < grid) grid = (unsigned)(need_blocks ? need_blocks : 1);
   ProfScope ps(ctx, "chase", s);
-  k_chase<C><<<grid, block, 0, s>>>(rec, n, nullptr, ruler_elem, r, nullptr, rec_next, work, ctx.d_status);
+  k_chase<C><<<grid, block, 0, s>>>(rec, n, nullptr, ruler_elem, r, nullptr, rec_next, work, nullptr, ctx.d_status);
   KS_CHECK_LAUNCH();
   return KASCADE_OK;
 }
@@ -725,7 +736,7 @@ kascade_status launch_chase(kascade_ctx& ctx, Rec* rec, uint32_t n, const uint32
 template <int C>
 kascade_status launch_chase_dev_c(kascade_ctx& ctx, Rec* rec, uint32_t n, const uint32_t* n_dev,
                                   const uint32_t* ruler_elem, uint32_t r, const uint32_t* r_dev, Rec* rec_next,
-                                  uint32_t* work, uint32_t block, cudaStream_t s) {
+                                  uint32_t* work, uint32_t* has_pred, uint32_t block, cudaStream_t s) {
   static int occ[3] = {-1, -1, -1};
   const int bi = block == 128 ? 0 : block == 512 ? 2 : 1;
   if (occ[bi] < 0) occ[bi] = occupancy(k_chase<C>, (int)block, 0);
@@ -735,21 +746,21 @@ kascade_status launch_chase_dev_c(kascade_ctx& ctx, Rec* rec, uint32_t n, const 
   const uint64_t need_blocks = (need + warps_per_block - 1) / warps_per_block;
   if (need_blocks < grid) grid = (unsigned)(need_blocks ? need_blocks : 1);
   ProfScope ps(ctx, "chase", s);
-  k_chase<C><<<grid, block, 0, s>>>(rec, n, n_dev, ruler_elem, r, r_dev, rec_next, work, ctx.d_status);
+  k_chase<C><<<grid, block, 0, s>>>(rec, n, n_dev, ruler_elem, r, r_dev, rec_next, work, has_pred, ctx.d_status);
   KS_CHECK_LAUNCH();
   return KASCADE_OK;
 }
 
 kascade_status launch_chase_dev(kascade_ctx& ctx, Rec* rec, uint32_t n, const uint32_t* n_dev,
                                 const uint32_t* ruler_elem, uint32_t r, const uint32_t* r_dev, Rec* rec_next,
-                                uint32_t* work, const Params& p, cudaStream_t s) {
+                                uint32_t* work, uint32_t* has_pred, const Params& p, cudaStream_t s) {
   switch (p.chains) {
     case 1:
-      return launch_chase_dev_c<1>(ctx, rec, n, n_dev, ruler_elem, r, r_dev, rec_next, work, p.block, s);
+      return launch_chase_dev_c<1>(ctx, rec, n, n_dev, ruler_elem, r, r_dev, rec_next, work, has_pred, p.block, s);
     case 4:
-      return launch_chase_dev_c<4>(ctx, rec, n, n_dev, ruler_elem, r, r_dev, rec_next, work, p.block, s);
+      return launch_chase_dev_c<4>(ctx, rec, n, n_dev, ruler_elem, r, r_dev, rec_next, work, has_pred, p.block, s);
     default:
-      return launch_chase_dev_c<2>(ctx, rec, n, n_dev, ruler_elem, r, r_dev, rec_next, work, p.block, s);
+      return launch_chase_dev_c<2>(ctx, rec, n, n_dev, ruler_elem, r, r_dev, rec_next, work, has_pred, p.block, s);
   }
 }
 
@@ -940,7 +951,8 @@ kascade_status rank_deep(kascade_ctx& ctx, Rec* rec, uint32_t n, const uint32_t*
   {
     ProfScope ps(ctx, "prepare_level", s);
     k_prepare_level<<<grid, 256, 0, s>>>(rec, n, nullptr, n, elem0, ruler_elem, elem0_next, ctr,
-                                         salt_for(p.seed, level), thresh_for(p.spacing_deep), ctx.d_status);
+                                         salt_for(p.seed, level), thresh_for(p.spacing_deep), nullptr,
+                                         ctx.d_status);
     KS_CHECK_LAUNCH();
   }
   uint32_t r = 0;
@@ -1005,7 +1017,8 @@ uint32_t dev_cap_next(uint32_t cap, uint32_t spacing) {
 // writes rec1 has run, already checked against caps1; elem0_1 gives each
 // level-1 element's level-0 index.  Fills out1 and cnt[2..L]; *levels = L.
 kascade_status rank_deep_dev(kascade_ctx& ctx, Rec* rec1, Out* out1, uint32_t cap1, uint32_t* cnt,
-                             const uint32_t* elem0_1, const Params& p, cudaStream_t s, int* levels) {
+                             const uint32_t* elem0_1, const uint32_t* pred1, const Params& p, cudaStream_t s,
+                             int* levels) {
   uint32_t caps[MAX_DEV_LEVELS + 1];
   caps[1] = cap1;
   int L = 1;
@@ -1020,10 +1033,12 @@ kascade_status rank_deep_dev(kascade_ctx& ctx, Rec* rec1, Out* out1, uint32_t ca
   uint32_t* rulers[MAX_DEV_LEVELS + 1];
   const uint32_t* elem0s[MAX_DEV_LEVELS + 1];
   const uint32_t* sizes[MAX_DEV_LEVELS + 1];
+  uint32_t* preds[MAX_DEV_LEVELS + 1] = {};  // level k: which elements a chain of level k-1 ended at
   recs[1] = rec1;
   outs[1] = out1;
   elem0s[1] = elem0_1;
   sizes[1] = cnt + 1;
+  preds[1] = const_cast<uint32_t*>(pred1);
   for (int k = 1; k <= L; ++k) {
     if (k > 1) {
       recs[k] = alloc<Rec>(ctx, caps[k]);
@@ -1037,6 +1052,12 @@ kascade_status rank_deep_dev(kascade_ctx& ctx, Rec* rec1, Out* out1, uint32_t ca
       elem0s[k + 1] = e0;
       sizes[k + 1] = cnt + k + 1;
     }
+    if (k > 1 && k < L) {  // the last level is ranked by doubling and samples no rulers
+      const uint64_t words = ((uint64_t)caps[k] + 31) / 32;
+      preds[k] = alloc<uint32_t>(ctx, words);
+      if (!preds[k]) return KASCADE_ERR_OOM;
+      KS_CUDA(cudaMemsetAsync(preds[k], 0, sizeof(uint32_t) * words, s));
+    }
   }
   for (int k = 1; k < L; ++k) {
     {
@@ -1045,14 +1066,15 @@ kascade_status rank_deep_dev(kascade_ctx& ctx, Rec* rec1, Out* out1, uint32_t ca
           grid_for(ctx, ((uint64_t)caps[k] + 256 * PREP_ITEMS - 1) / (256 * PREP_ITEMS) * 256, 256, 8);
       k_prepare_level<<<grid, 256, 0, s>>>(recs[k], caps[k], sizes[k], caps[k + 1], elem0s[k], rulers[k],
                                            const_cast<uint32_t*>(elem0s[k + 1]), cnt + k + 1,
-                                           salt_for(p.seed, k), thresh_for(p.spacing_deep), ctx.d_status);
+                                           salt_for(p.seed, k), thresh_for(p.spacing_deep), preds[k],
+                                           ctx.d_status);
       KS_CHECK_LAUNCH();
     }
     uint32_t* work = alloc<uint32_t>(ctx, 1);
     if (!work) return KASCADE_ERR_OOM;
     KS_CUDA(cudaMemsetAsync(work, 0, sizeof(uint32_t), s));
     KS_TRY(launch_chase_dev(ctx, recs[k], caps[k], sizes[k], rulers[k], caps[k + 1], sizes[k + 1], recs[k + 1], work,
-                            p, s));
+                            k + 1 < L ? preds[k + 1] : nullptr, p, s));
   }
   // final level: pointer doubling, enough rounds for any list it can hold
   {
@@ -1116,19 +1138,22 @@ kascade_status rank_records_dev(kascade_ctx& ctx, Rec* rec, uint32_t n, const ui
   uint32_t* cnt = alloc<uint32_t>(ctx, MAX_DEV_LEVELS + 2);
   Rec* rec1 = alloc<Rec>(ctx, cap1);
   Out* out1 = alloc<Out>(ctx, cap1);
-  if (!cnt || !rec1 || !out1) return KASCADE_ERR_OOM;
+  const uint64_t pwords = ((uint64_t)cap1 + 31) / 32;
+  uint32_t* pred1 = alloc<uint32_t>(ctx, pwords);
+  if (!cnt || !rec1 || !out1 || !pred1) return KASCADE_ERR_OOM;
   KS_CUDA(cudaMemsetAsync(cnt, 0, sizeof(uint32_t) * (MAX_DEV_LEVELS + 2), s));
+  KS_CUDA(cudaMemsetAsync(pred1, 0, sizeof(uint32_t) * pwords, s));
   KS_TRY(launch_check_count(ctx, r0_dev, cap1, cnt + 1, s));
   // level 0 chase: capacities as bounds, the ruler count from device memory
   {
     uint32_t* work = alloc<uint32_t>(ctx, 1);
     if (!work) return KASCADE_ERR_OOM;
     KS_CUDA(cudaMemsetAsync(work, 0, sizeof(uint32_t), s));
-    KS_TRY(launch_chase_dev(ctx, rec, n, nullptr, ruler_elem0, cap1, r0_dev, rec1, work, p, s));
+    KS_TRY(launch_chase_dev(ctx, rec, n, nullptr, ruler_elem0, cap1, r0_dev, rec1, work, pred1, p, s));
   }
   // level-1 elements are level-0 rulers: their level-0 index is ruler_elem0
   int L = 1;
-  KS_TRY(rank_deep_dev(ctx, rec1, out1, cap1, cnt, ruler_elem0, p, s, &L));
+  KS_TRY(rank_deep_dev(ctx, rec1, out1, cap1, cnt, ruler_elem0, pred1, p, s, &L));
   KS_TRY(launch_propagate(ctx, rec, sink.limit(n), n, out1, cap1, sink, s));
   // the level sizes travel back with the call's status
   return report_dev_levels(ctx, cnt, L, n, s);

@@ -198,9 +198,12 @@ uint32_t dev_cap_next(uint32_t cap, uint32_t spacing);
 constexpr int MAX_DEV_LEVELS = 8;
 // Levels 1.. of that recursion: rec1 / out1 hold cap1 elements, cnt (device,
 // MAX_DEV_LEVELS + 2 words) holds level 1's size in cnt[1] once the level-0
-// chase has run; fills out1 and cnt[2..L], *levels = L.
+// chase has run; pred1 (optional, cap1 bits): level-1 elements a level-0
+// chain ended at (the others head their lists and become rulers); fills out1
+// and cnt[2..L], *levels = L.
 kascade_status rank_deep_dev(kascade_ctx& ctx, Rec* rec1, Out* out1, uint32_t cap1, uint32_t* cnt,
-                             const uint32_t* elem0_1, const Params& p, cudaStream_t s, int* levels);
+                             const uint32_t* elem0_1, const uint32_t* pred1, const Params& p, cudaStream_t s,
+                             int* levels);
 // *copy = *cnt, and KASCADE_ERR_TIMEOUT in the status word when it exceeds cap.
 kascade_status launch_check_count(kascade_ctx& ctx, const uint32_t* cnt, uint32_t cap, uint32_t* copy,
                                   cudaStream_t s);
