@@ -742,7 +742,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=list(WORKLOADS), default="list")
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=8)
+    ap.add_argument("--e2e-contexts", type=int, default=2,
+                    help="contexts (and streams) the pipelined host-buffer calls take turns on")
     ap.add_argument("--cpu-sample", type=int, default=1 << 24)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-secondary", action="store_true")
@@ -793,7 +795,12 @@ def main():
     inp, w, root, rk = main_r["inp"], main_r["w"], main_r["root"], main_r["rank"]
     hbm, _ = peaks()
 
-    # end-to-end through the host-buffer API (pinned host memory)
+    # end-to-end through the host-buffer API (pinned host memory): K steps,
+    # each with its own copy-in, ranking and copy-out inside the timed region.
+    # Serial: one context, each call complete before the next.  Pipelined (the
+    # reported value): async host-buffer calls taking turns over a ring of
+    # contexts and streams, a context synced before its next call, so one
+    # step's copy-out overlaps the next steps' copy-in and ranking.
     e2e = None
     if args.e2e_steps > 0:
         pin_in = torch.empty(n, dtype=torch.int64, pin_memory=True)
@@ -802,41 +809,94 @@ def main():
         if w is not None:
             pin_w = torch.empty(n, dtype=torch.int32, pin_memory=True)
             pin_w.copy_(w.cpu())
-        pin_root = torch.empty(n, dtype=torch.int64, pin_memory=True)
-        pin_rank = torch.empty(n, dtype=torch.int64, pin_memory=True)
-        o = kb.GpuTuning(**tune).to_opts()
+        outs = [(torch.empty(n, dtype=torch.int64, pin_memory=True), torch.empty(n, dtype=torch.int64, pin_memory=True))]
+        o_sync = kb.GpuTuning(**tune).to_opts()
+        o_async = kb.GpuTuning(**tune).to_opts()
+        o_async.async_ = 1
+        ctxs, strs = [ctx], [stream]
 
-        def e2e_step():
+        def e2e_call(i, o):
+            c, s_, (r_, k_) = ctxs[i], strs[i], outs[i]
             if kind == "list":
-                st = kb.lib.kascade_rank_list_host(ctx.handle, pin_in.data_ptr(),
+                st = kb.lib.kascade_rank_list_host(c.handle, pin_in.data_ptr(),
                                                    pin_w.data_ptr() if pin_w is not None else None, n,
-                                                   pin_root.data_ptr(), pin_rank.data_ptr(), ctypes.byref(o),
-                                                   stream.cuda_stream)
+                                                   r_.data_ptr(), k_.data_ptr(), ctypes.byref(o), s_.cuda_stream)
             else:
-                st = kb.lib.kascade_root_forest_host(ctx.handle, pin_in.data_ptr(), n, pin_root.data_ptr(),
-                                                     pin_rank.data_ptr(), ctypes.byref(o), stream.cuda_stream)
-            kb._lib.check(st, "host-buffer call", ctx.handle)
+                st = kb.lib.kascade_root_forest_host(c.handle, pin_in.data_ptr(), n, r_.data_ptr(), k_.data_ptr(),
+                                                     ctypes.byref(o), s_.cuda_stream)
+            kb._lib.check(st, "host-buffer call", c.handle)
+
+        def e2e_sync(i):
+            kb._lib.check(kb.lib.kascade_ctx_sync(ctxs[i].handle, strs[i].cuda_stream), "kascade_ctx_sync",
+                          ctxs[i].handle)
+
+        def matches(i):
+            return bool(torch.equal(outs[i][1], rk.cpu()) and torch.equal(outs[i][0], root.cpu()))
 
         # two warm-up calls: the first grows the context's arena by the device
         # copies of the host buffers, the second folds it into one block
         for _ in range(2):
-            e2e_step()
+            e2e_call(0, o_sync)
         barrier(world)
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(args.e2e_steps):
-            e2e_step()
+            e2e_call(0, o_sync)
         e1.record(stream)
         torch.cuda.synchronize()
-        te = max_over_ranks(e0.elapsed_time(e1), world) / args.e2e_steps
-        ok = bool(torch.equal(pin_rank, rk.cpu()) and torch.equal(pin_root, root.cpu()))
+        te_serial = max_over_ranks(e0.elapsed_time(e1), world) / args.e2e_steps
+        ok = matches(0)
         h2d = n * 8 + (n * 4 if w is not None else 0)
-        e2e = {"value": n * world / (te / 1000.0), "unit": "elements/s" if kind == "list" else "vertices/s",
-               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 16 * n, "ms_per_step": round(te, 3),
-               "host_matches_device": ok}
-        del pin_in, pin_w, pin_root, pin_rank
+        unit_e = "elements/s" if kind == "list" else "vertices/s"
+        e2e = {"value": n * world / (te_serial / 1000.0), "unit": unit_e, "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": 16 * n, "ms_per_step": round(te_serial, 3), "host_matches_device": ok,
+               "mode": "serial: one context, each host-buffer call complete before the next"}
+        R = max(1, args.e2e_contexts)
+        try:
+            for i in range(1, R):
+                ctxs.append(kb.Context(dev.index or 0))
+                strs.append(torch.cuda.Stream(dev))
+                outs.append((torch.empty(n, dtype=torch.int64, pin_memory=True),
+                             torch.empty(n, dtype=torch.int64, pin_memory=True)))
+                for _ in range(2):
+                    e2e_call(i, o_sync)
+            barrier(world)
+            torch.cuda.synchronize()
+            g0 = torch.cuda.Event(enable_timing=True)
+            g1 = torch.cuda.Event(enable_timing=True)
+            g0.record(stream)
+            for i in range(1, R):
+                strs[i].wait_event(g0)
+            pending = [False] * R
+            for k in range(args.e2e_steps):
+                i = k % R
+                if pending[i]:
+                    e2e_sync(i)
+                e2e_call(i, o_async)
+                pending[i] = True
+            for i in range(R):
+                if pending[i]:
+                    e2e_sync(i)
+            for i in range(1, R):
+                tail = torch.cuda.Event()
+                tail.record(strs[i])
+                stream.wait_event(tail)
+            g1.record(stream)
+            torch.cuda.synchronize()
+            te = max_over_ranks(g0.elapsed_time(g1), world) / args.e2e_steps
+            serial = {k: e2e[k] for k in ("value", "ms_per_step", "mode")}
+            e2e.update(value=n * world / (te / 1000.0), ms_per_step=round(te, 3),
+                       host_matches_device=ok and all(matches(i) for i in range(R)), serial=serial,
+                       mode=f"pipelined: async host-buffer calls taking turns over {R} contexts and streams "
+                            "(a step's copy-out overlaps the next steps' copy-in and ranking)")
+        except (RuntimeError, kb.KascadeError) as ex:  # e.g. no room for a second set of pinned buffers
+            e2e["pipelined_error"] = str(ex)[:200]
+        finally:
+            for c in ctxs[1:]:
+                c.close()
+        del pin_in, pin_w, outs
 
     # CPU baseline on the same seeded input (host copy of the device arrays),
     # its full-size ruling-set result compared with the GPU result

@@ -137,7 +137,12 @@ KASCADE_API kascade_status kascade_rank_list(kascade_ctx* ctx, const uint64_t* s
                                              uint64_t* root_out, uint64_t* rank_out,
                                              const kascade_opts* opts, void* stream);
 
-/* Host-pointer variant: copies in, ranks, copies out (pinned or pageable). */
+/* Host-pointer variant: copies in, ranks, copies out (pinned or pageable).
+ * With kascade_opts.async set it returns once the copies and the ranking are
+ * enqueued: the host buffers stay the call's (inputs unchanged, outputs
+ * unread) until kascade_ctx_sync(ctx) returns.  Calls on two contexts and two
+ * streams, from pinned buffers, then overlap one call's copy-out with the
+ * next call's copy-in (the two PCIe directions) and its ranking. */
 KASCADE_API kascade_status kascade_rank_list_host(kascade_ctx* ctx, const uint64_t* succ,
                                                   const uint32_t* weights, uint64_t n,
                                                   uint64_t* root_out, uint64_t* rank_out,
@@ -234,6 +239,7 @@ KASCADE_API kascade_status kascade_root_forest(kascade_ctx* ctx, const uint64_t*
                                                uint64_t n, uint64_t* root_out,
                                                uint64_t* depth_out, const kascade_opts* opts,
                                                void* stream);
+/* Host-pointer variant; kascade_opts.async as for kascade_rank_list_host. */
 KASCADE_API kascade_status kascade_root_forest_host(kascade_ctx* ctx, const uint64_t* parent,
                                                     uint64_t n, uint64_t* root_out,
                                                     uint64_t* depth_out, const kascade_opts* opts,

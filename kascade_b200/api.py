@@ -258,6 +258,7 @@ def rank_list_host(succ: np.ndarray, weights: Optional[np.ndarray] = None, *, tu
     rank = np.empty(n, np.uint64)
     c = ctx or default_context()
     o = (tuning or GpuTuning()).to_opts()
+    o.async_ = 0  # the arrays are returned: the call completes first
     st = lib.kascade_rank_list_host(c.handle, succ.ctypes.data, weights.ctypes.data if weights is not None else None,
                                     n, root.ctypes.data, rank.ctypes.data, ctypes.byref(o),
                                     torch.cuda.current_stream(c.device).cuda_stream)
@@ -287,6 +288,7 @@ def root_forest_host(parent: np.ndarray, *, tuning: Optional[GpuTuning] = None, 
     depth = np.empty(n, np.uint64)
     c = ctx or default_context()
     o = (tuning or GpuTuning()).to_opts()
+    o.async_ = 0  # the arrays are returned: the call completes first
     st = lib.kascade_root_forest_host(c.handle, parent.ctypes.data, n, root.ctypes.data, depth.ctypes.data,
                                       ctypes.byref(o), torch.cuda.current_stream(c.device).cuda_stream)
     check(st, "kascade_root_forest_host", c.handle)

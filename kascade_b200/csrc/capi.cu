@@ -48,6 +48,7 @@ kascade_status begin_call(kascade_ctx* ctx, cudaStream_t s, const kascade_opts* 
   KS_TRY(status_reset(*ctx, s));
   ctx->profile = o && o->profile;
   ctx->async_pending = false;
+  ctx->host_rerun.set = false;
   ctx->pending_levels = 0;
   return KASCADE_OK;
 }
@@ -236,11 +237,25 @@ KASCADE_API uint64_t kascade_scratch_bytes_root_forest(uint64_t n) {
   return 16 * n + 8 * n + 32 * n + 8 * n + 32 * n + 16 * n + (80 * n) / 16 + (192ull << 20);
 }
 
+kascade_status rank_list_host_call(kascade_ctx* c, const uint64_t* succ, const uint32_t* weights, uint64_t n,
+                                   uint64_t* root_out, uint64_t* rank_out, const kascade_opts* opts,
+                                   cudaStream_t s, bool dev);
+
 KASCADE_API kascade_status kascade_ctx_sync(kascade_ctx* c, void* stream) {
   if (!c) return KASCADE_ERR_INVALID_ARG;
   if (!c->async_pending) return c->last_status;
   c->async_pending = false;
-  return status_finish(*c, as_stream(stream));
+  kascade_status st = status_finish(*c, as_stream(stream));
+  if (st == KASCADE_ERR_TIMEOUT && c->host_rerun.set) {
+    // an async host-buffer call whose level outgrew the device-driven
+    // recursion: rank it again, on the host-driven path, before returning
+    const kascade_ctx::HostRerun r = c->host_rerun;
+    kascade_opts o = r.opts;
+    o.async = 0;
+    st = rank_list_host_call(c, r.succ, r.weights, r.n, r.root_out, r.rank_out, &o, r.stream, false);
+  }
+  c->host_rerun.set = false;
+  return st;
 }
 
 KASCADE_API uint64_t kascade_ctx_error_info(kascade_ctx* c) { return c ? c->error_info : 0; }
@@ -291,12 +306,11 @@ KASCADE_API kascade_status kascade_rank_list(kascade_ctx* c, const uint64_t* suc
   return end_call(c, s, st, opts);
 }
 
-KASCADE_API kascade_status kascade_rank_list_host(kascade_ctx* c, const uint64_t* succ, const uint32_t* weights,
-                                                  uint64_t n, uint64_t* root_out, uint64_t* rank_out,
-                                                  const kascade_opts* opts, void* stream) {
-  cudaStream_t s = as_stream(stream);
-  if (n && (!succ || !root_out || !rank_out)) return KASCADE_ERR_INVALID_ARG;
-  if (n > MAX_LIST) return KASCADE_ERR_TOO_LARGE;
+// The host-buffer list call: copies in, ranks (dev: with the device-driven
+// recursion, no host wait inside the call), copies out.
+kascade_status rank_list_host_call(kascade_ctx* c, const uint64_t* succ, const uint32_t* weights, uint64_t n,
+                                   uint64_t* root_out, uint64_t* rank_out, const kascade_opts* opts,
+                                   cudaStream_t s, bool dev) {
   KS_TRY(begin_call(c, s, opts));
   Params p = make_params(*c, opts, n);
   kascade_status st = KASCADE_OK;
@@ -312,18 +326,36 @@ KASCADE_API kascade_status kascade_rank_list_host(kascade_ctx* c, const uint64_t
     }
     if (st == KASCADE_OK) st = validate_list(*c, d_succ, n, opts, p, s);
     if (st == KASCADE_OK)
-      st = rank_list_generic(*c, d_succ, d_w ? WKind::U32 : WKind::Unit, d_w, n, d_root, d_rank, 0, p, s);
+      st = rank_list_generic(*c, d_succ, d_w ? WKind::U32 : WKind::Unit, d_w, n, d_root, d_rank, 0, p, s, dev);
     if (st == KASCADE_OK) {
       cudaError_t e = cudaMemcpyAsync(root_out, d_root, n * 8, cudaMemcpyDeviceToHost, s);
       if (e == cudaSuccess) e = cudaMemcpyAsync(rank_out, d_rank, n * 8, cudaMemcpyDeviceToHost, s);
       st = cuda_status(e);
     }
   }
-  kascade_opts o2;
-  kascade_opts_init(&o2);
-  if (opts) o2 = *opts;
-  o2.async = 0;  // host buffers must be complete on return
-  return end_call(c, s, st, &o2);
+  // opts->async: return once enqueued; the host buffers belong to the call
+  // until kascade_ctx_sync
+  return end_call(c, s, st, opts);
+}
+
+KASCADE_API kascade_status kascade_rank_list_host(kascade_ctx* c, const uint64_t* succ, const uint32_t* weights,
+                                                  uint64_t n, uint64_t* root_out, uint64_t* rank_out,
+                                                  const kascade_opts* opts, void* stream) {
+  cudaStream_t s = as_stream(stream);
+  if (!c) return KASCADE_ERR_INVALID_ARG;
+  if (n && (!succ || !root_out || !rank_out)) return KASCADE_ERR_INVALID_ARG;
+  if (n > MAX_LIST) return KASCADE_ERR_TOO_LARGE;
+  kascade_status st = rank_list_host_call(c, succ, weights, n, root_out, rank_out, opts, s, true);
+  if (opts && opts->async) {
+    if (st == KASCADE_OK) {
+      c->host_rerun = kascade_ctx::HostRerun{true, succ, weights, n, root_out, rank_out, *opts, s};
+    }
+    return st;
+  }
+  if (st != KASCADE_ERR_TIMEOUT) return st;
+  // a level outgrew the device-driven recursion: copy in and rank again on
+  // the host-driven path
+  return rank_list_host_call(c, succ, weights, n, root_out, rank_out, opts, s, false);
 }
 
 KASCADE_API kascade_status kascade_sparse_ruling_set(kascade_ctx* c, const kascade_opts* opts, uint64_t* succ_array,
@@ -441,11 +473,9 @@ KASCADE_API kascade_status kascade_root_forest_host(kascade_ctx* c, const uint64
       st = cuda_status(e);
     }
   }
-  kascade_opts o2;
-  kascade_opts_init(&o2);
-  if (opts) o2 = *opts;
-  o2.async = 0;
-  return end_call(c, s, st, &o2);
+  // opts->async: return once enqueued; the host buffers belong to the call
+  // until kascade_ctx_sync
+  return end_call(c, s, st, opts);
 }
 
 KASCADE_API kascade_status kascade_rank_via_euler_tour(kascade_ctx* c, const kascade_opts* opts, uint64_t* succ_array,

@@ -52,6 +52,19 @@ struct kascade_ctx {
   cudaEvent_t done_event = nullptr;
   cudaStream_t last_stream = nullptr;
   bool async_pending = false;
+  // an async host-buffer list call ranked by the device-driven recursion:
+  // what kascade_ctx_sync needs to rank it again on the host-driven path when
+  // a level outgrew that recursion (the host buffers are the call's until then)
+  struct HostRerun {
+    bool set = false;
+    const uint64_t* succ = nullptr;
+    const uint32_t* weights = nullptr;
+    unsigned long long n = 0;
+    uint64_t* root_out = nullptr;
+    uint64_t* rank_out = nullptr;
+    kascade_opts opts{};
+    cudaStream_t stream = nullptr;
+  } host_rerun;
   // size classes: instances of at most class_max[i] elements use a mean ruler
   // spacing of class_spacing[i] inside a batch; a call (or a batch, by the class holding
   // most of its elements) chases with class_chains[i] chains per thread in

@@ -229,3 +229,90 @@ def test_profile_and_levels(kb):
     lv = ctx.levels()
     assert lv[0] == 1 << 20 and len(lv) >= 2 and lv[1] < lv[0] // 8
     ctx.close()
+
+
+def test_host_async_pipelined_on_two_contexts(kb, oracle_mod):
+    """Host-buffer calls with async set, alternating over two contexts and two
+    streams from pinned buffers (a call's copy-out overlaps the next call's
+    copy-in): every call's outputs equal the oracle's once its context has
+    been synced, lists and forests alike."""
+    import ctypes
+
+    n = 1 << 18
+    succ_h = oracle_mod.gen_list(n, 21, 0)
+    w_h = oracle_mod.gen_weights(n, 22, 16)
+    par_h = oracle_mod.gen_forest(n, 23, 0, 4)
+    want_list = oracle_mod.rank_list(succ_h, w_h)
+    want_forest = oracle_mod.root_forest(par_h)
+    pin = lambda a, dt: torch.from_numpy(a.view(dt)).pin_memory()
+    in_succ, in_w, in_par = pin(succ_h, np.int64), pin(w_h, np.int32), pin(par_h, np.int64)
+    ctxs = [kb.Context(), kb.Context()]
+    streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+    outs = [(torch.empty(n, dtype=torch.int64).pin_memory(), torch.empty(n, dtype=torch.int64).pin_memory())
+            for _ in range(2)]
+    o = kb.GpuTuning(async_=True).to_opts()
+    pending = [None, None]
+
+    def finish(i):
+        kb._lib.check(kb.lib.kascade_ctx_sync(ctxs[i].handle, streams[i].cuda_stream), "kascade_ctx_sync",
+                      ctxs[i].handle)
+        root_o, rank_o = want_list if pending[i] == "list" else want_forest
+        np.testing.assert_array_equal(outs[i][0].numpy().view(np.uint64), root_o, err_msg=pending[i])
+        np.testing.assert_array_equal(outs[i][1].numpy().view(np.uint64), rank_o, err_msg=pending[i])
+        outs[i][0].fill_(-1)
+        outs[i][1].fill_(-1)
+
+    for step in range(6):
+        i = step % 2
+        if pending[i]:
+            finish(i)
+        kind = "list" if step % 3 != 2 else "forest"
+        if kind == "list":
+            st = kb.lib.kascade_rank_list_host(ctxs[i].handle, in_succ.data_ptr(), in_w.data_ptr(), n,
+                                               outs[i][0].data_ptr(), outs[i][1].data_ptr(), ctypes.byref(o),
+                                               streams[i].cuda_stream)
+        else:
+            st = kb.lib.kascade_root_forest_host(ctxs[i].handle, in_par.data_ptr(), n, outs[i][0].data_ptr(),
+                                                 outs[i][1].data_ptr(), ctypes.byref(o), streams[i].cuda_stream)
+        kb._lib.check(st, "host-buffer call", ctxs[i].handle)
+        pending[i] = kind
+    for i in range(2):
+        finish(i)
+
+
+@pytest.mark.parametrize("shape", ["all_roots", "short_lists"])
+def test_host_call_rerun_when_a_level_outgrows_the_device_recursion(kb, oracle_mod, shape):
+    """Host-buffer calls rank with the device-driven recursion; an input whose
+    level outgrows it (every element a root, or 2^18 lists of four elements)
+    is ranked again on the host-driven path -- at once for a synchronous
+    call, inside kascade_ctx_sync for an async one -- with the same results."""
+    import ctypes
+
+    n = 1 << 20
+    if shape == "all_roots":
+        succ_h = np.arange(n, dtype=np.uint64)
+    else:
+        succ_h = np.arange(1, n + 1, dtype=np.uint64)
+        succ_h[3::4] = np.arange(3, n, 4, dtype=np.uint64)  # every fourth element ends a list
+    w_h = oracle_mod.gen_weights(n, 5, 16)
+    root_o, rank_o = oracle_mod.rank_list(succ_h, w_h)
+    root, rank = kb.rank_list_host(succ_h, w_h)
+    np.testing.assert_array_equal(root, root_o)
+    np.testing.assert_array_equal(rank, rank_o)
+    ctx = kb.Context()
+    stream = torch.cuda.Stream()
+    in_s = torch.from_numpy(succ_h.view(np.int64)).pin_memory()
+    in_w = torch.from_numpy(w_h.view(np.int32)).pin_memory()
+    out_r = torch.full((n,), -1, dtype=torch.int64).pin_memory()
+    out_k = torch.full((n,), -1, dtype=torch.int64).pin_memory()
+    o = kb.GpuTuning(async_=True).to_opts()
+    for _ in range(2):
+        kb._lib.check(kb.lib.kascade_rank_list_host(ctx.handle, in_s.data_ptr(), in_w.data_ptr(), n, out_r.data_ptr(),
+                                                    out_k.data_ptr(), ctypes.byref(o), stream.cuda_stream),
+                      "kascade_rank_list_host", ctx.handle)
+        kb._lib.check(kb.lib.kascade_ctx_sync(ctx.handle, stream.cuda_stream), "kascade_ctx_sync", ctx.handle)
+        np.testing.assert_array_equal(out_r.numpy().view(np.uint64), root_o)
+        np.testing.assert_array_equal(out_k.numpy().view(np.uint64), rank_o)
+        out_r.fill_(-1)
+        out_k.fill_(-1)
+    ctx.close()
