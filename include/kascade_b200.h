@@ -377,7 +377,7 @@ typedef struct kascade_server_config {
                                     elements (default 2^20)                       */
   uint64_t small_batch_elements; /* elements per batch, latency lane (2^23)       */
   uint32_t latency_sms;          /* SMs the throughput lane leaves free while the
-                                    latency lane has work (default 80): its
+                                    latency lane has work (default 32): its
                                     batches then run in an SM partition (a green
                                     context) of the other SMs, rounded down to a
                                     multiple of 8; 0 = no partition             */

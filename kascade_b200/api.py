@@ -630,7 +630,7 @@ class Server:
 
     def __init__(self, device: int = 0, hbm_budget: int = 40 << 30, small_max: int = 1 << 20,
                  small_batch_elements: int = 1 << 23, max_batch_elements: int = 1 << 27,
-                 max_batch_requests: int = 4096, latency_sms: int = 80, small_reserve_pct: int = 10):
+                 max_batch_requests: int = 4096, latency_sms: int = 32, small_reserve_pct: int = 10):
         cfg = ServerConfig()
         lib.kascade_server_config_init(ctypes.byref(cfg))
         cfg.device = device

@@ -632,7 +632,7 @@ KASCADE_API void kascade_server_config_init(kascade_server_config* c) {
   c->max_batch_elements = 1ull << 27;
   c->small_max = 1ull << 20;
   c->small_batch_elements = 1ull << 23;
-  c->latency_sms = 80;
+  c->latency_sms = 32;
   c->small_reserve_pct = 10;
   c->result_heap_bytes = 0;
 }
