@@ -155,7 +155,7 @@ KASCADE_API kascade_status kascade_rank_list_host(kascade_ctx* ctx, const uint64
  * to the root on output.  Roots keep their input values, exactly as the
  * reference's GatherChase leaves them (local_pointer_chasing.cpp:18-59).
  * ------------------------------------------------------------------------- */
-/* kascade::sparse_ruling_set (sparse_ruling_set.hpp:13-18, .cpp:335-392) */
+/* kascade::sparse_ruling_set (sparse_ruling_set.hpp:13-18, sparse_ruling_set.cpp:335-392) */
 KASCADE_API kascade_status kascade_sparse_ruling_set(kascade_ctx* ctx, const kascade_opts* opts,
                                                      uint64_t* succ_array, int64_t* rank_array,
                                                      uint64_t n, void* stream);
@@ -168,7 +168,7 @@ KASCADE_API kascade_status kascade_pointer_doubling(kascade_ctx* ctx, const kasc
  * the GatherChase contract, forests of trees allowed */
 KASCADE_API kascade_status kascade_rank_on_root(kascade_ctx* ctx, uint64_t* succ_array,
                                                 int64_t* rank_array, uint64_t n, void* stream);
-/* kascade::set_initial_ranking_state (list_ranking.hpp:47-50, .cpp:60-80):
+/* kascade::set_initial_ranking_state (list_ranking.hpp:47-50, list_ranking.cpp:60-80):
  * root := succ, rank := 1 (0 at roots) */
 KASCADE_API kascade_status kascade_set_initial_ranking_state(kascade_ctx* ctx, const uint64_t* succ,
                                                              uint64_t* root_array,
@@ -233,7 +233,7 @@ KASCADE_API kascade_status kascade_compute_stats(kascade_ctx* ctx, const uint64_
  *   parent[v] (parent[v] == v marks a root) -> root_out[v], depth_out[v]
  *   (edge count to the root; 0 at roots), via an Euler tour of the forest
  *   ranked by the ruling-set ranker.
- * Replaces: rank_via_euler_tour (eulertour.hpp:22-27, .cpp:372-412).
+ * Replaces: rank_via_euler_tour (eulertour.hpp:22-27, eulertour.cpp:337-377).
  * ------------------------------------------------------------------------- */
 KASCADE_API kascade_status kascade_root_forest(kascade_ctx* ctx, const uint64_t* parent,
                                                uint64_t n, uint64_t* root_out,
@@ -250,10 +250,12 @@ KASCADE_API kascade_status kascade_root_forest_host(kascade_ctx* ctx, const uint
 KASCADE_API kascade_status kascade_rank_via_euler_tour(kascade_ctx* ctx, const kascade_opts* opts,
                                                        uint64_t* succ_array, int64_t* rank_array,
                                                        uint64_t n, void* stream);
-/* kascade::compute_euler_tour (eulertour.hpp:32-34, .cpp:414-427) on one rank:
- * the tour's successor array in the reference's element numbering, m =
- * 2 (n - #roots) + #roots elements.  tour_succ must hold 2n entries; *m_out
- * receives m.  (The high-degree proxy variant is not provided.) */
+/* kascade::compute_euler_tour (eulertour.hpp:32-34, eulertour.cpp:379-392) on
+ * one rank: the tour's successor array in the reference's element numbering,
+ * m = 2 (n - #roots) + #roots elements.  tour_succ must hold 2n entries;
+ * *m_out receives m.  The high-degree proxy construction
+ * (use_high_degree_handling, successor_utils.cpp:302-418) builds the same
+ * tour on one rank: its proxies stand in for remote parents only. */
 KASCADE_API kascade_status kascade_compute_euler_tour(kascade_ctx* ctx, const uint64_t* parent,
                                                       uint64_t n, uint64_t* tour_succ,
                                                       uint64_t* m_out, void* stream);

@@ -406,9 +406,10 @@ def compute_stats(root_array: torch.Tensor, rank_array: torch.Tensor, level: int
 def rank_via_euler_tour(config: EulerTourConfig, succ_array: torch.Tensor, rank_array: torch.Tensor,
                         ctx: Optional[Context] = None) -> None:
     """kascade::rank_via_euler_tour (eulertour.hpp:22-27), in place: parents in,
-    roots and depths out for non-roots."""
-    if config.use_high_degree_handling:
-        raise KascadeError(9, "rank_via_euler_tour: high-degree proxy handling is a multi-rank scheme")
+    roots and depths out for non-roots.  use_high_degree_handling selects the
+    reference's proxy construction (successor_utils.cpp:302-418), which on
+    one rank creates no proxy (proxies stand in for remote parents only) and
+    builds the same tree, so it changes nothing here."""
     o = config.gpu.to_opts(Algorithm.SparseRulingSet)
     _inplace(lib.kascade_rank_via_euler_tour, "kascade_rank_via_euler_tour", o, succ_array, rank_array, ctx)
 
@@ -416,9 +417,9 @@ def rank_via_euler_tour(config: EulerTourConfig, succ_array: torch.Tensor, rank_
 def compute_euler_tour(parent_array: torch.Tensor, use_high_degree_handling: bool = False,
                        ctx: Optional[Context] = None) -> torch.Tensor:
     """kascade::compute_euler_tour (eulertour.hpp:32-34): the tour's successor
-    array in the reference's element numbering (one rank)."""
-    if use_high_degree_handling:
-        raise KascadeError(9, "compute_euler_tour: high-degree proxy handling is a multi-rank scheme")
+    array in the reference's element numbering (one rank).  With
+    use_high_degree_handling the reference builds the same tour on one rank
+    (no remote parent, so no proxy vertex; successor_utils.cpp:322-339)."""
     _dev64(parent_array, "parent_array")
     n = parent_array.numel()
     out = torch.empty(max(2 * n, 1), dtype=torch.int64, device=parent_array.device)

@@ -323,10 +323,14 @@ def compute_stats_transcribed(root, rank, level: int) -> tuple[dict, list]:
     return out, (per_tree if level >= 4 else [])
 
 
-def euler_tour_transcribed(parent) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+def euler_tour_transcribed(parent, high_degree: bool = False) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
     """compute_euler_tour for one rank, transcribed statement by statement in
     plain Python (small inputs): the forest as reverse_rooted_tree(...,
-    add_back_edge=true) sends it (lib/kascade/successor_utils.cpp:265-300),
+    add_back_edge=true) sends it (lib/kascade/successor_utils.cpp:265-300;
+    high_degree: the resolve_high_degree_tag variant, successor_utils.cpp:
+    302-418, which on one rank finds no remote parent, creates no proxy and
+    sends, for each non-root i, the edge from the parent first and then the
+    back edge),
     the CSR graph as make_graph fills it -- each vertex's adjacency from its
     end backwards, in arrival order (successor_utils.cpp:236-260) -- and the
     tour as compute_euler_tour_impl builds it (lib/kascade/eulertour.cpp:
@@ -344,8 +348,15 @@ def euler_tour_transcribed(parent) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
     for i in range(n):
         if parent[i] == i:  # is_root (successor_utils.cpp:65-70)
             continue
-        recv_edges.append((i, parent[i]))
-        recv_edges.append((parent[i], i))
+        if high_degree:
+            # every parent is owned by this rank: no entry in remote_info, no
+            # proxy (successor_utils.cpp:322-339); edge to the parent's new
+            # name, then the back edge (:381-389)
+            recv_edges.append((parent[i], i))
+            recv_edges.append((i, parent[i]))
+        else:
+            recv_edges.append((i, parent[i]))
+            recv_edges.append((parent[i], i))
     # make_graph
     xadj = [0] * (n + 1)
     adjncy = [0] * len(recv_edges)

@@ -30,6 +30,7 @@ ANCHORS = {
     ("lib/kascade/eulertour.cpp", 235): "map_euler_tour_back",
     ("lib/kascade/eulertour.cpp", 337): "rank_via_euler_tour",
     ("lib/kascade/eulertour.cpp", 379): "compute_euler_tour",
+    ("lib/kascade/successor_utils.cpp", 302): "reverse_rooted_tree",
     ("lib/kascade/eulertour.hpp", 22): "rank_via_euler_tour",
     ("lib/kascade/sparse_ruling_set.hpp", 13): "sparse_ruling_set",
     ("lib/kascade/pointer_doubling.hpp", 18): "pointer_doubling",
@@ -104,6 +105,20 @@ def test_every_citation_is_inside_its_file():
                 break
         if not ok:
             bad.append(f"{where}: {name}:{ranges} runs past the end of the file")
+    assert not bad, "\n".join(bad)
+
+
+def test_no_citation_without_a_file_name():
+    """A shorthand like `eulertour.hpp:22-27, .cpp:337-377` cannot be checked:
+    every citation names its file."""
+    bare = re.compile(r"(?<![A-Za-z0-9_/-])\.(?:cpp|hpp|h):\d")
+    bad = []
+    for f in _scanned_files():
+        if f.name == "test_citations.py":
+            continue
+        for ln, line in enumerate(f.read_text(errors="replace").splitlines(), 1):
+            if bare.search(line):
+                bad.append(f"{f.relative_to(ROOT)}:{ln}: {line.strip()}")
     assert not bad, "\n".join(bad)
 
 

@@ -4,6 +4,7 @@ from __future__ import annotations
 
 import numpy as np
 import pytest
+import torch
 
 from gpu_util import DEEP, SPARSE, dev64, host_i64, host_u64
 
@@ -170,3 +171,22 @@ def test_compute_euler_tour_vs_reference_transcription(kb, oracle_mod):
         exp, _, _ = oracle_mod.euler_tour_transcribed(par)
         tour = kb.compute_euler_tour(dev64(par))
         np.testing.assert_array_equal(host_u64(tour), exp, err_msg=str(par[:16]))
+
+
+def test_high_degree_handling_flag_gives_the_same_results(kb, oracle_mod):
+    """use_high_degree_handling=True: the same tour from compute_euler_tour
+    and the same roots and depths from rank_via_euler_tour (on one rank the
+    reference's proxy construction creates no proxy)."""
+    for par in (np.zeros(3000, np.uint64), oracle_mod.gen_forest(20000, 31, 0, 3),
+                oracle_mod.gen_forest(20000, 32, 1, 2, 2000)):
+        t0 = kb.compute_euler_tour(dev64(par))
+        t1 = kb.compute_euler_tour(dev64(par), use_high_degree_handling=True)
+        assert torch.equal(t0, t1)
+        s_o = par.copy()
+        r_o = np.where(par == np.arange(par.size, dtype=np.uint64), 0, 1).astype(np.int64)
+        oracle_mod.rank_via_euler_tour(s_o, r_o)
+        s = dev64(par)
+        r = dev64(np.where(par == np.arange(par.size, dtype=np.uint64), 0, 1).astype(np.int64))
+        kb.rank_via_euler_tour(kb.EulerTourConfig(use_high_degree_handling=True), s, r)
+        np.testing.assert_array_equal(host_u64(s), s_o)
+        np.testing.assert_array_equal(host_i64(r), r_o)

@@ -193,3 +193,20 @@ def test_euler_tour_restatement_equals_transcription(oracle_mod):
         np.testing.assert_array_equal(ts, t2, err_msg=str(par[:20]))
         np.testing.assert_array_equal(tw, w2)
         np.testing.assert_array_equal(up, up2)
+
+
+def test_high_degree_variant_builds_the_same_tour_on_one_rank(oracle_mod):
+    """The resolve_high_degree_tag construction, transcribed for one rank
+    (no remote parent, so no proxy; its two edges per vertex sent in the
+    other order), gives the same CSR graph and so the same tour as the plain
+    construction: compute_euler_tour and rank_via_euler_tour accept the flag
+    with unchanged results."""
+    forests = _tour_forests()
+    forests.append(np.zeros(40, np.uint64))  # a star
+    for n in (200, 1000):
+        forests.append(oracle_mod.gen_forest(n, n + 7, 0, 5))
+    for par in forests:
+        a = oracle_mod.euler_tour_transcribed(par)
+        b = oracle_mod.euler_tour_transcribed(par, high_degree=True)
+        for x, y in zip(a, b):
+            np.testing.assert_array_equal(x, y)
