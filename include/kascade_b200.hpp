@@ -122,6 +122,14 @@ inline std::uint64_t compute_euler_tour(Context& c, std::span<const idx_t> paren
   return m;
 }
 
+// The reference's use_high_degree_handling argument: on one rank its proxy
+// construction (lib/kascade/successor_utils.cpp:302-418) creates no proxy and
+// builds the same tour, so the flag does not change the result.
+inline std::uint64_t compute_euler_tour(Context& c, std::span<const idx_t> parent, std::span<idx_t> tour,
+                                        bool /*use_high_degree_handling*/, void* stream = nullptr) {
+  return compute_euler_tour(c, parent, tour, stream);
+}
+
 inline bool is_list(Context& c, std::span<const idx_t> succ, void* stream = nullptr) {
   int ok = 0;
   check(kascade_is_list(c.get(), succ.data(), succ.size(), &ok, stream), "is_list");
