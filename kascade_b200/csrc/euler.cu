@@ -36,6 +36,7 @@ namespace {
 
 constexpr int TB_ITEMS = 2;  // vertices per thread in the tour kernels (fewer registers, more resident warps)
 constexpr int LINK_ITEMS = 8;  // vertices per thread in one linking round
+constexpr int TB_BATCH_ITEMS = 1;  // vertices per thread in a batch's tour build (its forest search adds registers)
 
 inline int bits_for(uint64_t n) {
   int b = 1;
@@ -202,11 +203,11 @@ __global__ void __launch_bounds__(256) k_tour_links(const uint32_t* __restrict__
   __shared__ uint32_t sm[33];
   __shared__ uint32_t sbase;
   const uint32_t lane = threadIdx.x & 31u;
-  const uint64_t tile_sz = (uint64_t)blockDim.x * TB_ITEMS;
+  const uint64_t tile_sz = (uint64_t)blockDim.x * TB_BATCH_ITEMS;
   for (uint64_t tile = (uint64_t)blockIdx.x * tile_sz; tile < n; tile += (uint64_t)gridDim.x * tile_sz) {
-    uint32_t pv[TB_ITEMS], sib[TB_ITEMS], first[TB_ITEMS], hw[TB_ITEMS], jv[TB_ITEMS];
+    uint32_t pv[TB_BATCH_ITEMS], sib[TB_BATCH_ITEMS], first[TB_BATCH_ITEMS], hw[TB_BATCH_ITEMS], jv[TB_BATCH_ITEMS];
 #pragma unroll
-    for (int i = 0; i < TB_ITEMS; ++i) {
+    for (int i = 0; i < TB_BATCH_ITEMS; ++i) {
       const uint64_t v = tile + (uint64_t)i * blockDim.x + threadIdx.x;
       pv[i] = (uint32_t)v;
       sib[i] = first[i] = NO_CHILD;
@@ -219,9 +220,9 @@ __global__ void __launch_bounds__(256) k_tour_links(const uint32_t* __restrict__
         jv[i] = slots.seg_of((uint32_t)v);  // v, its parent and its children belong to the same forest
       }
     }
-    uint32_t wsib[TB_ITEMS], wfirst[TB_ITEMS];
+    uint32_t wsib[TB_BATCH_ITEMS], wfirst[TB_BATCH_ITEMS];
 #pragma unroll
-    for (int i = 0; i < TB_ITEMS; ++i) {
+    for (int i = 0; i < TB_BATCH_ITEMS; ++i) {
       const uint32_t v = (uint32_t)(tile + (uint64_t)i * blockDim.x + threadIdx.x);
       if (pv[i] >= n) pv[i] = v;
       wsib[i] = wfirst[i] = 0;
@@ -230,11 +231,11 @@ __global__ void __launch_bounds__(256) k_tour_links(const uint32_t* __restrict__
         if (first[i] != NO_CHILD) wfirst[i] = __ldg(ibits + (first[i] >> 5));
       }
     }
-    Rec ru[TB_ITEMS], rd[TB_ITEMS];
-    uint32_t su[TB_ITEMS], sd[TB_ITEMS];
+    Rec ru[TB_BATCH_ITEMS], rd[TB_BATCH_ITEMS];
+    uint32_t su[TB_BATCH_ITEMS], sd[TB_BATCH_ITEMS];
     uint32_t rl = 0, cnt = 0;
 #pragma unroll
-    for (int i = 0; i < TB_ITEMS; ++i) {
+    for (int i = 0; i < TB_BATCH_ITEMS; ++i) {
       const uint32_t v = (uint32_t)(tile + (uint64_t)i * blockDim.x + threadIdx.x);
       su[i] = sd[i] = 0;
       bool leaf = false;
@@ -292,7 +293,7 @@ __global__ void __launch_bounds__(256) k_tour_links(const uint32_t* __restrict__
     __syncthreads();
     uint32_t id = sbase + pre;
 #pragma unroll
-    for (int i = 0; i < TB_ITEMS; ++i) {
+    for (int i = 0; i < TB_BATCH_ITEMS; ++i) {
       const uint64_t v = tile + (uint64_t)i * blockDim.x + threadIdx.x;
       if (v >= n) continue;
       ru[i].c = TAG_UNREACHED;
@@ -622,7 +623,8 @@ kascade_status build_tour(kascade_ctx& ctx, const uint64_t* parent, uint32_t n, 
   ProfScope ps(ctx, "tour_build", s);
   k_internal_words<<<grid_for(ctx, n, 256, 8), 256, 0, s>>>(p32, fc, n, ibits, icount, head_bits);
   KS_CHECK_LAUNCH();
-  const unsigned grid = grid_for(ctx, ((uint64_t)n + 256 * TB_ITEMS - 1) / (256 * TB_ITEMS) * 256, 256, 8);
+  const unsigned grid =
+      grid_for(ctx, ((uint64_t)n + 256 * TB_BATCH_ITEMS - 1) / (256 * TB_BATCH_ITEMS) * 256, 256, 8);
   k_tour_links<Slots><<<grid, 256, 0, s>>>(p32, n, fc, nsib, ibits, head_bits, rec, ruler_elem, counter, leaf_out,
                                            salt, slots, ctx.d_status);
   KS_CHECK_LAUNCH();
