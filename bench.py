@@ -742,7 +742,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=list(WORKLOADS), default="list")
-    ap.add_argument("--e2e-steps", type=int, default=8)
+    ap.add_argument("--e2e-steps", type=int, default=16)
     ap.add_argument("--e2e-contexts", type=int, default=2,
                     help="contexts (and streams) the pipelined host-buffer calls take turns on")
     ap.add_argument("--cpu-sample", type=int, default=1 << 24)
