@@ -240,6 +240,8 @@ KASCADE_API uint64_t kascade_scratch_bytes_root_forest(uint64_t n) {
 kascade_status rank_list_host_call(kascade_ctx* c, const uint64_t* succ, const uint32_t* weights, uint64_t n,
                                    uint64_t* root_out, uint64_t* rank_out, const kascade_opts* opts,
                                    cudaStream_t s, bool dev);
+kascade_status root_forest_host_call(kascade_ctx* c, const uint64_t* parent, uint64_t n, uint64_t* root_out,
+                                     uint64_t* depth_out, const kascade_opts* opts, cudaStream_t s, bool dev);
 
 KASCADE_API kascade_status kascade_ctx_sync(kascade_ctx* c, void* stream) {
   if (!c) return KASCADE_ERR_INVALID_ARG;
@@ -252,7 +254,8 @@ KASCADE_API kascade_status kascade_ctx_sync(kascade_ctx* c, void* stream) {
     const kascade_ctx::HostRerun r = c->host_rerun;
     kascade_opts o = r.opts;
     o.async = 0;
-    st = rank_list_host_call(c, r.succ, r.weights, r.n, r.root_out, r.rank_out, &o, r.stream, false);
+    st = r.kind == 0 ? rank_list_host_call(c, r.succ, r.weights, r.n, r.root_out, r.rank_out, &o, r.stream, false)
+                     : root_forest_host_call(c, r.succ, r.n, r.root_out, r.rank_out, &o, r.stream, false);
   }
   c->host_rerun.set = false;
   return st;
@@ -348,7 +351,7 @@ KASCADE_API kascade_status kascade_rank_list_host(kascade_ctx* c, const uint64_t
   kascade_status st = rank_list_host_call(c, succ, weights, n, root_out, rank_out, opts, s, true);
   if (opts && opts->async) {
     if (st == KASCADE_OK) {
-      c->host_rerun = kascade_ctx::HostRerun{true, succ, weights, n, root_out, rank_out, *opts, s};
+      c->host_rerun = kascade_ctx::HostRerun{true, 0, succ, weights, n, root_out, rank_out, *opts, s};
     }
     return st;
   }
@@ -448,12 +451,10 @@ KASCADE_API kascade_status kascade_root_forest(kascade_ctx* c, const uint64_t* p
   return end_call(c, s, st, opts);
 }
 
-KASCADE_API kascade_status kascade_root_forest_host(kascade_ctx* c, const uint64_t* parent, uint64_t n,
-                                                    uint64_t* root_out, uint64_t* depth_out, const kascade_opts* opts,
-                                                    void* stream) {
-  cudaStream_t s = as_stream(stream);
-  if (n && (!parent || !root_out || !depth_out)) return KASCADE_ERR_INVALID_ARG;
-  if (n > MAX_FOREST) return KASCADE_ERR_TOO_LARGE;
+// The host-buffer forest call: copies in, roots (dev: with the device-driven
+// recursion, no host wait inside the call), copies out.
+kascade_status root_forest_host_call(kascade_ctx* c, const uint64_t* parent, uint64_t n, uint64_t* root_out,
+                                     uint64_t* depth_out, const kascade_opts* opts, cudaStream_t s, bool dev) {
   KS_TRY(begin_call(c, s, opts));
   Params p = make_params(*c, opts, 2 * n);
   p.algorithm = KASCADE_ALGO_SPARSE_RULING_SET;
@@ -466,7 +467,7 @@ KASCADE_API kascade_status kascade_root_forest_host(kascade_ctx* c, const uint64
       d_depth = alloc<uint64_t>(*c, n);
       if (!d_root || !d_depth) st = KASCADE_ERR_OOM;
     }
-    if (st == KASCADE_OK) st = root_forest_impl(*c, d_par, (uint32_t)n, d_root, d_depth, 0, p, s);
+    if (st == KASCADE_OK) st = root_forest_impl(*c, d_par, (uint32_t)n, d_root, d_depth, 0, p, s, dev);
     if (st == KASCADE_OK) {
       cudaError_t e = cudaMemcpyAsync(root_out, d_root, n * 8, cudaMemcpyDeviceToHost, s);
       if (e == cudaSuccess) e = cudaMemcpyAsync(depth_out, d_depth, n * 8, cudaMemcpyDeviceToHost, s);
@@ -476,6 +477,25 @@ KASCADE_API kascade_status kascade_root_forest_host(kascade_ctx* c, const uint64
   // opts->async: return once enqueued; the host buffers belong to the call
   // until kascade_ctx_sync
   return end_call(c, s, st, opts);
+}
+
+KASCADE_API kascade_status kascade_root_forest_host(kascade_ctx* c, const uint64_t* parent, uint64_t n,
+                                                    uint64_t* root_out, uint64_t* depth_out, const kascade_opts* opts,
+                                                    void* stream) {
+  cudaStream_t s = as_stream(stream);
+  if (!c) return KASCADE_ERR_INVALID_ARG;
+  if (n && (!parent || !root_out || !depth_out)) return KASCADE_ERR_INVALID_ARG;
+  if (n > MAX_FOREST) return KASCADE_ERR_TOO_LARGE;
+  kascade_status st = root_forest_host_call(c, parent, n, root_out, depth_out, opts, s, true);
+  if (opts && opts->async) {
+    if (st == KASCADE_OK)
+      c->host_rerun = kascade_ctx::HostRerun{true, 1, parent, nullptr, n, root_out, depth_out, *opts, s};
+    return st;
+  }
+  if (st != KASCADE_ERR_TIMEOUT) return st;
+  // a tour level outgrew the device-driven recursion: copy in and root again
+  // on the host-driven path
+  return root_forest_host_call(c, parent, n, root_out, depth_out, opts, s, false);
 }
 
 KASCADE_API kascade_status kascade_rank_via_euler_tour(kascade_ctx* c, const kascade_opts* opts, uint64_t* succ_array,

@@ -276,13 +276,16 @@ __device__ uint32_t block_exclusive_scan(uint32_t* v, uint32_t m) {
 //   otherwise (second pass): tiles inside one window's region, buckets are
 //     its SUBS sub-windows
 // More entries than a bucket holds means some element was logged twice.
+//   used (first pass, optional): the chunks the chase took (its chunk
+//     cursor); the chunks after them are empty and are skipped
 template <bool FROM_LOG, uint32_t ITEMS, uint32_t BLOCKS>
 __global__ void __launch_bounds__(PT_THREADS, BLOCKS) k_partition(const LogEnt* __restrict__ src,
                                                              const uint32_t* __restrict__ src_info, uint32_t nchunks,
                                                              const Out* __restrict__ out1, uint32_t limit,
                                                              uint32_t nb, LogEnt* __restrict__ dst,
                                                              uint32_t* __restrict__ dcursor,
-                                                             uint32_t* __restrict__ beyond, DevStatus* st) {
+                                                             uint32_t* __restrict__ beyond,
+                                                             const uint32_t* __restrict__ used, DevStatus* st) {
   constexpr uint32_t PT_TILE = PT_THREADS * ITEMS;
   constexpr uint32_t PT_TILE_CHUNKS = PT_TILE / LOG_CHUNK;
   static_assert(PT_TILE % LOG_CHUNK == 0 && WIN % PT_TILE == 0, "tiles hold whole log chunks");
@@ -293,6 +296,7 @@ __global__ void __launch_bounds__(PT_THREADS, BLOCKS) k_partition(const LogEnt* 
   uint32_t* gbase = cnt + nbk;                                   // the tile's start in each bucket
   __shared__ uint32_t fills[PT_TILE_CHUNKS];
   __shared__ uint32_t nbeyond;
+  if (FROM_LOG && used) nchunks = min(nchunks, __ldcg(used));
   const uint32_t ntiles =
       FROM_LOG ? (nchunks + PT_TILE_CHUNKS - 1) / PT_TILE_CHUNKS : nb * (WIN / PT_TILE);
   for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
@@ -396,14 +400,15 @@ __global__ void __launch_bounds__(FIN_THREADS, 2) k_place(const LogEnt* __restri
                                                             uint32_t* __restrict__ ucount, uint32_t ucap,
                                                             const uint64_t* __restrict__ seg_off,
                                                             const uint32_t* __restrict__ hint, uint32_t nseg,
-                                                            const uint32_t* __restrict__ plus_one, DevStatus* st) {
+                                                            const uint32_t* __restrict__ plus_one,
+                                                            const uint32_t* __restrict__ beyond_want, DevStatus* st) {
   extern __shared__ __align__(16) unsigned char smraw[];
   unsigned long long* rank_s = reinterpret_cast<unsigned long long*>(smraw);  // SUB entries
   uint32_t* root_s = reinterpret_cast<uint32_t*>(rank_s + SUB);               // SUB entries
   __shared__ uint32_t plus_s[SUB / 32];                                       // the sub-window's plus_one words
   const uint32_t lane = threadIdx.x & 31u;
   if (blockIdx.x == 0 && threadIdx.x == 0 && heads_are_rulers) {
-    const uint32_t want = n - limit;
+    const uint32_t want = beyond_want ? *beyond_want : n - limit;
     if (*beyond > want) set_error(st, KASCADE_ERR_NOT_A_LIST, *beyond);
     if (*beyond < want) set_error(st, KASCADE_ERR_CYCLE, *beyond);
   }
@@ -629,6 +634,8 @@ kascade_status rank_level0_log(kascade_ctx& ctx, const Rec* rec, uint32_t n, uin
   if (r0_dev) {
     KS_CUDA(cudaMemsetAsync(lv, 0, sizeof(uint32_t) * (MAX_DEV_LEVELS + 2), s));
     KS_CUDA(cudaMemsetAsync(pred1, 0, sizeof(uint32_t) * pwords, s));
+    // a tour sized for a bound: its length is the output slots plus the down edges
+    if (t.beyond_want) KS_TRY(launch_set_level0(ctx, lv, t.limit, t.beyond_want, s));
     KS_TRY(launch_check_count(ctx, r0_dev, r0, lv + 1, s));
   }
   const uint32_t* r_dev = r0_dev ? lv + 1 : nullptr;
@@ -687,14 +694,14 @@ kascade_status rank_level0_log(kascade_ctx& ctx, const Rec* rec, uint32_t n, uin
     ProfScope ps(ctx, "resolve", s);
     const uint32_t tiles1 = (nchunks + TILE1 / LOG_CHUNK - 1) / (TILE1 / LOG_CHUNK);
     k1<<<(unsigned)std::min<uint64_t>(tiles1, (uint64_t)ctx.usable_sms() * P1_BLOCKS), PT_THREADS, smem1, s>>>(
-        log, chunk_fill, nchunks, out1, limit, nb, part, cursor1, beyond, ctx.d_status);
+        log, chunk_fill, nchunks, out1, limit, nb, part, cursor1, beyond, chunk_cursor, ctx.d_status);
     KS_CHECK_LAUNCH();
   }
   const uint32_t tiles2 = nb * (WIN / TILE2);
   if (tiles2) {
     ProfScope ps(ctx, "partition", s);
     k2<<<(unsigned)std::min<uint64_t>(tiles2, (uint64_t)ctx.usable_sms() * P2_BLOCKS), PT_THREADS, smem2, s>>>(
-        part, cursor1, 0, nullptr, limit, nb, part2, cursor2, beyond, ctx.d_status);
+        part, cursor1, 0, nullptr, limit, nb, part2, cursor2, beyond, nullptr, ctx.d_status);
     KS_CHECK_LAUNCH();
   }
   // the first pass's output is dead after the second: it holds the unreached list
@@ -706,7 +713,8 @@ kascade_status rank_level0_log(kascade_ctx& ctx, const Rec* rec, uint32_t n, uin
     const size_t smem = SUB * (sizeof(unsigned long long) + sizeof(uint32_t));
     k_place<<<(unsigned)std::max<uint64_t>(1, std::min<uint64_t>(items, (uint64_t)ctx.usable_sms() * 2)),
                 FIN_THREADS, smem, s>>>(part2, cursor2, nb, limit, n, beyond, t.heads_are_rulers, t.root, t.rank,
-                                        ulist, ucount, ucap, t.seg_off, t.hint, t.nseg, t.plus_one, ctx.d_status);
+                                        ulist, ucount, ucap, t.seg_off, t.hint, t.nseg, t.plus_one, t.beyond_want,
+                                        ctx.d_status);
     KS_CHECK_LAUNCH();
   }
   if (!t.heads_are_rulers) {

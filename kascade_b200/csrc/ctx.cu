@@ -107,7 +107,9 @@ kascade_status status_finish(kascade_ctx& ctx, cudaStream_t s) {
   collect_times(ctx);
   if (ctx.pending_levels) {
     const uint32_t* lv = reinterpret_cast<const uint32_t*>(ctx.h_pinned + KS_PINNED_LEVELS);
-    ctx.last_levels.assign(1, ctx.pending_n);
+    // level 0's size: the call's n, or the device's count when only that
+    // knows it (a tour sized for a bound)
+    ctx.last_levels.assign(1, lv[0] ? (unsigned long long)lv[0] : ctx.pending_n);
     for (int k = 1; k <= ctx.pending_levels; ++k) ctx.last_levels.push_back(lv[k]);
     ctx.pending_levels = 0;
   }

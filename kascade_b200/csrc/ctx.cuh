@@ -52,16 +52,17 @@ struct kascade_ctx {
   cudaEvent_t done_event = nullptr;
   cudaStream_t last_stream = nullptr;
   bool async_pending = false;
-  // an async host-buffer list call ranked by the device-driven recursion:
-  // what kascade_ctx_sync needs to rank it again on the host-driven path when
-  // a level outgrew that recursion (the host buffers are the call's until then)
+  // an async host-buffer call ranked by the device-driven recursion: what
+  // kascade_ctx_sync needs to rank it again on the host-driven path when a
+  // level outgrew that recursion (the host buffers are the call's until then)
   struct HostRerun {
     bool set = false;
-    const uint64_t* succ = nullptr;
+    int kind = 0;                     // 0: kascade_rank_list_host, 1: kascade_root_forest_host
+    const uint64_t* succ = nullptr;  // successors, or parents
     const uint32_t* weights = nullptr;
     unsigned long long n = 0;
     uint64_t* root_out = nullptr;
-    uint64_t* rank_out = nullptr;
+    uint64_t* rank_out = nullptr;  // ranks, or depths
     kascade_opts opts{};
     cudaStream_t stream = nullptr;
   } host_rerun;

@@ -657,7 +657,6 @@ kascade_status root_forest_impl(kascade_ctx& ctx, const uint64_t* parent, uint32
   KS_CUDA(cudaMemsetAsync(ctr, 0, 2 * sizeof(uint32_t), s));
   KS_CUDA(cudaMemsetAsync(head_bits, 0, sizeof(uint32_t) * (size_t)words, s));
   KS_TRY(link_children(ctx, parent, n, fc, nsib, p32, root_bits, s));
-  uint32_t downs = 0;
   {
     ProfScope ps(ctx, "tour_build", s);
     k_internal_words<<<grid_for(ctx, n, 256, 8), 256, 0, s>>>(p32, fc, n, ibits, icount, head_bits);
@@ -666,10 +665,6 @@ kascade_status root_forest_impl(kascade_ctx& ctx, const uint64_t* parent, uint32
     k_internal_pack<<<grid_for(ctx, words, 256, 8), 256, 0, s>>>(ibits, ipre, words, iw);
     KS_CHECK_LAUNCH();
   }
-  // the tour's length: one element per vertex, and a down edge per non-root
-  // vertex with children (one host read)
-  KS_TRY(read_u32(ctx, ctr + 1, &downs, s));
-  const uint32_t m = n + downs;
   {
     ProfScope ps(ctx, "tour_build", s);
     const unsigned grid = grid_for(ctx, ((uint64_t)n + 256 * TB_ITEMS - 1) / (256 * TB_ITEMS) * 256, 256, 8);
@@ -679,15 +674,26 @@ kascade_status root_forest_impl(kascade_ctx& ctx, const uint64_t* parent, uint32
     KS_CHECK_LAUNCH();
   }
   SinkTour sink{root_out, depth_out, n, keep_roots, leaf_bits};
-  if (device_levels && m > p.base_max && p.max_levels > 0) {
-    if (m < p.level0_log_min)
-      return rank_records_dev(ctx, rec, m, ctr, dev_cap_next(m, p.spacing0), ruler_elem, sink, p, s);
+  // The tour's length m = n + (down edges) is on the device (ctr[1]).  The
+  // device-driven recursion sizes for the bound 2n instead of reading it: no
+  // element points into the unused slots [m, 2n), no chase visits them, and
+  // outputs come only from slots below n; the write-free level 0 takes its
+  // count of down-edge entries from ctr[1].  (Every element below m exists
+  // and m >= n > base_max, so no path that reads every record is taken.)
+  const uint32_t m_cap = 2 * n;  // n <= 2^31 - 1
+  if (device_levels && n > p.base_max && p.max_levels > 0) {
+    sink.downs_dev = ctr + 1;
+    if (m_cap < p.level0_log_min)
+      return rank_records_dev(ctx, rec, m_cap, ctr, dev_cap_next(m_cap, p.spacing0), ruler_elem, sink, p, s);
     if (!keep_roots)  // the write-free level 0 with the ruler count and the deeper levels on the device
-      return rank_level0_log(ctx, rec, m, dev_cap_next(m, p.spacing0), ruler_elem, sink.log_target(m), p, s, ctr);
+      return rank_level0_log(ctx, rec, m_cap, dev_cap_next(m_cap, p.spacing0), ruler_elem,
+                             sink.log_target(m_cap), p, s, ctr);
   }
-  uint32_t r = 0;
+  // the host-driven path: the tour's length and the ruler count (host reads)
+  uint32_t downs = 0, r = 0;
+  KS_TRY(read_u32(ctx, ctr + 1, &downs, s));
   KS_TRY(read_u32(ctx, ctr, &r, s));
-  return rank_records(ctx, rec, m, r, ruler_elem, sink, p, s);
+  return rank_records(ctx, rec, n + downs, r, ruler_elem, sink, p, s);
 }
 
 // Tours of a batch of forests whose parents are given in one compact vertex

@@ -1113,6 +1113,16 @@ kascade_status rank_deep_dev(kascade_ctx& ctx, Rec* rec1, Out* out1, uint32_t ca
   return KASCADE_OK;
 }
 
+__global__ void k_set_level0(uint32_t* lv, uint32_t base, const uint32_t* add) { lv[0] = base + *add; }
+
+kascade_status launch_set_level0(kascade_ctx& ctx, uint32_t* lv, uint32_t base, const uint32_t* add,
+                                 cudaStream_t s) {
+  (void)ctx;
+  k_set_level0<<<1, 1, 0, s>>>(lv, base, add);
+  KS_CHECK_LAUNCH();
+  return KASCADE_OK;
+}
+
 kascade_status launch_check_count(kascade_ctx& ctx, const uint32_t* cnt, uint32_t cap, uint32_t* copy,
                                   cudaStream_t s) {
   k_check_count<<<1, 1, 0, s>>>(cnt, cap, copy, ctx.d_status);
@@ -1126,6 +1136,17 @@ kascade_status report_dev_levels(kascade_ctx& ctx, const uint32_t* cnt, int L, u
   ctx.pending_levels = L;
   ctx.pending_n = n;
   return KASCADE_OK;
+}
+
+// the device count to add to a sink's element count for level 0's size
+// (tours sized for a bound), or null
+template <class Sink>
+const uint32_t* level0_add(const Sink&) {
+  return nullptr;
+}
+template <>
+const uint32_t* level0_add<SinkTour>(const SinkTour& t) {
+  return t.downs_dev;
 }
 
 template <class Sink>
@@ -1143,6 +1164,7 @@ kascade_status rank_records_dev(kascade_ctx& ctx, Rec* rec, uint32_t n, const ui
   if (!cnt || !rec1 || !out1 || !pred1) return KASCADE_ERR_OOM;
   KS_CUDA(cudaMemsetAsync(cnt, 0, sizeof(uint32_t) * (MAX_DEV_LEVELS + 2), s));
   KS_CUDA(cudaMemsetAsync(pred1, 0, sizeof(uint32_t) * pwords, s));
+  if (const uint32_t* d = level0_add(sink)) KS_TRY(launch_set_level0(ctx, cnt, sink.limit(n), d, s));
   KS_TRY(launch_check_count(ctx, r0_dev, cap1, cnt + 1, s));
   // level 0 chase: capacities as bounds, the ruler count from device memory
   {

@@ -57,6 +57,9 @@ struct LogTarget {
   // bit x set: element x's rank output is one more than its rank in the list
   // (a tree rooting's leaves, whose down and up edge share one element)
   const uint32_t* plus_one = nullptr;
+  // heads_are_rulers: how many elements at or above limit a valid input logs
+  // (device memory; null: every element from limit to n)
+  const uint32_t* beyond_want = nullptr;
 };
 
 // Plain arrays. keep_roots: leave root entries untouched (the reference's
@@ -93,11 +96,15 @@ struct SinkTour {
   uint32_t nv;
   int keep_roots;
   const uint32_t* leaf_bits = nullptr;
+  // the tour's down-edge count in device memory when the records are sized
+  // for a bound (2 nv) rather than the tour's length
+  const uint32_t* downs_dev = nullptr;
   uint32_t limit(uint32_t n) const { return n < nv ? n : nv; }
   // the tour build makes every tour head a ruler
   LogTarget log_target(uint32_t n) const {
     LogTarget t{root, depth, limit(n), keep_roots, 1};
     t.plus_one = leaf_bits;
+    t.beyond_want = downs_dev;
     return t;
   }
   __device__ __forceinline__ void put(uint32_t x, uint64_t rk, uint32_t rt, bool is_root) const {
@@ -205,6 +212,10 @@ kascade_status rank_deep_dev(kascade_ctx& ctx, Rec* rec1, Out* out1, uint32_t ca
                              const uint32_t* elem0_1, const uint32_t* pred1, const Params& p, cudaStream_t s,
                              int* levels);
 // *copy = *cnt, and KASCADE_ERR_TIMEOUT in the status word when it exceeds cap.
+// lv[0] = base + *add: level 0's size in the device-driven level array when
+// only the device knows it (a tour's length), reported in place of the call's n.
+kascade_status launch_set_level0(kascade_ctx& ctx, uint32_t* lv, uint32_t base, const uint32_t* add,
+                                 cudaStream_t s);
 kascade_status launch_check_count(kascade_ctx& ctx, const uint32_t* cnt, uint32_t cap, uint32_t* copy,
                                   cudaStream_t s);
 // Level sizes cnt[1..L] travel back with the call's status read.

@@ -190,3 +190,58 @@ def test_high_degree_handling_flag_gives_the_same_results(kb, oracle_mod):
         kb.rank_via_euler_tour(kb.EulerTourConfig(use_high_degree_handling=True), s, r)
         np.testing.assert_array_equal(host_u64(s), s_o)
         np.testing.assert_array_equal(host_i64(r), r_o)
+
+
+@pytest.mark.parametrize("shape", ["all_roots", "pairs"])
+def test_forest_host_call_rerun_when_a_level_outgrows_the_device_recursion(kb, oracle_mod, shape):
+    """Forests whose tour gives ~n rulers (every vertex a root, or 2^19
+    two-vertex trees) outgrow the device-driven recursion: the host-buffer
+    call roots them again on the host-driven path -- at once when
+    synchronous, inside kascade_ctx_sync when async -- and the device-pointer
+    call likewise; the results equal the oracle's."""
+    import ctypes
+
+    n = 1 << 20
+    par = np.arange(n, dtype=np.uint64)
+    if shape == "pairs":
+        par[1::2] = np.arange(0, n, 2, dtype=np.uint64)
+    root_o, depth_o = oracle_mod.root_forest(par)
+    root, depth = kb.root_forest_host(par)
+    np.testing.assert_array_equal(root, root_o)
+    np.testing.assert_array_equal(depth, depth_o)
+    root_d, depth_d = kb.root_forest(dev64(par))
+    np.testing.assert_array_equal(host_u64(root_d), root_o)
+    np.testing.assert_array_equal(host_u64(depth_d), depth_o)
+    ctx = kb.Context()
+    stream = torch.cuda.Stream()
+    in_p = torch.from_numpy(par.view(np.int64)).pin_memory()
+    out_r = torch.full((n,), -1, dtype=torch.int64).pin_memory()
+    out_d = torch.full((n,), -1, dtype=torch.int64).pin_memory()
+    o = kb.GpuTuning(async_=True).to_opts()
+    for _ in range(2):
+        kb._lib.check(kb.lib.kascade_root_forest_host(ctx.handle, in_p.data_ptr(), n, out_r.data_ptr(),
+                                                      out_d.data_ptr(), ctypes.byref(o), stream.cuda_stream),
+                      "kascade_root_forest_host", ctx.handle)
+        kb._lib.check(kb.lib.kascade_ctx_sync(ctx.handle, stream.cuda_stream), "kascade_ctx_sync", ctx.handle)
+        np.testing.assert_array_equal(out_r.numpy().view(np.uint64), root_o)
+        np.testing.assert_array_equal(out_d.numpy().view(np.uint64), depth_o)
+        out_r.fill_(-1)
+        out_d.fill_(-1)
+    ctx.close()
+
+
+def test_forest_levels_report_the_tour_length(kb, oracle_mod):
+    """The device-driven tour ranking sizes its records for 2n but reports
+    the tour's length (n + vertices with a down edge) as level 0."""
+    n = 1 << 21
+    par = oracle_mod.gen_forest(n, 77, 0, 4)
+    ctx = kb.Context()
+    kb.root_forest(dev64(par), ctx=ctx)
+    torch.cuda.synchronize()
+    lv = ctx.levels()
+    internal = np.zeros(n, bool)
+    nonroot = par != np.arange(n, dtype=np.uint64)
+    internal[par[nonroot].astype(np.int64)] = True
+    downs = int((internal & nonroot).sum())
+    assert lv[0] == n + downs, (lv[:2], n, downs)
+    ctx.close()
