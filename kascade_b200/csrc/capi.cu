@@ -580,18 +580,6 @@ kascade_status rank_batch_device_call(kascade_ctx* c, const kascade_segment* seg
   const kascade_status st = rank_batch_impl(*c, segs, nseg, in, weights, total, root_out, rank_out, opts, s, true);
   return end_call(c, s, st, opts);
 }
-// A complete call on the host-driven recursion only: every level's kernels are
-// launched after the previous level's size is read back, so a change of the
-// context's SM budget applies from the next level on.
-kascade_status rank_batch_host_levels_call(kascade_ctx* c, const kascade_segment* segs, uint32_t nseg,
-                                           const uint64_t* in, const uint32_t* weights, uint64_t total,
-                                           uint64_t* root_out, uint64_t* rank_out, const kascade_opts* opts,
-                                           cudaStream_t s) {
-  if (total && (!segs || !nseg || !in || !root_out || !rank_out)) return KASCADE_ERR_INVALID_ARG;
-  KS_TRY(begin_call(c, s, opts));
-  const kascade_status st = rank_batch_impl(*c, segs, nseg, in, weights, total, root_out, rank_out, opts, s, false);
-  return end_call(c, s, st, opts);
-}
 kascade_status batch_plan_create(int device, const kascade_segment* segs, uint32_t nseg, const uint64_t* in,
                                  const uint32_t* weights, uint64_t total, uint64_t* root_out, uint64_t* rank_out,
                                  const kascade_opts* opts, kascade_batch_plan** out);
