@@ -133,18 +133,34 @@ constexpr uint32_t PIECE = 16384;
 constexpr int LATENCY_HOLD_MS = 20;
 
 // Gather device-resident request inputs (and weights, or their unit / zero
-// fill) into the batch's concatenated buffers: one launch per batch.
+// fill) into the batch's concatenated buffers: one launch per batch.  A thread
+// has GATHER_UNROLL independent loads in flight per round (one load at a time
+// left the copy far below the HBM rate).
+constexpr uint32_t GATHER_UNROLL = 4;
 __global__ void __launch_bounds__(256) k_gather(const Piece* __restrict__ pieces, uint32_t npieces,
                                                 uint64_t* __restrict__ d_in, uint32_t* __restrict__ d_w) {
   for (uint32_t p = blockIdx.x; p < npieces; p += gridDim.x) {
     const Piece pc = pieces[p];
-    if (pc.src_in)
-      for (uint32_t i = threadIdx.x; i < pc.n; i += blockDim.x) d_in[pc.dst + i] = __ldcs(pc.src_in + i);
-    if (d_w) {
-      if (pc.src_w)
-        for (uint32_t i = threadIdx.x; i < pc.n; i += blockDim.x) d_w[pc.dst + i] = __ldcs(pc.src_w + i);
-      else
-        for (uint32_t i = threadIdx.x; i < pc.n; i += blockDim.x) d_w[pc.dst + i] = pc.fill;
+    for (uint32_t i0 = threadIdx.x; i0 < pc.n; i0 += blockDim.x * GATHER_UNROLL) {
+      unsigned long long v[GATHER_UNROLL];
+      uint32_t wv[GATHER_UNROLL];
+#pragma unroll
+      for (uint32_t u = 0; u < GATHER_UNROLL; ++u) {
+        const uint32_t i = i0 + u * blockDim.x;
+        v[u] = 0;
+        wv[u] = pc.fill;
+        if (i < pc.n) {
+          if (pc.src_in) v[u] = __ldcs(reinterpret_cast<const unsigned long long*>(pc.src_in) + i);
+          if (d_w && pc.src_w) wv[u] = __ldcs(pc.src_w + i);
+        }
+      }
+#pragma unroll
+      for (uint32_t u = 0; u < GATHER_UNROLL; ++u) {
+        const uint32_t i = i0 + u * blockDim.x;
+        if (i >= pc.n) continue;
+        if (pc.src_in) d_in[pc.dst + i] = v[u];
+        if (d_w) d_w[pc.dst + i] = wv[u];
+      }
     }
   }
 }
