@@ -858,6 +858,9 @@ def main():
                "d2h_bytes_per_step": 16 * n, "ms_per_step": round(te_serial, 3), "host_matches_device": ok,
                "mode": "serial: one context, each host-buffer call complete before the next"}
         R = max(1, args.e2e_contexts)
+        # set-up of the extra contexts on every rank first; the ranks agree on
+        # its outcome before any of them enters a collective of the timed part
+        setup_err = None
         try:
             for i in range(1, R):
                 ctxs.append(kb.Context(dev.index or 0))
@@ -866,6 +869,11 @@ def main():
                              torch.empty(n, dtype=torch.int64, pin_memory=True)))
                 for _ in range(2):
                     e2e_call(i, o_sync)
+        except (RuntimeError, kb.KascadeError) as ex:  # e.g. no room for a second set of pinned buffers
+            setup_err = str(ex)[:200]
+        if max_over_ranks(1.0 if setup_err else 0.0, world) > 0.0:
+            e2e["pipelined_error"] = setup_err or "set-up failed on another rank"
+        else:
             barrier(world)
             torch.cuda.synchronize()
             g0 = torch.cuda.Event(enable_timing=True)
@@ -895,11 +903,8 @@ def main():
                        host_matches_device=ok and all(matches(i) for i in range(R)), serial=serial,
                        mode=f"pipelined: async host-buffer calls taking turns over {R} contexts and streams "
                             "(a step's copy-out overlaps the next steps' copy-in and ranking)")
-        except (RuntimeError, kb.KascadeError) as ex:  # e.g. no room for a second set of pinned buffers
-            e2e["pipelined_error"] = str(ex)[:200]
-        finally:
-            for c in ctxs[1:]:
-                c.close()
+        for c in ctxs[1:]:
+            c.close()
         del pin_in, pin_w, outs
 
     # CPU baseline on the same seeded input (host copy of the device arrays),
