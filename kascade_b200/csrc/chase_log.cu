@@ -56,8 +56,8 @@ constexpr uint32_t PT_THREADS = 256;    // partition: threads per block
 // SM (more tiles in flight per SM than 4096-entry tiles at 2 blocks)
 constexpr uint32_t P1_ITEMS = 8, P1_BLOCKS = 4;
 constexpr uint32_t P2_ITEMS = 8, P2_BLOCKS = 4;
-constexpr uint32_t FIN_THREADS = 256;  // resolve: threads per block (one sub-window per iteration)
-constexpr uint32_t FIN_GROUP = 8;      // resolve: entries a thread has in flight
+constexpr uint32_t FIN_THREADS = 512;  // place: threads per block (one sub-window per iteration; 2 blocks per SM)
+constexpr uint32_t FIN_GROUP = 8;      // place: entries a thread has in flight
 constexpr uint32_t NO_ROOT = 0xFFFFFFFFu;          // shared-memory root slot not written
 constexpr unsigned long long NOT_REACHED = ~0ull;  // root output of an element no chain reached
 
