@@ -620,19 +620,28 @@ __global__ void __launch_bounds__(256) k_pd_init(const Rec* __restrict__ rec, ui
   }
 }
 
+// One round of pointer jumping over the previous round's records `a`: an
+// element not yet at its root follows its pointer JUMPS times there (a chain
+// of dependent reads of `a` only, never of `b`), so a round multiplies every
+// pointer's reach by JUMPS + 1.  JUMPS = 1 is classic doubling; the last level
+// of the device-driven recursion (at most 2^17 elements, L2-resident, a fixed
+// number of launches) takes JUMPS = 3: half the launches for three reads each.
+template <int JUMPS>
 __global__ void __launch_bounds__(256) k_pd_round(const PdRec* __restrict__ a, PdRec* __restrict__ b, uint32_t n,
                                                   const uint32_t* __restrict__ n_dev, uint32_t* __restrict__ active) {
   if (n_dev) n = min(*n_dev, n);
   uint32_t cnt = 0;
   for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; x < n; x += (uint64_t)gridDim.x * blockDim.x) {
     PdRec e = a[x];
-    if (!(e.done & 1u)) {
-      PdRec t = a[e.succ];
+#pragma unroll
+    for (int j = 0; j < JUMPS; ++j) {
+      if (e.done & 1u) break;
+      const PdRec t = a[e.succ];
       e.rank += t.rank;
       e.succ = t.succ;
       e.done = t.done & 1u;
-      cnt += (e.done & 1u) ? 0u : 1u;
     }
+    cnt += (e.done & 1u) ? 0u : 1u;
     b[x] = e;
   }
 #pragma unroll
@@ -914,7 +923,7 @@ kascade_status pointer_double_records(kascade_ctx& ctx, const Rec* rec, uint32_t
     KS_CUDA(cudaMemsetAsync(active, 0, sizeof(uint32_t), s));
     {
       ProfScope ps(ctx, "pd_round", s);
-      k_pd_round<<<grid, 256, 0, s>>>(a, b, n, nullptr, active);
+      k_pd_round<1><<<grid, 256, 0, s>>>(a, b, n, nullptr, active);
       KS_CHECK_LAUNCH();
     }
     PdRec* t = a;
@@ -1087,10 +1096,12 @@ kascade_status rank_deep_dev(kascade_ctx& ctx, Rec* rec1, Out* out1, uint32_t ca
     ProfScope ps(ctx, "pd_final_level", s);
     k_pd_init<<<grid, 256, 0, s>>>(recs[L], m, sizes[L], a, ctx.d_status);
     KS_CHECK_LAUNCH();
-    int rounds = 2;
-    while ((1ull << (rounds - 2)) < m) ++rounds;
+    // rounds of reach x4 until 4^rounds >= 4m: any list of at most m elements
+    int lg = 0;
+    while ((1ull << lg) < m) ++lg;
+    const int rounds = (lg + 1) / 2 + 1;
     for (int i = 0; i < rounds; ++i) {
-      k_pd_round<<<grid, 256, 0, s>>>(a, b, m, sizes[L], active);
+      k_pd_round<3><<<grid, 256, 0, s>>>(a, b, m, sizes[L], active);
       KS_CHECK_LAUNCH();
       PdRec* t = a;
       a = b;
