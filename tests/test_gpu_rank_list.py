@@ -116,6 +116,31 @@ def test_write_free_many_lists_several_windows(kb, oracle_mod):
         np.testing.assert_array_equal(host_u64(rank), rank_o)
 
 
+@pytest.mark.parametrize("spacing", [16, 48, 2000])
+@pytest.mark.parametrize("lists", [1, 3000])
+def test_write_free_spacings_and_list_counts(kb, oracle_mod, spacing, lists):
+    """The write-free level 0 from dense to very sparse rulers: at spacing
+    2000 the few rulers are all taken at once and every chain is long (the
+    longest ~15 000 hops); with 3000 lists most lists hold no ruler but their
+    root, so their heads are walked after the place step.  Results stay
+    exact, and a second call on the same input agrees."""
+    rng = np.random.default_rng(spacing * 7 + lists)
+    n = (1 << 22) + 5
+    order = rng.permutation(n).astype(np.uint64)
+    cuts = np.sort(rng.choice(np.arange(1, n), size=lists - 1, replace=False))
+    succ_h = np.empty(n, np.uint64)
+    for seg in np.split(order, cuts):
+        succ_h[seg[:-1]] = seg[1:]
+        succ_h[seg[-1]] = seg[-1]
+    w_h = rng.integers(0, 1 << 16, n).astype(np.uint32)
+    root_o, rank_o = oracle_mod.rank_list(succ_h, w_h)
+    tuning = kb.GpuTuning(level0_mode=2, ruler_spacing=spacing)
+    for _ in range(2):
+        root, rank = kb.rank_list(dev64(succ_h), dev32(w_h), tuning=tuning)
+        np.testing.assert_array_equal(host_u64(root), root_o)
+        np.testing.assert_array_equal(host_u64(rank), rank_o)
+
+
 @pytest.mark.parametrize("offset", [(0, 0), (1, 0), (0, 1), (1, 3)])
 def test_input_alignment(kb, oracle_mod, offset):
     """Inputs that start 16 B aligned take the bulk-copy prepare for their full
