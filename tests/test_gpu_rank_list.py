@@ -233,6 +233,53 @@ def test_host_variant(kb, oracle_mod):
     np.testing.assert_array_equal(rank, rank_o)
 
 
+def test_host_calls_odd_sizes_offset_outputs_and_an_unsynced_async_call(kb, oracle_mod):
+    """Host-buffer calls on one context: odd sizes from 1 to 9 Mi elements
+    (the context's arena grows between them), output buffers that start 8 B
+    past an aligned address (pageable numpy memory), and an async call that is
+    followed by another call on the same context without kascade_ctx_sync
+    (the async call's outputs are complete all the same)."""
+    import ctypes
+
+    ctx = kb.Context()
+    for n in (1, 7, 4097, (9 << 20) + 3):
+        succ_h = oracle_mod.gen_list(n, 0x51 + n, 0)
+        w_h = oracle_mod.gen_weights(n, 0x52, 16)
+        root_o, rank_o = oracle_mod.rank_list(succ_h, w_h)
+        root, rank = kb.rank_list_host(succ_h, w_h, ctx=ctx)
+        np.testing.assert_array_equal(root, root_o)
+        np.testing.assert_array_equal(rank, rank_o)
+        # outputs 8 B past a 32 B boundary (pageable numpy memory)
+        big_r = np.zeros(n + 1, np.uint64)
+        big_k = np.zeros(n + 1, np.uint64)
+        o = kb.GpuTuning().to_opts()
+        st = kb.lib.kascade_rank_list_host(ctx.handle, succ_h.ctypes.data, w_h.ctypes.data, n,
+                                           big_r[1:].ctypes.data, big_k[1:].ctypes.data, ctypes.byref(o),
+                                           torch.cuda.current_stream().cuda_stream)
+        kb._lib.check(st, "kascade_rank_list_host", ctx.handle)
+        np.testing.assert_array_equal(big_r[1:], root_o)
+        np.testing.assert_array_equal(big_k[1:], rank_o)
+        assert big_r[0] == 0 and big_k[0] == 0
+    # an async call, then a forest call on the same context before any sync
+    n = 300_001
+    succ_h = oracle_mod.gen_list(n, 0x53, 1)
+    root_o, rank_o = oracle_mod.rank_list(succ_h)
+    par_h = oracle_mod.gen_forest(n, 0x54, 0, 5)
+    froot_o, depth_o = oracle_mod.root_forest(par_h)
+    r1 = np.zeros(n, np.uint64)
+    k1 = np.zeros(n, np.uint64)
+    o = kb.GpuTuning(async_=True).to_opts()
+    s = torch.cuda.current_stream().cuda_stream
+    kb._lib.check(kb.lib.kascade_rank_list_host(ctx.handle, succ_h.ctypes.data, None, n, r1.ctypes.data,
+                                                k1.ctypes.data, ctypes.byref(o), s), "async call", ctx.handle)
+    froot, depth = kb.root_forest_host(par_h, ctx=ctx)
+    np.testing.assert_array_equal(r1, root_o)
+    np.testing.assert_array_equal(k1, rank_o)
+    np.testing.assert_array_equal(froot, froot_o)
+    np.testing.assert_array_equal(depth, depth_o)
+    ctx.close()
+
+
 def test_seed_independence(kb, oracle_mod):
     """Ruler choice cannot change the result."""
     n = 250_000
