@@ -112,6 +112,10 @@ __global__ void __launch_bounds__(512) k_chase_log(const Rec* __restrict__ rec, 
                                                    uint32_t max_hops, uint32_t* __restrict__ has_pred,
                                                    DevStatus* st) {
   constexpr uint32_t BATCH = 32u * C;
+  // has_pred holds one bit per ruler of the capacity; a count past the
+  // capacity (reported by the caller's count check, and the level redone)
+  // leaves tags beyond it, whose bits are not recorded
+  const uint32_t pred_cap = r;
   if (r_dev) r = min(r, *r_dev);  // the ruler count on the device, r its capacity
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t lt = lanemask_lt();
@@ -194,7 +198,7 @@ __global__ void __launch_bounds__(512) k_chase_log(const Rec* __restrict__ rec, 
           // back at its own ruler: a rootless cycle holding one ruler
           if (tag_id(rr[c].c) == cid[c])
             set_error(st, KASCADE_ERR_CYCLE, cid[c]);
-          else if (has_pred)  // that ruler has a predecessor in the ruler sub-list
+          else if (has_pred && tag_id(rr[c].c) < pred_cap)  // that ruler has a predecessor in the ruler sub-list
             atomicOr(has_pred + (tag_id(rr[c].c) >> 5), 1u << (tag_id(rr[c].c) & 31));
           Rec o;
           o.a = acc[c];

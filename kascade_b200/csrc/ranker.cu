@@ -328,6 +328,9 @@ __global__ void __launch_bounds__(512) k_chase(Rec* __restrict__ rec, uint32_t n
                                                uint32_t* __restrict__ work, uint32_t* __restrict__ has_pred,
                                                DevStatus* st) {
   // device-driven recursion: sizes from device memory, n and r capacities
+  // (has_pred holds one bit per ruler of the capacity; a count past it is
+  // reported by the caller's count check and the level redone)
+  const uint32_t pred_cap = r;
   if (n_dev) n = min(*n_dev, n);
   if (r_dev) r = min(*r_dev, r);
   constexpr uint32_t BATCH = 32u * C;
@@ -420,7 +423,7 @@ __global__ void __launch_bounds__(512) k_chase(Rec* __restrict__ rec, uint32_t n
         // (a valid chain only ends at another ruler)
         if (tag_id(tg) == cid[c])
           set_error(st, KASCADE_ERR_CYCLE, cid[c]);
-        else if (has_pred)
+        else if (has_pred && tag_id(tg) < pred_cap)
           atomicOr(has_pred + (tag_id(tg) >> 5), 1u << (tag_id(tg) & 31));  // that ruler has a predecessor
         Rec o;
         o.a = acc[c];
